@@ -1,0 +1,352 @@
+#!/usr/bin/env python
+"""bench.py -- Newton-solve ms to 1e-4 FP64 relative residual on B200.
+
+Workload (default ``hetcube48``): the 352,947-DOF heterogeneous cube (48^3 hexes, 6 tets
+each, per-tet E log-uniform in [1e4, 1e8] from 8 seeded Voronoi regions, nu = 0.45, squashed
+by a rigid slab, ground + slab IPC plane barriers), seeded synthetic data in StiffGIPC's
+triplet layout (stgipc/scenes.py).  Its 6.75 M triplets (540 MB) exceed the 126 MB L2, so
+no flush is needed between steps.
+
+One step = one Newton linear solve through the public C ABI, ``stg_solve_linear_system``:
+triplets -> convert (sort/merge to unique upper BCOO) -> MAS hierarchy build -> Galerkin
+assembly + bank inverses -> PCG until ||b - A x|| / ||b|| <= 1e-4 (FP64 recursive residual,
+FP64 true residual reported).
+
+  value  : ms per solve of the FP32 path (FP32 blocks/vectors in SpMV + MAS, FP64 dots,
+           FP64 residual replacement), inputs resident in HBM.
+  plain  : the same solve with FP64 SpMV/vectors (the reference's numerics), same stop rule.
+  e2e    : the FP32 solve with the triplets and b copied host->device from pinned memory and
+           x copied back, every step.
+
+``--impl reference`` times the CPU oracle port (the reference's MAS-PCG restated in C,
+oracle/) on the host cores: the reference itself is GPU-only and cannot be built here
+(it needs Eigen 3.4).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "stiff-gipc_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "Newton-solve ms to 1e-4 FP64 rel. residual: learned+FP32 vs plain MAS-PCG"
+WORKLOADS = {
+    "hetcube48": dict(builder="make_heterogeneous_cube", kw=dict(n=48),
+                      desc="352,947-DOF heterogeneous cube (48^3 hexes, 663,552 tets, E logU[1e4,1e8] x 8 Voronoi regions)"),
+    "cube16": dict(builder="make_cube_drop", kw=dict(n=16),
+                   desc="14,739-DOF cube drop (16^3 hexes, 24,576 tets, E=1e5, ground barrier)"),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="hetcube48")
+    ap.add_argument("--bank", type=int, default=16)
+    ap.add_argument("--refine", type=int, default=32)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget-s", type=float, default=20.0)
+    return ap.parse_args()
+
+
+def load_system(name, seed_offset=0):
+    from stgipc import scenes
+    w = WORKLOADS[name]
+    kw = dict(w["kw"])
+    cache = os.environ.get("STGIPC_SCENE_CACHE") or os.path.join(tempfile.gettempdir(), "stgipc_scenes")
+    os.environ["STGIPC_SCENE_CACHE"] = cache
+    if seed_offset:
+        kw["seed"] = {"hetcube48": 1005, "cube16": 1001}[name] + seed_offset
+    key = name + (f"_s{seed_offset}" if seed_offset else "")
+    return scenes.cached(getattr(scenes, w["builder"]), key, **kw), w["desc"]
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.strip()]
+        except Exception:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(sysm, budget_s, bank):
+    """The oracle's MAS-PCG (single thread C port) on a bounded sample: convert + MAS build +
+    assembly once, then PCG iterations until the relative residual reaches 1e-4 or the time
+    budget ends; the per-solve time is set-up + per-iteration time x the iterations the full
+    solve needs (measured if it finished, else the GPU FP64 path's count)."""
+    from oracle import oracle as orc
+    t0 = time.perf_counter()
+    r, c, b = orc.convert(sysm.rows, sysm.cols, sysm.blocks)
+    m = orc.Mas(bank, sysm.num_verts, sysm.neighbor_start, sysm.neighbor_num, sysm.neighbor_list, *sysm.slot_maps(bank))
+    m.build()
+    m.assemble(r, c, b)
+    t_setup = time.perf_counter() - t0
+    return orc, (r, c, b), m, t_setup
+
+
+def run_reference(args):
+    """--impl reference: the CPU oracle port of the reference's MAS-PCG on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sysm, desc = load_system(args.workload)
+    from oracle import oracle as orc
+    orc.build()
+    cores = 1
+    times, iters_seen = [], []
+    budget = max(2.0, 150.0 / max(1, args.steps + args.warmup))
+    for step in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        r, c, b = orc.convert(sysm.rows, sysm.cols, sysm.blocks)
+        m = orc.Mas(args.bank, sysm.num_verts, sysm.neighbor_start, sysm.neighbor_num, sysm.neighbor_list,
+                    *sysm.slot_maps(args.bank))
+        m.build()
+        m.assemble(r, c, b)
+        t_setup = time.perf_counter() - t0
+        x, st, t_iter, done = orc.pcg_timed(r, c, b, sysm.b, mas=m, tol=1e-4, stop_rule="relative_residual",
+                                            budget_s=budget)
+        per_solve = t_setup + t_iter * (st["iterations"] if done else orc.extrapolated_iterations(st))
+        if step >= args.warmup:
+            times.append(per_solve * 1e3)
+            iters_seen.append(st["iterations"])
+    ms = statistics.mean(times)
+    line = {"metric": METRIC, "value": ms, "unit": "ms", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": args.workload, "desc": desc, "dof": sysm.n, "bank": args.bank,
+                       "stop": "||b-Ax||/||b|| <= 1e-4"},
+            "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores, "kind": "port",
+                             "sample": f"per step: convert + MAS build/assembly + up to {budget:.0f} s of PCG "
+                                       f"iterations, scaled to a full solve ({iters_seen[-1]} iterations seen)"},
+            "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    from stgipc import PCGSolverConfig, Solver
+
+    # every rank solves its own independent replica (a single Newton solve does not shard)
+    sysm, desc = load_system(args.workload, seed_offset=rank)
+    stream = torch.cuda.current_stream(dev)
+
+    rows = torch.from_numpy(sysm.rows).to(dev)
+    cols = torch.from_numpy(sysm.cols).to(dev)
+    blocks = torch.from_numpy(sysm.blocks.reshape(-1)).to(dev)
+    b = torch.from_numpy(sysm.b).to(dev)
+    x = torch.zeros_like(b)
+    pm, rm = sysm.slot_maps(args.bank)
+
+    def make(precision):
+        cfg = PCGSolverConfig(bank_size=args.bank, precision=precision, stop_rule="relative_residual",
+                              global_tol_rate=1e-4, refine_interval=args.refine, loop="graph",
+                              graph_batch=args.batch, max_iter_ratio=0.3)
+        s = Solver(cfg, stream=stream)
+        s.mas_init(sysm.num_verts, sysm.neighbor_start, sysm.neighbor_num, sysm.neighbor_list, pm, rm)
+        return s
+
+    fast, plain = make("fp32"), make("fp64")
+
+    def solve(s, xx=x):
+        return s.solve_linear_system(rows, cols, blocks, b, xx, stats=False)
+
+    def timed(s, k):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(k):
+            solve(s)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        return ev0.elapsed_time(ev1) / k
+
+    for _ in range(args.warmup):
+        solve(fast)
+        solve(plain)
+    st_fast = fast.solve_linear_system(rows, cols, blocks, b, x)
+    x_fast = x.clone()
+    st_plain = plain.solve_linear_system(rows, cols, blocks, b, x)
+    x_plain = x.clone()
+    err_fast = float(torch.linalg.norm(x_fast - x_plain) / torch.linalg.norm(x_plain))
+
+    with ClockSampler(local) as clk:
+        ms_fast = timed(fast, args.steps)
+    ms_plain = timed(plain, max(1, args.steps // 2))
+
+    # e2e: host (pinned) -> device copies of the triplets and b, solve, x back to the host
+    h_rows = torch.from_numpy(sysm.rows).pin_memory()
+    h_cols = torch.from_numpy(sysm.cols).pin_memory()
+    h_blocks = torch.from_numpy(sysm.blocks.reshape(-1)).pin_memory()
+    h_b = torch.from_numpy(sysm.b).pin_memory()
+    h_x = torch.empty_like(h_b).pin_memory()
+    d_rows, d_cols, d_blocks, d_b, d_x = (torch.empty_like(t, device=dev) for t in (h_rows, h_cols, h_blocks, h_b, h_b))
+
+    def e2e_step():
+        d_rows.copy_(h_rows, non_blocking=True)
+        d_cols.copy_(h_cols, non_blocking=True)
+        d_blocks.copy_(h_blocks, non_blocking=True)
+        d_b.copy_(h_b, non_blocking=True)
+        fast.solve_linear_system(d_rows, d_cols, d_blocks, d_b, d_x, stats=False)
+        h_x.copy_(d_x, non_blocking=True)
+
+    e2e_step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1) / args.steps
+    h2d = sum(t.numel() * t.element_size() for t in (h_rows, h_cols, h_blocks, h_b))
+    d2h = h_x.numel() * h_x.element_size()
+
+    # roofline of the dominant kernel: the PCG SpMV of the FP32 path, timed live
+    solve(fast)
+    spmv_ms, spmv_bytes = fast.profile_spmv(reps=100)
+
+    def gmax(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ms_fast, ms_plain, ms_e2e = gmax(ms_fast), gmax(ms_plain), gmax(ms_e2e)
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as orc
+        orc.build()
+        t0 = time.perf_counter()
+        r, c, bb = orc.convert(sysm.rows, sysm.cols, sysm.blocks)
+        m = orc.Mas(args.bank, sysm.num_verts, sysm.neighbor_start, sysm.neighbor_num, sysm.neighbor_list, pm, rm)
+        m.build()
+        m.assemble(r, c, bb)
+        t_setup = time.perf_counter() - t0
+        _, st_c, t_iter, done = orc.pcg_timed(r, c, bb, sysm.b, mas=m, tol=1e-4, stop_rule="relative_residual",
+                                             budget_s=args.cpu_budget_s)
+        n_it = st_c["iterations"] if done else st_plain["iterations"]
+        cpu = {"value": (t_setup + t_iter * n_it) * 1e3, "unit": "ms", "cores": 1, "kind": "port",
+               "sample": f"oracle MAS-PCG (bank {args.bank}): convert + MAS build/assembly ({t_setup:.1f} s) + "
+                         f"{st_c['iterations']} PCG iterations ({'converged' if done else 'time-bounded'}), "
+                         f"per-iteration time x {n_it} iterations"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ms_fast, "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_fast, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64 dots, FP64 residual replacement)", "data": "synthetic",
+            "config": {"workload": args.workload, "desc": desc, "dof": sysm.n, "nnzb": st_fast["nnzb"],
+                       "triplets": int(sysm.rows.size), "bank": args.bank, "ordering": "Morton",
+                       "stop": "||b-Ax||/||b|| <= 1e-4", "refine_interval": args.refine, "graph_batch": args.batch,
+                       "l2": "inputs larger than L2 (triplets 540 MB); no flush",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "iterations": st_fast["iterations"], "rel_residual": st_fast["rel_residual"],
+            "plain_fp64_ms": ms_plain, "plain_fp64_iterations": st_plain["iterations"],
+            "plain_fp64_rel_residual": st_plain["rel_residual"], "speedup_vs_plain": ms_plain / ms_fast,
+            "fp32_vs_fp64_solution_rel_err": err_fast,
+            "phases_ms": {k: round(st_fast[k], 3) for k in ("ms_convert", "ms_mas_build", "ms_mas_assemble", "ms_pcg")},
+            "dof_iter_per_s": sysm.n * st_fast["iterations"] / (ms_fast * 1e-3),
+            "roofline": {"bound": "hbm", "kernel": "k_pcg_spmv<float>", "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                         "bytes_per_launch": spmv_bytes, "ms_per_launch": spmv_ms,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(st_fast["kernel_launches"] * args.steps),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    fast.close()
+    plain.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

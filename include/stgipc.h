@@ -1,0 +1,204 @@
+/*
+ * stgipc.h -- C ABI of the B200 (sm_100a) Newton linear solve for StiffGIPC.
+ *
+ * One handle = one GlobalLinearSystem + PCGSolver + MAS preconditioner instance, bound to
+ * one CUDA stream and one host thread (the reference is single-threaded per simulation;
+ * its statistics are thread_local, gipc/statistics.h:14-16).  Handles share no state.
+ *
+ * Pointer conventions
+ *   - stg_mas_init() takes HOST arrays: they are the mesh-side tables that the reference
+ *     uploads from host vectors once per scene (app/common/sim_bootstrap.cpp:276-306).
+ *   - every other entry point takes DEVICE pointers on the handle's stream, as the
+ *     reference's GIPCTripletMatrix / DenseVectorView buffers live on the device
+ *     (linear_system/linear_system/global_matrix.h:52-253).
+ *   - 3x3 blocks are FP64, column-major (Eigen::Matrix3d): element (i,j) at [j*3+i].
+ *   - block indices: ABD bodies own [0, 4*abd_bodies), FEM vertex v owns
+ *     4*abd_bodies + v (GIPC.cu:10329-10330, 10482-10483).  n = 3 * block rows.
+ *
+ * Error convention
+ *   The reference aborts on CUDA errors (CUDA_SAFE_CALL, cuda_tools/cuda_tools.h:36-46) or
+ *   exit(0)s on launch errors (:52-96).  Here every entry point returns an int status
+ *   (STG_OK or a code below) and never aborts; stg_last_error() gives a message.
+ */
+#ifndef STGIPC_H
+#define STGIPC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define STGIPC_VERSION 1
+
+/* ---- status codes ---------------------------------------------------------------- */
+enum
+{
+    STG_OK = 0,
+    STG_ERR_INVALID = 1,        /* bad argument / size                                */
+    STG_ERR_CUDA = 2,           /* a CUDA call failed (message in stg_last_error)       */
+    STG_ERR_NOT_READY = 3,      /* stg_mas_init / assemble not called yet              */
+    STG_MAX_ITER = 4,           /* PCG stopped at max_iter; x holds the last iterate   */
+    STG_BREAKDOWN = 5,          /* p^T A p <= 0 or non-finite                          */
+    STG_ERR_TIMEOUT = 6,        /* a bounded device wait gave up                       */
+    STG_ERR_NO_DEVICE = 7       /* no usable CUDA device                               */
+};
+
+/* ---- configuration ---------------------------------------------------------------- */
+enum { STG_PREC_FP64 = 0, STG_PREC_FP32 = 1 };
+enum { STG_PRECOND_DIAG = 0, STG_PRECOND_MAS = 1, STG_PRECOND_NONE = 2 };
+enum { STG_STOP_REFERENCE = 0, STG_STOP_RELATIVE_RESIDUAL = 1 };
+enum { STG_LOOP_HOST = 0, STG_LOOP_GRAPH = 1, STG_LOOP_PERSISTENT = 2 };
+
+typedef struct stg_config
+{
+    int bank_size;          /* MAS partition size: 16 (CEMAS as shipped) or 32         */
+    int precision;          /* STG_PREC_FP64: FP64 SpMV/vectors, FP32 MAS apply (as the
+                               reference); STG_PREC_FP32: FP32 blocks/vectors for SpMV and
+                               MAS, FP64 dots, FP64 residual replacement               */
+    int preconditioner;     /* STG_PRECOND_MAS (P_type==1) / STG_PRECOND_DIAG / NONE   */
+    int stop_rule;          /* STG_STOP_REFERENCE: |r.z| <= tol * r0.z0 (pcg_solver.cu:279-280)
+                               STG_STOP_RELATIVE_RESIDUAL: ||r||/||b|| <= tol            */
+    double tol;             /* PCGSolverConfig::global_tol_rate (1e-4)                 */
+    double max_iter_ratio;  /* PCGSolverConfig::max_iter_ratio (0.3): max_iter = ratio*n */
+    int refine_interval;    /* FP32 mode: recompute r = b - A x in FP64 every k iters    */
+    int loop_mode;          /* STG_LOOP_HOST / STG_LOOP_GRAPH / STG_LOOP_PERSISTENT      */
+    int graph_batch;        /* iterations per captured graph launch (STG_LOOP_GRAPH)     */
+    int learned;            /* 1: learned coarse correction inside flexible PCG          */
+    void* stream;           /* cudaStream_t (NULL = legacy default stream)               */
+} stg_config;
+
+/* Fills `cfg` with the reference defaults: bank 16, FP64, MAS, reference stop rule,
+ * tol 1e-4, ratio 0.3, refine 32, graph loop, batch 8, learned off, default stream. */
+void stg_config_default(stg_config* cfg);
+
+typedef struct stg_stats
+{
+    int status;             /* same value the call returned                          */
+    int iterations;         /* PCG iteration count as returned by PCGSolver::pcg     */
+    double rz0;             /* r0 . z0                                               */
+    double rz_final;        /* last r . z                                            */
+    double rel_residual;    /* ||b - A x|| / ||b|| recomputed in FP64 after the solve */
+    double rel_residual_recursive; /* ||r_k|| / ||b|| of the recurrence at exit      */
+    int nnzb;               /* unique upper blocks after convert                     */
+    int levels;             /* MAS levelnum                                          */
+    int total_clusters;     /* MAS totalNumberClusters                               */
+    int replacements;       /* FP64 residual replacements (FP32 mode)                */
+    int learned_accepted;   /* learned corrections kept                              */
+    int learned_rejected;   /* learned corrections rejected (plain MAS used)         */
+    float ms_convert;       /* device time per phase (CUDA events; 0 if not timed)   */
+    float ms_mas_build;
+    float ms_mas_assemble;
+    float ms_pcg;
+    float ms_total;
+    int kernel_launches;    /* kernels this call launched                            */
+} stg_stats;
+
+typedef struct stg_solver* stg_handle;
+
+/* Latest error message of this thread (never NULL). */
+const char* stg_last_error(void);
+
+/* ---- lifetime ---------------------------------------------------------------------- */
+/* Replaces: GIPC::create_LinearSystem (StiffGIPC/gipc/gipc.cu:46-75) building
+ * GlobalLinearSystem + PCGSolver(PCGSolverConfig) (linear_system/solver/pcg_solver.h:6-16)
+ * + MAS_Preconditioner / DiagPreconditioner. */
+int stg_create(const stg_config* cfg, stg_handle* out);
+int stg_destroy(stg_handle h);
+
+/* Replaces: MASPreconditioner::initPreconditioner_Neighbor + initPreconditioner_Matrix
+ * (MASPreconditioner.cu:2291-2358) with the uploads of sim_bootstrap.cpp:276-306.
+ * HOST arrays: neighbour CSR (load_mesh.cpp:934-1040), partId_map_real (part_map_size =
+ * part_offset * bank_size, -1 padding) and real_map_partId (vert_num), set_mas_partition
+ * (sim_bootstrap.cpp:90-113).  collision_node_offset = first FEM vertex in the contact
+ * pair numbering (tet_mesh.abd_vertexOffset). */
+int stg_mas_init(stg_handle h, int vert_num, int collision_node_offset,
+                 const uint32_t* neighbor_start, const uint32_t* neighbor_num,
+                 const uint32_t* neighbor_list, int neighbor_list_size,
+                 const int32_t* part_map, int part_map_size, const int32_t* real_map);
+
+/* ---- individual stages ------------------------------------------------------------- */
+/* Replaces: Converter::srbk_convert (linear_system/utils/converter.cu:32-51, 88-238).
+ * Sorts `count` triplets by (row<<32)+col, merges duplicates (summing blocks) and writes
+ * the unique sorted BCOO back into the first *unique_count entries of the same arrays,
+ * as the reference does in place. */
+int stg_convert(stg_handle h, int count, int32_t* rows, int32_t* cols, double* blocks,
+                int* unique_count);
+
+/* Replaces: Spmv::srbk_spmv (linear_system/utils/spmv.cu:188-313):
+ * y = a * A * x + b * y, A symmetric given by its unique upper blocks sorted by (row,col). */
+int stg_spmv(stg_handle h, double a, const double* blocks, const int32_t* rows,
+             const int32_t* cols, int nnzb, const double* x, double b, double* y, int n);
+
+/* Replaces: MAS_Preconditioner::assemble (preconditioner/fem_mas_preconditioner.cu:18-31):
+ * calculate_subsystem_bcoo_indices (i_preconditioner.cu:32-73) + setPreconditioner_bcoo
+ * (MASPreconditioner.cu:2207-2245: ReorderRealtime + PrepareHessian_bcoo + inverse).
+ * `contacts` is the device int4 array _collisonPairs (GIPC.cuh:49-66), `ncp` = h_cpNum[0]. */
+int stg_mas_assemble(stg_handle h, const double* blocks, const int32_t* rows,
+                     const int32_t* cols, int nnzb, int fem_block_offset,
+                     const int32_t* contacts, int ncp);
+
+/* Replaces: MAS_Preconditioner::apply -> MASPreconditioner::preconditioning
+ * (fem_mas_preconditioner.cu:33-37, MASPreconditioner.cu:2248-2289).  r, z: the FEM
+ * sub-range, 3 * vert_num doubles. */
+int stg_mas_apply(stg_handle h, const double* r, double* z);
+
+/* Replaces: PCGSolver::solve / pcg (linear_system/solver/pcg_solver.cu:158-332) with the
+ * preconditioner composition of GlobalLinearSystem::apply_preconditioner
+ * (global_linear_system.cu:167-180).  Requires the BCOO to be the one last assembled
+ * (stg_mas_assemble or stg_solve_linear_system).  x is overwritten (x0 = 0). */
+int stg_pcg_solve(stg_handle h, const double* blocks, const int32_t* rows, const int32_t* cols,
+                  int nnzb, const double* b, double* x, int n, stg_stats* stats);
+
+/* ---- the whole Newton linear solve ------------------------------------------------- */
+typedef struct stg_system
+{
+    /* triplets as GIPCTripletMatrix holds them before convert (global_triplet_offset) */
+    int triplet_count;
+    const int32_t* rows;
+    const int32_t* cols;
+    const double* blocks;
+    int n;                      /* 3 * block rows                                      */
+    const double* b;            /* right-hand side (gradient), n doubles              */
+    /* MAS inputs */
+    int fem_block_offset;       /* 4 * abd_bodies                                      */
+    const int32_t* contacts;    /* int4 collision pairs or NULL                        */
+    int ncp;
+    /* ABD 12x12 block-Jacobi (abd_preconditioner.cu:20-38): row-major inverses or NULL */
+    int abd_bodies;
+    const double* abd_inv;
+} stg_system;
+
+/* Replaces: GlobalLinearSystem::solve_linear_system (global_linear_system.cu:136-148):
+ * convert_new -> preconditioner assemble -> PCG -> solution.  Writes x (n doubles).
+ * Returns STG_OK, STG_MAX_ITER or an error. */
+int stg_solve_linear_system(stg_handle h, const stg_system* sys, double* x, stg_stats* stats);
+
+/* ---- introspection (tests) ---------------------------------------------------------- */
+/* Level count and cluster count of the last MAS build. */
+int stg_mas_info(stg_handle h, int* levels, int* total_clusters, int* level_size /* 2*(L+1) */);
+
+/* Copies the last MAS hierarchy to HOST arrays (any may be NULL):
+ * fine_mask[V], prefix_orig[M/bank], coarse_tables[L*V], going_next[max(total,V)],
+ * coarse_table[V*(L-1)]. */
+int stg_mas_export_hierarchy(stg_handle h, uint32_t* fine_mask, int32_t* prefix_orig,
+                             int32_t* coarse_tables, int32_t* going_next,
+                             int32_t* coarse_table);
+
+/* Copies the assembled FP64 bank matrices and FP32 inverses to HOST arrays
+ * (nbanks * bank*(bank+1)/2 * 9 values each; either may be NULL). */
+int stg_mas_export_matrices(stg_handle h, double* mat, float* inv, int* nbanks);
+
+/* Measurement hook (no counterpart in the reference, whose PCG times phases with
+ * cudaEventSynchronize, pcg_solver.cu:204-323): times `reps` back-to-back launches of the
+ * PCG's SpMV kernel (q = A p with p.q fused) on the system of the last solve, with CUDA
+ * events on the handle's stream.  avg_ms = mean duration per launch; bytes = algorithmic
+ * bytes per launch, nnzb*(block + 8) + 3*n*vec with block = 72 (FP64) or 36 (FP32) and
+ * vec = 8 or 4 (each array counted once). */
+int stg_profile_spmv(stg_handle h, int reps, float* avg_ms, double* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STGIPC_H */

@@ -1,0 +1,905 @@
+/*
+ * stg_oracle.c -- CPU oracle for the StiffGIPC Newton linear solve.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker the GPU path is compared against; it
+ * is loaded by tests/, by __graft_entry__.smoke() and by bench.py's CPU-baseline leg, and by
+ * nothing else.  The product (libstgipc.so) never links or calls it.
+ *
+ * It restates, serially and in plain C, the reference's algorithms for the hot path:
+ *   - srbk_convert  : StiffGIPC/linear_system/utils/converter.cu:32-51, 88-131, 171-238
+ *   - srbk_spmv     : StiffGIPC/linear_system/utils/spmv.cu:188-313
+ *   - PCG           : StiffGIPC/linear_system/solver/pcg_solver.cu:158-332
+ *   - preconditioner composition: global_linear_system.cu:167-180,
+ *                     abd_preconditioner.cu:20-38, diag_preconditioner.cu:9-66
+ *   - MAS hierarchy : StiffGIPC/MASPreconditioner.cu:29-625 (kernels), 1132-1548 (contacts),
+ *                     1551-1826 (drivers), 1731-1750 (level count)
+ *   - MAS assembly  : MASPreconditioner.cu:1829-2075 (PrepareHessian_bcoo), 2207-2245
+ *   - MAS inverse   : MASPreconditioner.cu:630-726 (__inverse6_P96x96)
+ *   - MAS apply     : MASPreconditioner.cu:729-879, 957-1027, 2248-2289
+ *   - subsystem index selection: i_preconditioner.cu:32-73
+ *
+ * Where the reference kernels rely on warp-synchronous shared-memory races
+ * (_preparePrefixSumL0_new, _buildConnectMaskLx_new, _nextLevelCluster, _buildLevel1_new),
+ * this oracle implements the intended semantics: per-bank connected components of the
+ * in-bank connectivity graph, and the union of connectivity masks over all vertices that
+ * share a coarse node.
+ *
+ * Parity status: the integer ordering inputs are pinned by the reference's
+ * Assets/sorted_mesh .part fixtures (tests/golden); the floating-point results of convert /
+ * SpMV / MAS / PCG are "parity unpinned" -- the reference needs Eigen 3.4, which is absent, so
+ * it cannot be built and run to produce golden outputs.
+ *
+ * Bank size is a run-time parameter (16 = CEMAS as shipped, 32 = Morton-ordered GPU MAS).
+ */
+#define _POSIX_C_SOURCE 199309L
+#include <math.h>
+#include <stdint.h>
+#include <time.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORC_MAX_LEVELS 6
+
+/* ------------------------------------------------------------------------------------ */
+/* 3x3 helpers; blocks are column-major (Eigen Matrix3d): element (i,j) at [j*3+i]       */
+/* ------------------------------------------------------------------------------------ */
+static inline double bget(const double* b, int i, int j) { return b[j * 3 + i]; }
+
+/* ------------------------------------------------------------------------------------ */
+/* srbk_convert: triplets -> sorted unique BCOO (converter.cu:88-238).                  */
+/* Key = (row << 32) + col, stable sort (cub radix sort keeps input order on ties),     */
+/* duplicates summed.  Returns the unique count.                                        */
+/* ------------------------------------------------------------------------------------ */
+typedef struct { uint64_t key; int idx; } orc_kv;
+
+static int kv_cmp(const void* a, const void* b)
+{
+    const orc_kv* x = (const orc_kv*)a;
+    const orc_kv* y = (const orc_kv*)b;
+    if(x->key < y->key) return -1;
+    if(x->key > y->key) return 1;
+    return (x->idx < y->idx) ? -1 : (x->idx > y->idx);
+}
+
+int orc_convert(int count, const int* rows, const int* cols, const double* blocks,
+                int* out_rows, int* out_cols, double* out_blocks)
+{
+    if(count < 1) return 0;
+    orc_kv* kv = (orc_kv*)malloc(sizeof(orc_kv) * (size_t)count);
+    for(int i = 0; i < count; i++)
+    {
+        kv[i].key = ((uint64_t)(uint32_t)rows[i] << 32) + (uint64_t)(uint32_t)cols[i];
+        kv[i].idx = i;
+    }
+    qsort(kv, (size_t)count, sizeof(orc_kv), kv_cmp);
+    int u = -1;
+    uint64_t prev = 0;
+    for(int i = 0; i < count; i++)
+    {
+        if(i == 0 || kv[i].key != prev)
+        {
+            u++;
+            out_rows[u] = (int)(kv[i].key >> 32);
+            out_cols[u] = (int)(kv[i].key & 0xffffffffu);
+            memcpy(out_blocks + 9 * (size_t)u, blocks + 9 * (size_t)kv[i].idx, 9 * sizeof(double));
+            prev = kv[i].key;
+        }
+        else
+        {
+            for(int e = 0; e < 9; e++) out_blocks[9 * (size_t)u + e] += blocks[9 * (size_t)kv[i].idx + e];
+        }
+    }
+    free(kv);
+    return u + 1;
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* srbk_spmv: y = a*A*x + b*y with A symmetric, stored as unique upper blocks           */
+/* (spmv.cu:188-313).  Diagonal block: H x_j.  Off-diagonal: H x_j into row i and       */
+/* H^T x_i into row j.                                                                  */
+/* ------------------------------------------------------------------------------------ */
+void orc_spmv(double a, int nnzb, const int* rows, const int* cols, const double* blocks,
+              const double* x, double b, double* y, int n)
+{
+    for(int i = 0; i < n; i++) y[i] = (b != 0.0) ? b * y[i] : 0.0;
+    for(int k = 0; k < nnzb; k++)
+    {
+        int i = rows[k], j = cols[k];
+        const double* H = blocks + 9 * (size_t)k;
+        for(int r = 0; r < 3; r++)
+        {
+            double s = 0;
+            for(int c = 0; c < 3; c++) s += bget(H, r, c) * x[3 * j + c];
+            y[3 * i + r] += a * s;
+        }
+        if(i != j)
+        {
+            for(int r = 0; r < 3; r++)
+            {
+                double s = 0;
+                for(int c = 0; c < 3; c++) s += bget(H, c, r) * x[3 * i + c];
+                y[3 * j + r] += a * s;
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* MAS                                                                                  */
+/* ------------------------------------------------------------------------------------ */
+typedef struct
+{
+    int bank;            /* BANKSIZE (16 or 32)                     */
+    int V;               /* totalNodes (FEM vertices)               */
+    int M;               /* totalMapNodes = part_offset * bank      */
+    int L;               /* levelnum                                */
+    int node_offset;     /* collision_node_Offset                   */
+    int nlist_size;
+    unsigned* nstart;    /* neighbour CSR (init copies)             */
+    unsigned* nnum_init;
+    unsigned* nlist_init;
+    unsigned* nnum;      /* working copies                          */
+    unsigned* nlist;
+    int* part_map;       /* partId_map_real [M]                     */
+    int* real_map;       /* real_map_partId [V]                     */
+    /* hierarchy */
+    unsigned* fine_mask;       /* [V]                */
+    unsigned* next_mask;       /* [V]                */
+    int* prefix_orig;          /* [M/bank]           */
+    int* prefix_sum_orig;      /* [M/bank]           */
+    unsigned* next_prefix;     /* [V]                */
+    unsigned* next_prefix_sum; /* [V]                */
+    int* coarse_tables;        /* [L*V]              */
+    int* going_next;           /* [L*V + M]          */
+    int* coarse_table;         /* [V*(L-1)] (itable) */
+    int level_size[2 * (ORC_MAX_LEVELS + 1)];
+    int total_clusters;
+    /* matrices */
+    int nbanks;                /* total_clusters / bank */
+    double* mat;               /* [nbanks * nsym * 9] FP64 packed upper (column-major 3x3) */
+    float* inv;                /* [nbanks * nsym * 9] FP32                                 */
+} orc_mas;
+
+static inline int nsym(int bank) { return bank * (bank + 1) / 2; }
+static inline int upper_index(int bank, int r, int c) { return bank * r - r * (r + 1) / 2 + c; }
+static inline unsigned lanemask_lt(int lane) { return (lane >= 32) ? 0xffffffffu : ((1u << lane) - 1u); }
+static inline int ffs32(unsigned m) { return m ? __builtin_ctz(m) + 1 : 0; }
+
+/* computeNumLevels (MASPreconditioner.cu:1731-1750) */
+int orc_mas_num_levels(int n, int bank)
+{
+    int nLevel = 1;
+    int levelSz = (n + bank - 1) / bank * bank;
+    while(levelSz > bank)
+    {
+        levelSz /= bank;
+        nLevel++;
+        levelSz = (levelSz + bank - 1) / bank * bank;
+    }
+    nLevel = nLevel + 1;
+    return nLevel > ORC_MAX_LEVELS ? ORC_MAX_LEVELS : nLevel;
+}
+
+void orc_mas_destroy(orc_mas* m)
+{
+    if(!m) return;
+    free(m->nstart); free(m->nnum_init); free(m->nlist_init); free(m->nnum); free(m->nlist);
+    free(m->part_map); free(m->real_map); free(m->fine_mask); free(m->next_mask);
+    free(m->prefix_orig); free(m->prefix_sum_orig); free(m->next_prefix); free(m->next_prefix_sum);
+    free(m->coarse_tables); free(m->going_next); free(m->coarse_table); free(m->mat); free(m->inv);
+    free(m);
+}
+
+/* initPreconditioner_Neighbor (MASPreconditioner.cu:2291-2328) + the uploads of
+ * sim_bootstrap.cpp:276-306 */
+orc_mas* orc_mas_create(int bank, int V, const unsigned* nstart, const unsigned* nnum,
+                        const unsigned* nlist, int nlist_size, const int* part_map, int M,
+                        const int* real_map, int node_offset)
+{
+    orc_mas* m = (orc_mas*)calloc(1, sizeof(orc_mas));
+    m->bank = bank; m->V = V; m->M = M; m->node_offset = node_offset; m->nlist_size = nlist_size;
+    m->L = orc_mas_num_levels(M > V ? M : V, bank);
+    m->nstart = (unsigned*)malloc(sizeof(unsigned) * V);
+    m->nnum_init = (unsigned*)malloc(sizeof(unsigned) * V);
+    m->nnum = (unsigned*)malloc(sizeof(unsigned) * V);
+    m->nlist_init = (unsigned*)malloc(sizeof(unsigned) * (nlist_size > 0 ? nlist_size : 1));
+    m->nlist = (unsigned*)malloc(sizeof(unsigned) * (nlist_size > 0 ? nlist_size : 1));
+    memcpy(m->nstart, nstart, sizeof(unsigned) * V);
+    memcpy(m->nnum_init, nnum, sizeof(unsigned) * V);
+    if(nlist_size > 0) memcpy(m->nlist_init, nlist, sizeof(unsigned) * nlist_size);
+    m->part_map = (int*)malloc(sizeof(int) * M);
+    m->real_map = (int*)malloc(sizeof(int) * V);
+    memcpy(m->part_map, part_map, sizeof(int) * M);
+    memcpy(m->real_map, real_map, sizeof(int) * V);
+    m->fine_mask = (unsigned*)calloc(V, sizeof(unsigned));
+    m->next_mask = (unsigned*)calloc(V, sizeof(unsigned));
+    int nb0 = M / bank + 1;
+    m->prefix_orig = (int*)calloc(nb0, sizeof(int));
+    m->prefix_sum_orig = (int*)calloc(nb0, sizeof(int));
+    m->next_prefix = (unsigned*)calloc(V + 1, sizeof(unsigned));
+    m->next_prefix_sum = (unsigned*)calloc(V + 1, sizeof(unsigned));
+    m->coarse_tables = (int*)calloc((size_t)m->L * V, sizeof(int));
+    m->going_next = (int*)calloc((size_t)m->L * V + M, sizeof(int));
+    m->coarse_table = (int*)calloc((size_t)V * (m->L > 1 ? m->L - 1 : 1), sizeof(int));
+    return m;
+}
+
+int orc_mas_levels(const orc_mas* m) { return m->L; }
+int orc_mas_total_clusters(const orc_mas* m) { return m->total_clusters; }
+
+/* Decode one sign-encoded collision pair (MASPreconditioner.cu:1141-1548) into up to four
+ * FEM-local vertex ids (-1 = absent or ABD).  Returns the vertex count. */
+static int decode_pair(const int* cp, int node_offset, int out[4])
+{
+    int v[4] = {cp[0], cp[1], cp[2], cp[3]};
+    int cnt = 4;
+    if(v[0] >= 0)
+    {
+        if(v[3] < 0) v[3] = -v[3] - 1;
+    }
+    else
+    {
+        v[0] = -v[0] - 1;
+        if(v[2] < 0)
+        {
+            if(v[1] < 0)
+            {
+                v[1] = -v[1] - 1; v[2] = -v[2] - 1; v[3] = -v[3] - 1;
+            }
+            else
+                cnt = 2;
+        }
+        else if(v[3] < 0)
+        {
+            if(v[1] < 0)
+            {
+                v[1] = -v[1] - 1; v[3] = -v[3] - 1;
+            }
+            else
+                cnt = 3;
+        }
+    }
+    for(int i = 0; i < 4; i++) out[i] = -1;
+    for(int i = 0; i < cnt; i++)
+    {
+        int id = v[i] - node_offset;
+        out[i] = id >= 0 ? id : -1;
+    }
+    return cnt;
+}
+
+/* _buildCollisionConnection_new for one level (level 0: coarse == NULL). */
+static void collision_connection(orc_mas* m, unsigned* conn, const int* coarse, const int* pairs, int ncp)
+{
+    const int B = m->bank;
+    for(int p = 0; p < ncp; p++)
+    {
+        int vid[4];
+        int cnt = decode_pair(pairs + 4 * p, m->node_offset, vid);
+        int cpv[4];
+        for(int i = 0; i < cnt; i++)
+            cpv[i] = vid[i] >= 0 ? (coarse ? coarse[vid[i]] : m->real_map[vid[i]]) : -1;
+        unsigned msk[4] = {0, 0, 0, 0};
+        for(int i = 0; i < cnt; i++)
+            for(int j = i + 1; j < cnt; j++)
+            {
+                int a = cpv[i], b = cpv[j];
+                if(a == b || a < 0 || b < 0) continue;
+                if(a / B == b / B)
+                {
+                    msk[i] |= 1u << (b % B);
+                    msk[j] |= 1u << (a % B);
+                }
+            }
+        for(int i = 0; i < cnt; i++)
+        {
+            if(coarse)
+            {
+                if(cpv[i] >= 0) conn[cpv[i]] |= msk[i];
+            }
+            else if(vid[i] >= 0)
+                conn[vid[i]] |= msk[i];
+        }
+    }
+}
+
+/* closure of the in-bank graph: visit lanes reachable from `lane` through the original
+ * masks `orig` of the bank (the loop of _preparePrefixSumL0_new / _nextLevelCluster) */
+static unsigned closure(const unsigned* orig, int lane, unsigned start)
+{
+    unsigned conn = start;
+    unsigned visited = 1u << lane;
+    for(;;)
+    {
+        unsigned todo = visited ^ conn;
+        if(!todo) break;
+        int nv = ffs32(todo) - 1;
+        visited |= 1u << nv;
+        conn |= orig[nv];
+    }
+    return conn;
+}
+
+/* ReorderRealtime (MASPreconditioner.cu:1785-1826) with intended (race-free) semantics. */
+int orc_mas_build(orc_mas* m, const int* pairs, int ncp)
+{
+    const int B = m->bank, V = m->V, M = m->M, L = m->L;
+    const int nb0 = M / B;
+    unsigned orig[32];
+    memcpy(m->nlist, m->nlist_init, sizeof(unsigned) * (m->nlist_size > 0 ? m->nlist_size : 0));
+    memcpy(m->nnum, m->nnum_init, sizeof(unsigned) * V);
+    memset(m->level_size, 0, sizeof(m->level_size));
+
+    /* BuildConnectMaskL0: _buildCML0_new (MASPreconditioner.cu:62-98) */
+    for(int s = 0; s < M; s++)
+    {
+        int v = m->part_map[s];
+        if(v < 0) continue;
+        int bank = s / B, lane = s % B;
+        unsigned msk = 1u << lane;
+        unsigned nk = 0, st = m->nstart[v], num = m->nnum[v];
+        for(unsigned i = 0; i < num; i++)
+        {
+            unsigned u = m->nlist[st + i];
+            int su = m->real_map[u];
+            if(su / B == bank)
+                msk |= 1u << (su % B);
+            else
+                m->nlist[st + nk++] = u;
+        }
+        m->nnum[v] = nk;
+        m->fine_mask[v] = msk;
+    }
+    if(ncp > 0) collision_connection(m, m->fine_mask, NULL, pairs, ncp);
+
+    /* PreparePrefixSumL0: _preparePrefixSumL0_new (MASPreconditioner.cu:159-214) */
+    for(int b = 0; b < nb0; b++)
+    {
+        for(int l = 0; l < B; l++)
+        {
+            int v = m->part_map[b * B + l];
+            orig[l] = v >= 0 ? m->fine_mask[v] : 0u;
+        }
+        int comps = 0;
+        for(int l = 0; l < B; l++)
+        {
+            int v = m->part_map[b * B + l];
+            if(v < 0) continue;
+            unsigned c = closure(orig, l, orig[l]);
+            m->fine_mask[v] = c;
+            if(__builtin_popcount(c & lanemask_lt(l)) == 0) comps++;
+        }
+        m->prefix_orig[b] = comps;
+    }
+
+    /* BuildLevel1: exclusive scan + _buildLevel1_new (MASPreconditioner.cu:270-328) */
+    {
+        int acc = 0;
+        for(int b = 0; b < nb0; b++) { m->prefix_sum_orig[b] = acc; acc += m->prefix_orig[b]; }
+        m->level_size[2 * 1 + 0] = acc;
+        m->level_size[2 * 1 + 1] = M;
+        for(int b = 0; b < nb0; b++)
+        {
+            unsigned elected = 0;
+            for(int l = 0; l < B; l++)
+            {
+                int v = m->part_map[b * B + l];
+                if(v < 0) continue;
+                if(__builtin_popcount(m->fine_mask[v] & lanemask_lt(l)) == 0) elected |= 1u << l;
+            }
+            for(int l = 0; l < B; l++)
+            {
+                int v = m->part_map[b * B + l];
+                if(v < 0) continue;
+                int lead = ffs32(m->fine_mask[v]) - 1;
+                int id = __builtin_popcount(elected & lanemask_lt(lead)) + m->prefix_sum_orig[b];
+                m->coarse_tables[v] = id;
+                m->going_next[v] = id + M;
+            }
+        }
+    }
+
+    for(int level = 1; level < L; level++)
+    {
+        memset(m->next_mask, 0, sizeof(unsigned) * V);
+        const int* prev = m->coarse_tables + (size_t)(level - 1) * V;
+        /* _buildConnectMaskLx_new (MASPreconditioner.cu:401-470), union semantics */
+        for(int s = 0; s < M; s++)
+        {
+            int v = m->part_map[s];
+            if(v < 0) continue;
+            unsigned c = (unsigned)prev[v];
+            unsigned msk = 0, nk = 0, st = m->nstart[v], num = m->nnum[v];
+            for(unsigned i = 0; i < num; i++)
+            {
+                unsigned u = m->nlist[st + i];
+                unsigned cu = (unsigned)prev[u];
+                if(c / B == cu / B)
+                    msk |= 1u << (cu % B);
+                else
+                    m->nlist[st + nk++] = u;
+            }
+            m->nnum[v] = nk;
+            m->next_mask[c] |= msk;
+        }
+        if(ncp > 0) collision_connection(m, m->next_mask, prev, pairs, ncp);
+
+        int number = m->level_size[2 * level + 0];
+        int level_begin = m->level_size[2 * level + 1];
+        int nb = (number + B - 1) / B;
+        /* _nextLevelCluster (MASPreconditioner.cu:473-520) */
+        for(int b = 0; b < nb; b++)
+        {
+            int cnt = (b == nb - 1) ? number - b * B : B;
+            for(int l = 0; l < B; l++) orig[l] = (l < cnt) ? ((1u << l) | m->next_mask[b * B + l]) : 0u;
+            int comps = 0;
+            for(int l = 0; l < cnt; l++)
+            {
+                unsigned c = closure(orig, l, orig[l]);
+                m->next_mask[b * B + l] = c;
+                if(__builtin_popcount(c & lanemask_lt(l)) == 0) comps++;
+            }
+            m->next_prefix[b] = (unsigned)comps;
+        }
+        /* exclusive scan + _prefixSumLx (MASPreconditioner.cu:522-566) */
+        unsigned acc = 0;
+        for(int b = 0; b < nb; b++) { m->next_prefix_sum[b] = acc; acc += m->next_prefix[b]; }
+        int rounded = (number + B - 1) / B * B;
+        m->level_size[2 * (level + 1) + 0] = (int)acc;
+        m->level_size[2 * (level + 1) + 1] = level_begin + rounded;
+        for(int b = 0; b < nb; b++)
+        {
+            int cnt = (b == nb - 1) ? number - b * B : B;
+            unsigned elected = 0;
+            for(int l = 0; l < cnt; l++)
+                if(__builtin_popcount(m->next_mask[b * B + l] & lanemask_lt(l)) == 0) elected |= 1u << l;
+            int ids[32];
+            for(int l = 0; l < cnt; l++)
+            {
+                int lead = ffs32(m->next_mask[b * B + l]) - 1;
+                ids[l] = __builtin_popcount(elected & lanemask_lt(lead)) + (int)m->next_prefix_sum[b];
+            }
+            for(int l = 0; l < cnt; l++)
+            {
+                m->next_mask[b * B + l] = (unsigned)ids[l];
+                m->going_next[b * B + l + level_begin] = ids[l] + level_begin + rounded;
+            }
+        }
+        /* _computeNextLevel (MASPreconditioner.cu:568-579) */
+        int* cur = m->coarse_tables + (size_t)level * V;
+        for(int v = 0; v < V; v++) cur[v] = (int)m->next_mask[prev[v]];
+    }
+    m->total_clusters = m->level_size[2 * L + 1];
+
+    /* _aggregationKernel (MASPreconditioner.cu:581-608) */
+    for(int v = 0; v < V; v++)
+    {
+        int cur = v;
+        for(int l = 0; l < L - 1; l++)
+        {
+            cur = m->going_next[cur];
+            m->coarse_table[(size_t)v * (L - 1) + l] = cur;
+        }
+    }
+    return m->total_clusters;
+}
+
+/* Copies of the hierarchy for bit-exact comparisons.  Any pointer may be NULL. */
+void orc_mas_export(const orc_mas* m, unsigned* fine_mask, int* prefix_orig, int* coarse_tables,
+                    int* going_next, int* coarse_table, int* level_size, unsigned* nlist, unsigned* nnum)
+{
+    const int V = m->V, L = m->L;
+    if(fine_mask) memcpy(fine_mask, m->fine_mask, sizeof(unsigned) * V);
+    if(prefix_orig) memcpy(prefix_orig, m->prefix_orig, sizeof(int) * (m->M / m->bank));
+    if(coarse_tables) memcpy(coarse_tables, m->coarse_tables, sizeof(int) * (size_t)L * V);
+    if(going_next)
+    {
+        /* entries [0, V) for vertices and [M, total) for coarse nodes */
+        memcpy(going_next, m->going_next, sizeof(int) * (size_t)((m->total_clusters > V) ? m->total_clusters : V));
+    }
+    if(coarse_table) memcpy(coarse_table, m->coarse_table, sizeof(int) * (size_t)V * (L > 1 ? L - 1 : 1));
+    if(level_size) memcpy(level_size, m->level_size, sizeof(int) * 2 * (L + 1));
+    if(nlist) memcpy(nlist, m->nlist, sizeof(unsigned) * m->nlist_size);
+    if(nnum) memcpy(nnum, m->nnum, sizeof(unsigned) * V);
+}
+
+/* calculate_subsystem_bcoo_indices (i_preconditioner.cu:32-73): entries whose row and col
+ * both lie in [offset, end), in BCOO order. */
+int orc_select_range(int nnzb, const int* rows, const int* cols, int offset, int end, int* out)
+{
+    int c = 0;
+    for(int k = 0; k < nnzb; k++)
+        if(rows[k] >= offset && rows[k] < end && cols[k] >= offset && cols[k] < end) out[c++] = k;
+    return c;
+}
+
+static inline double* mblk(orc_mas* m, int gid_bank, int idx) { return m->mat + ((size_t)gid_bank * nsym(m->bank) + idx) * 9; }
+
+/* In-place Gauss-Jordan inverse of one bank (__inverse6_P96x96, MASPreconditioner.cu:630-726). */
+static void invert_bank(orc_mas* m, int bk, double* A, double* colm)
+{
+    const int B = m->bank, N = 3 * B;
+    for(int j = 0; j < N; j++)
+        for(int i = 0; i < N; i++)
+        {
+            int rowId = j / 3, colId = i / 3;
+            double v;
+            if(colId >= rowId)
+                v = bget(mblk(m, bk, upper_index(B, rowId, colId)), j % 3, i % 3);
+            else
+                v = bget(mblk(m, bk, upper_index(B, colId, rowId)), i % 3, j % 3);
+            if(i == j && v == 0.0) v = 1.0;
+            A[(size_t)j * N + i] = v;
+        }
+    for(int j = 0; j < N; j++)
+    {
+        double rt = A[(size_t)j * N + j];
+        for(int i = 0; i < N; i++) colm[i] = A[(size_t)i * N + j];
+        for(int i = 0; i < N; i++) A[(size_t)i * N + j] = (i == j) ? 1.0 : 0.0;
+        for(int i = 0; i < N; i++) A[(size_t)j * N + i] /= rt;
+        for(int k = 0; k < N; k++)
+        {
+            if(k == j) continue;
+            double rate = -colm[k];
+            for(int i = 0; i < N; i++) A[(size_t)k * N + i] = fma(rate, A[(size_t)j * N + i], A[(size_t)k * N + i]);
+        }
+    }
+    for(int i = 0; i < N; i++)
+    {
+        if(i % 3 < 2)
+            A[(size_t)(i + 1) * N + i] = A[(size_t)i * N + i + 1];
+        else
+            A[(size_t)i * N + i - 2] = A[(size_t)(i - 2) * N + i];
+    }
+    float* P = m->inv + (size_t)bk * nsym(B) * 9;
+    for(int j = 0; j < N; j++)
+        for(int i = 0; i < N; i++)
+        {
+            int rowId = j / 3, colId = i / 3;
+            if(colId >= rowId)
+                P[(size_t)upper_index(B, rowId, colId) * 9 + (i % 3) * 3 + (j % 3)] = (float)A[(size_t)j * N + i];
+        }
+}
+
+/* setPreconditioner_bcoo after ReorderRealtime: PrepareHessian_bcoo + inverse
+ * (MASPreconditioner.cu:1829-2075, 2207-2245).  `sel` lists the BCOO entries of the FEM
+ * range (orc_select_range); `offset` is the FEM block offset. */
+void orc_mas_assemble(orc_mas* m, const int* rows, const int* cols, const double* blocks,
+                      const int* sel, int nsel, int offset)
+{
+    const int B = m->bank, L = m->L, NS = nsym(B);
+    m->nbanks = m->total_clusters / B;
+    free(m->mat); free(m->inv);
+    m->mat = (double*)calloc((size_t)m->nbanks * NS * 9, sizeof(double));
+    m->inv = (float*)calloc((size_t)m->nbanks * NS * 9, sizeof(float));
+
+    /* lambda 1 (MASPreconditioner.cu:1849-1944) */
+    for(int I = 0; I < nsel; I++)
+    {
+        int k = sel[I];
+        const double* H = blocks + 9 * (size_t)k;
+        int rr = rows[k] - offset, cc = cols[k] - offset;
+        int sc = m->real_map[cc], sr = m->real_map[rr];
+        if(sc / B == sr / B)
+        {
+            if(sc >= sr) memcpy(mblk(m, sc / B, upper_index(B, sr % B, sc % B)), H, 9 * sizeof(double));
+            continue;
+        }
+        int gc = cc, gr = rr;
+        for(int level = 1; level < L; level++)
+        {
+            gc = m->going_next[gc];
+            gr = m->going_next[gr];
+            if(gc / B != gr / B) continue;
+            if(gc >= gr)
+            {
+                double* D = mblk(m, gc / B, upper_index(B, gr % B, gc % B));
+                for(int i = 0; i < 3; i++)
+                    for(int j = 0; j < 3; j++)
+                    {
+                        D[j * 3 + i] += bget(H, i, j);
+                        if(gc == gr) D[j * 3 + i] += bget(H, j, i);
+                    }
+            }
+            else
+            {
+                double* D = mblk(m, gc / B, upper_index(B, gc % B, gr % B));
+                for(int i = 0; i < 3; i++)
+                    for(int j = 0; j < 3; j++) D[j * 3 + i] += bget(H, j, i);
+            }
+        }
+    }
+
+    /* lambda 2 (MASPreconditioner.cu:1946-2075) */
+    const int nb0 = m->M / B;
+    for(int b = 0; b < nb0; b++)
+    {
+        double S[9] = {0};
+        int any = -1;
+        for(int LR = 0; LR < B; LR++)
+            for(int LC = 0; LC < B; LC++)
+            {
+                int rdx = m->part_map[b * B + LR], cdx = m->part_map[b * B + LC];
+                if(rdx < 0 || cdx < 0) continue;
+                double mat3[9];
+                if(LC >= LR)
+                    memcpy(mat3, mblk(m, b, upper_index(B, LR, LC)), sizeof(mat3));
+                else
+                {
+                    const double* src = mblk(m, b, upper_index(B, LC, LR));
+                    for(int i = 0; i < 3; i++)
+                        for(int j = 0; j < 3; j++) mat3[j * 3 + i] = src[i * 3 + j];
+                }
+                if(m->prefix_orig[b] == 1)
+                {
+                    for(int e = 0; e < 9; e++) S[e] += mat3[e];
+                    any = rdx;
+                }
+                else
+                {
+                    for(int level = 1; level < L; level++)
+                    {
+                        rdx = m->going_next[rdx];
+                        cdx = m->going_next[cdx];
+                        if(rdx / B == cdx / B && cdx >= rdx)
+                        {
+                            double* D = mblk(m, cdx / B, upper_index(B, rdx % B, cdx % B));
+                            for(int e = 0; e < 9; e++) D[e] += mat3[e];
+                        }
+                    }
+                }
+            }
+        if(m->prefix_orig[b] == 1 && any >= 0)
+        {
+            int nid = m->going_next[any];
+            for(int level = 1; level < L; level++)
+            {
+                double* D = mblk(m, nid / B, upper_index(B, nid % B, nid % B));
+                for(int e = 0; e < 9; e++) D[e] += S[e];
+                nid = m->going_next[nid];
+            }
+        }
+    }
+
+    /* __inverse6_P96x96 over every bank of every level */
+    {
+        const int N = 3 * B;
+        double* A = (double*)malloc(sizeof(double) * N * N);
+        double* colm = (double*)malloc(sizeof(double) * N);
+        for(int bk = 0; bk < m->nbanks; bk++) invert_bank(m, bk, A, colm);
+        free(A); free(colm);
+    }
+}
+
+int orc_mas_nbanks(const orc_mas* m) { return m->nbanks; }
+
+void orc_mas_export_matrices(const orc_mas* m, double* mat, float* inv)
+{
+    size_t cnt = (size_t)m->nbanks * nsym(m->bank) * 9;
+    if(mat) memcpy(mat, m->mat, cnt * sizeof(double));
+    if(inv) memcpy(inv, m->inv, cnt * sizeof(float));
+}
+
+/* preconditioning (MASPreconditioner.cu:2248-2289): restrict (729-847), local solves
+ * (957-1027), prolong (850-879).  r, z: FEM sub-range, 3V doubles. */
+void orc_mas_apply(const orc_mas* m, const double* r, double* z)
+{
+    const int B = m->bank, V = m->V, M = m->M, L = m->L, T = m->total_clusters;
+    float* R = (float*)calloc((size_t)T * 3, sizeof(float));
+    float* Zc = (float*)calloc((size_t)T * 3, sizeof(float));
+    for(int s = 0; s < M; s++)
+    {
+        int v = m->part_map[s];
+        if(v < 0) continue;
+        float rv[3] = {(float)r[3 * v], (float)r[3 * v + 1], (float)r[3 * v + 2]};
+        for(int c = 0; c < 3; c++) R[3 * s + c] = rv[c];
+        int id = v;
+        for(int level = 1; level < L; level++)
+        {
+            id = m->going_next[id];
+            for(int c = 0; c < 3; c++) R[3 * (size_t)id + c] += rv[c];
+        }
+    }
+    const int NS = nsym(B);
+    for(int bk = 0; bk < T / B; bk++)
+    {
+        const float* P = m->inv + (size_t)bk * NS * 9;
+        for(int a = 0; a < B; a++)
+        {
+            float acc[3] = {0, 0, 0};
+            for(int c = 0; c < B; c++)
+            {
+                const float* rc = R + 3 * ((size_t)bk * B + c);
+                if(c >= a)
+                {
+                    const float* Pb = P + (size_t)upper_index(B, a, c) * 9;
+                    for(int i = 0; i < 3; i++)
+                        acc[i] += Pb[0 * 3 + i] * rc[0] + Pb[1 * 3 + i] * rc[1] + Pb[2 * 3 + i] * rc[2];
+                }
+                else
+                {
+                    const float* Pb = P + (size_t)upper_index(B, c, a) * 9;
+                    for(int i = 0; i < 3; i++)
+                        acc[i] += Pb[i * 3 + 0] * rc[0] + Pb[i * 3 + 1] * rc[1] + Pb[i * 3 + 2] * rc[2];
+                }
+            }
+            for(int i = 0; i < 3; i++) Zc[3 * ((size_t)bk * B + a) + i] = acc[i];
+        }
+    }
+    for(int v = 0; v < V; v++)
+    {
+        int s = m->real_map[v];
+        float cz[3] = {Zc[3 * (size_t)s], Zc[3 * (size_t)s + 1], Zc[3 * (size_t)s + 2]};
+        for(int l = 1; l < L; l++)
+        {
+            int now = m->coarse_table[(size_t)v * (L - 1) + l - 1];
+            for(int c = 0; c < 3; c++) cz[c] += Zc[3 * (size_t)now + c];
+        }
+        for(int c = 0; c < 3; c++) z[3 * v + c] = (double)cz[c];
+    }
+    free(R); free(Zc);
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* Preconditioner composition + PCG                                                      */
+/* ------------------------------------------------------------------------------------ */
+typedef struct
+{
+    int iterations;
+    double rz0, rz_final;
+    double rel_residual;      /* ||b - A x|| / ||b||, FP64 */
+} orc_pcg_stats;
+
+/* 3x3 inverse of a column-major block (cofactor / determinant) */
+static void inv3(const double* H, double* D)
+{
+    double a = bget(H, 0, 0), b = bget(H, 0, 1), c = bget(H, 0, 2);
+    double d = bget(H, 1, 0), e = bget(H, 1, 1), f = bget(H, 1, 2);
+    double g = bget(H, 2, 0), h = bget(H, 2, 1), i = bget(H, 2, 2);
+    double A = e * i - f * h, Bc = -(d * i - f * g), C = d * h - e * g;
+    double det = a * A + b * Bc + c * C;
+    double inv_det = 1.0 / det;
+    double R[9] = {A, -(b * i - c * h), b * f - c * e, Bc, a * i - c * g, -(a * f - c * d), C, -(a * h - b * g), a * e - b * d};
+    /* R row-major adjugate */
+    for(int r = 0; r < 3; r++)
+        for(int col = 0; col < 3; col++) D[col * 3 + r] = R[r * 3 + col] * inv_det;
+}
+
+typedef struct
+{
+    int nnzb;
+    const int* rows;
+    const int* cols;
+    const double* blocks;
+    int n;
+    /* global block-Jacobi (DiagPreconditioner) when nonzero */
+    int use_diag;
+    double* diag_inv;          /* [n/3 * 9] */
+    /* ABD 12x12 block-Jacobi over the first abd_bodies*12 dofs */
+    int abd_bodies;
+    const double* abd_inv;     /* [bodies * 144] row-major */
+    /* MAS over [fem_offset, fem_offset + V) blocks */
+    const orc_mas* mas;
+    int fem_offset;
+} orc_system;
+
+static void apply_preconditioner(const orc_system* s, const double* r, double* z)
+{
+    /* GlobalLinearSystem::apply_preconditioner (global_linear_system.cu:167-180) */
+    if(s->use_diag)
+    {
+        for(int bi = 0; bi < s->n / 3; bi++)
+        {
+            const double* D = s->diag_inv + 9 * (size_t)bi;
+            for(int rr = 0; rr < 3; rr++)
+                z[3 * bi + rr] = bget(D, rr, 0) * r[3 * bi] + bget(D, rr, 1) * r[3 * bi + 1] + bget(D, rr, 2) * r[3 * bi + 2];
+        }
+    }
+    else
+        memcpy(z, r, sizeof(double) * s->n);
+    for(int body = 0; body < s->abd_bodies; body++)
+    {
+        const double* J = s->abd_inv + 144 * (size_t)body;
+        for(int rr = 0; rr < 12; rr++)
+        {
+            double acc = 0;
+            for(int c = 0; c < 12; c++) acc += J[rr * 12 + c] * r[12 * body + c];
+            z[12 * body + rr] = acc;
+        }
+    }
+    if(s->mas) orc_mas_apply(s->mas, r + 3 * s->fem_offset, z + 3 * s->fem_offset);
+}
+
+static double dot(const double* a, const double* b, int n)
+{
+    double s = 0;
+    for(int i = 0; i < n; i++) s += a[i] * b[i];
+    return s;
+}
+
+static double now_s(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+/* PCGSolver::solve + pcg (pcg_solver.cu:158-332).  max_iter = (SizeT)(ratio * n).
+ * stop_rule 0: |r.z| <= tol * r0.z0 (the reference); 1: ||r||/||b|| <= tol.
+ * budget_s > 0 bounds the iteration loop in wall time (CPU baseline sampling); *t_iter gets
+ * the mean seconds per iteration and *done whether the stop rule (or max_iter) ended it. */
+int orc_pcg_ex(const int* rows, const int* cols, const double* blocks, int nnzb, int n,
+               const double* b, double* x, const orc_mas* mas, int fem_offset, int use_diag,
+               int abd_bodies, const double* abd_inv, double tol, double max_iter_ratio,
+               int stop_rule, double budget_s, orc_pcg_stats* st, double* t_iter, int* done);
+
+int orc_pcg(const int* rows, const int* cols, const double* blocks, int nnzb, int n,
+            const double* b, double* x, const orc_mas* mas, int fem_offset, int use_diag,
+            int abd_bodies, const double* abd_inv, double tol, double max_iter_ratio,
+            orc_pcg_stats* st)
+{
+    return orc_pcg_ex(rows, cols, blocks, nnzb, n, b, x, mas, fem_offset, use_diag, abd_bodies, abd_inv, tol,
+                      max_iter_ratio, 0, 0.0, st, NULL, NULL);
+}
+
+int orc_pcg_ex(const int* rows, const int* cols, const double* blocks, int nnzb, int n,
+               const double* b, double* x, const orc_mas* mas, int fem_offset, int use_diag,
+               int abd_bodies, const double* abd_inv, double tol, double max_iter_ratio,
+               int stop_rule, double budget_s, orc_pcg_stats* st, double* t_iter, int* done)
+{
+    orc_system s = {nnzb, rows, cols, blocks, n, use_diag, NULL, abd_bodies, abd_inv, mas, fem_offset};
+    if(use_diag)
+    {
+        s.diag_inv = (double*)calloc((size_t)n / 3 * 9, sizeof(double));
+        for(int k = 0; k < nnzb; k++)
+            if(rows[k] == cols[k]) inv3(blocks + 9 * (size_t)k, s.diag_inv + 9 * (size_t)rows[k]);
+    }
+    double* r = (double*)malloc(sizeof(double) * n);
+    double* z = (double*)malloc(sizeof(double) * n);
+    double* p = (double*)malloc(sizeof(double) * n);
+    double* Ap = (double*)malloc(sizeof(double) * n);
+    long max_iter = (long)(max_iter_ratio * (double)n);
+    for(int i = 0; i < n; i++) { x[i] = 0; r[i] = b[i]; }
+    apply_preconditioner(&s, r, z);
+    double rz = dot(r, z, n);
+    memcpy(p, z, sizeof(double) * n);
+    double rz0 = rz;
+    const double bb = dot(b, b, n);
+    long k;
+    int finished = 0;
+    double t0 = now_s();
+    long counted = 0;
+    for(k = 1; k < max_iter; ++k)
+    {
+        orc_spmv(1.0, nnzb, rows, cols, blocks, p, 0.0, Ap, n);
+        double alpha = rz / dot(p, Ap, n);
+        for(int i = 0; i < n; i++) { x[i] += alpha * p[i]; r[i] -= alpha * Ap[i]; }
+        counted = k;
+        if(stop_rule == 0 ? (fabs(rz) <= tol * rz0) : (dot(r, r, n) <= tol * tol * bb))
+        {
+            finished = 1;
+            break;
+        }
+        if(budget_s > 0 && now_s() - t0 > budget_s) break;
+        apply_preconditioner(&s, r, z);
+        double rz_new = dot(r, z, n);
+        double beta = rz_new / rz;
+        for(int i = 0; i < n; i++) p[i] = z[i] + beta * p[i];
+        rz = rz_new;
+    }
+    if(k >= max_iter) finished = 1;
+    if(t_iter) *t_iter = counted > 0 ? (now_s() - t0) / (double)counted : 0.0;
+    if(done) *done = finished;
+    if(st)
+    {
+        st->iterations = (int)k;
+        st->rz0 = rz0;
+        st->rz_final = rz;
+        orc_spmv(1.0, nnzb, rows, cols, blocks, x, 0.0, Ap, n);
+        double nr = 0, nb = 0;
+        for(int i = 0; i < n; i++) { double d = b[i] - Ap[i]; nr += d * d; nb += b[i] * b[i]; }
+        st->rel_residual = nb > 0 ? sqrt(nr / nb) : 0.0;
+    }
+    free(r); free(z); free(p); free(Ap); free(s.diag_inv);
+    return (int)k;
+}

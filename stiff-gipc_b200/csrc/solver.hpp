@@ -1,0 +1,133 @@
+// solver.hpp -- internal state of one libstgipc handle.
+//
+// A handle mirrors the reference's GlobalLinearSystem (global_linear_system.h:15-113)
+// holding one IterativeSolver (PCGSolver, pcg_solver.h:19-52), the MAS preconditioner
+// (MASPreconditioner.cuh) and the converted BCOO, all on one CUDA stream.
+#pragma once
+#include "common.cuh"
+#include "../../include/stgipc.h"
+
+#include <algorithm>
+
+namespace stg
+{
+
+constexpr int kMaxLevels = 6;
+constexpr int kSMs = 148;
+
+// Sorted unique upper BCOO plus the derived row / transpose structure the SpMV uses.
+struct Bcoo
+{
+    int nnzb = 0;
+    int nrows = 0;
+    bool external = false;       // blocks/rows/cols point at caller memory
+    bool row_ptr_valid = false;
+    const double* ext_blocks = nullptr;
+    const int* ext_rows = nullptr;
+    const int* ext_cols = nullptr;
+    DBuf<int> rows, cols;        // owned copies (converter output)
+    DBuf<double> blocks;
+    DBuf<int> row_ptr;           // [nrows+1]
+    // transpose references: for block row i, the strictly-upper blocks k with col(k) == i,
+    // stored as (k, row(k)) pairs sorted by k
+    DBuf<int> t_ptr;             // [nrows+1]
+    DBuf<int> t_cnt;             // [nrows+1]
+    DBuf<int2> t_ent;            // [offdiag]
+    DBuf<float> blocks32;        // FP32 copy (FP32 mode)
+    DBuf<double> diag_inv;       // 3x3 block-Jacobi inverses [nrows*9]
+    int offdiag = 0;
+
+    const double* B() const { return external ? ext_blocks : blocks.data(); }
+    const int* R() const { return external ? ext_rows : rows.data(); }
+    const int* C() const { return external ? ext_cols : cols.data(); }
+};
+
+struct ConvertScratch
+{
+    DBuf<int> row_cnt, row_start, cursor, perm, perm2, scol, uniq, scratch;
+};
+
+struct MasState
+{
+    bool inited = false, built = false, assembled = false;
+    int bank = 16, V = 0, M = 0, L = 0, node_offset = 0, nlist_size = 0;
+    int total_clusters = 0, nbanks = 0, nb0 = 0;
+    int level_size[2 * (kMaxLevels + 1)] = {};
+    int gn_size = 0;
+    DBuf<unsigned> nstart, nnum_init, nlist_init, nnum, nlist;
+    DBuf<int> part_map, real_map;
+    DBuf<unsigned> fine_mask, next_mask;
+    DBuf<unsigned> closed;        // closed masks of coarse nodes, by global id
+    DBuf<int> prefix_orig, prefix_sum_orig;
+    DBuf<int> next_prefix, next_prefix_sum;
+    DBuf<int> coarse_tables;      // [L*V]
+    DBuf<int> going_next;         // [L*V + M]
+    DBuf<int> coarse_table;       // [V*(L-1)]
+    DBuf<int2> level_size_d;      // [kMaxLevels+1]
+    DBuf<int> scratch;
+    DBuf<double> mat;             // [nbanks * NS * 9]
+    DBuf<float> inv;              // [nbanks * NS * 9]
+    DBuf<float> R, Z;             // [total_clusters * 3]
+};
+
+struct PcgState
+{
+    DBuf<double> r, z, p, q, x64;  // FP64 vectors
+    DBuf<float> p32, q32, z32;     // FP32 vectors (FP32 mode)
+    DBuf<double> partials;         // per-block partial sums
+    DBuf<double> scal;             // device scalars, see enum below
+    DBuf<unsigned> counters;       // last-block counters
+    DBuf<int> flags;               // [0] done, [1] status
+    int partial_slots = 0;
+    cudaGraphExec_t graph = nullptr;
+    long long graph_key[8] = {};
+};
+
+// device scalar slots
+enum : int
+{
+    S_RZ = 0,      // current r.z
+    S_RZ0 = 1,     // r0.z0
+    S_PQ = 2,      // p.Aq
+    S_ALPHA = 3,
+    S_BETA = 4,
+    S_RZNEW = 5,
+    S_RR = 6,      // r.r
+    S_BB = 7,      // b.b
+    S_TOL = 8,     // stop threshold
+    S_ITER = 9,    // completed iterations (as double)
+    S_COUNT = 16
+};
+
+struct Solver
+{
+    stg_config cfg{};
+    cudaStream_t stream = nullptr;
+    int launches = 0;
+    Bcoo bcoo;
+    ConvertScratch cv;
+    MasState mas;
+    PcgState pcg;
+    cudaEvent_t ev[6] = {};
+    bool events = false;
+    int mas_fem_offset = 0;       // FEM block offset of the last MAS assembly
+    long long generation = 0;     // bumped by every (re)assembly; keys the captured graph
+    bool graph_dirty = true;
+    int launches_per_batch = 0;
+
+    ~Solver();
+
+    // stages
+    int convert(int count, const int* rows, const int* cols, const double* blocks, int nrows_hint);
+    int bind_bcoo(const double* blocks, const int* rows, const int* cols, int nnzb, int nrows);
+    int prepare_spmv();   // row_ptr, transpose refs, FP32 copy, diag inverses
+    int spmv(double a, const double* x, double b, double* y);
+    int mas_init(int V, int node_offset, const uint32_t* ns, const uint32_t* nn, const uint32_t* nl, int nls,
+                 const int* pm, int pms, const int* rm);
+    int mas_build(const int* contacts, int ncp);
+    int mas_assemble(int fem_block_offset);
+    int mas_apply(const double* r, double* z);
+    int pcg_solve(const double* b, double* x, int n, int abd_bodies, const double* abd_inv, stg_stats* st);
+};
+
+}  // namespace stg

@@ -1,0 +1,206 @@
+// spmv.cu -- symmetric 3x3-block BCOO SpMV on sm_100a.
+//
+// Replaces Spmv::srbk_spmv (StiffGIPC/linear_system/utils/spmv.cu:188-313).  The reference
+// runs one thread per stored upper block, reduces row segments with cub's warp
+// HeadSegmentedReduce and scatters both the row result and the transposed contribution
+// H^T x_i with FP64 atomicAdd (two atomics per off-diagonal block; summation order depends
+// on scheduling).
+//
+// Here each block row i is owned by a group of LPR lanes ("owner computes"):
+//   y_i = sum_{k in row i} H_k x_{col k}  +  sum_{k: col k == i, row k < i} H_k^T x_{row k}
+// The first list is the contiguous upper segment of the sorted BCOO; the second is a
+// transpose reference list built once per assembly (prepare_spmv).  No atomics, fixed
+// summation order, bitwise deterministic.  A transposed block is read a second time by a
+// nearby row (Morton-ordered vertices keep it in the 126 MB L2), so DRAM sees each block
+// about once.
+#include "solver.hpp"
+#include "spmv_core.cuh"
+
+namespace stg
+{
+
+// ---------------------------------------------------------------------------------------
+// structure preparation
+// ---------------------------------------------------------------------------------------
+__global__ void k_row_ptr(const int* rows, int nnzb, int nrows, int* row_ptr)
+{
+    for(int k = blockIdx.x * blockDim.x + threadIdx.x; k <= nnzb; k += gridDim.x * blockDim.x)
+    {
+        int rp = k > 0 ? rows[k - 1] : -1;
+        int rc = k < nnzb ? rows[k] : nrows;
+        for(int r = rp + 1; r <= rc; r++) row_ptr[r] = k;
+    }
+}
+
+__global__ void k_t_count(const int* rows, const int* cols, int nnzb, int* t_cnt)
+{
+    for(int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnzb; k += gridDim.x * blockDim.x)
+    {
+        int i = rows[k], j = cols[k];
+        if(i != j) atomicAdd(t_cnt + j, 1);
+    }
+}
+
+__global__ void k_t_fill(const int* rows, const int* cols, int nnzb, const int* t_ptr, int* cursor, int2* t_ent)
+{
+    for(int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnzb; k += gridDim.x * blockDim.x)
+    {
+        int i = rows[k], j = cols[k];
+        if(i != j)
+        {
+            int pos = t_ptr[j] + atomicAdd(cursor + j, 1);
+            t_ent[pos] = make_int2(k, i);
+        }
+    }
+}
+
+// sort each transpose list by block index (insertion sort; lists are short) so that the
+// summation order does not depend on atomic arrival order
+__global__ void k_t_sort(const int* t_ptr, int2* t_ent, int nrows)
+{
+    for(int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x)
+    {
+        int s = t_ptr[r], e = t_ptr[r + 1];
+        for(int a = s + 1; a < e; a++)
+        {
+            int2 v = t_ent[a];
+            int b = a - 1;
+            while(b >= s && t_ent[b].x > v.x)
+            {
+                t_ent[b + 1] = t_ent[b];
+                b--;
+            }
+            t_ent[b + 1] = v;
+        }
+    }
+}
+
+__global__ void k_to_f32(const double* in, float* out, size_t count)
+{
+    for(size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
+}
+
+// 3x3 inverse of every diagonal block (DiagPreconditioner::assemble,
+// diag_preconditioner.cu:12-33), cofactor / determinant, column-major in and out
+__global__ void k_diag_inv(const int* rows, const int* cols, const double* blocks, int nnzb, double* diag_inv)
+{
+    for(int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnzb; k += gridDim.x * blockDim.x)
+    {
+        if(rows[k] != cols[k]) continue;
+        const double* H = blocks + 9 * (size_t)k;
+        double a = H[0], b = H[3], c = H[6], d = H[1], e = H[4], f = H[7], g = H[2], h = H[5], i = H[8];
+        double A = e * i - f * h, Bc = -(d * i - f * g), Cc = d * h - e * g;
+        double inv_det = 1.0 / (a * A + b * Bc + c * Cc);
+        double R[9] = {A, -(b * i - c * h), b * f - c * e, Bc, a * i - c * g, -(a * f - c * d), Cc, -(a * h - b * g), a * e - b * d};
+        double* D = diag_inv + 9 * (size_t)rows[k];
+#pragma unroll
+        for(int r = 0; r < 3; r++)
+#pragma unroll
+            for(int cc = 0; cc < 3; cc++) D[cc * 3 + r] = R[r * 3 + cc] * inv_det;
+    }
+}
+
+int Solver::bind_bcoo(const double* blocks, const int* rows, const int* cols, int nnzb, int nrows)
+{
+    bcoo.external = true;
+    bcoo.ext_blocks = blocks;
+    bcoo.ext_rows = rows;
+    bcoo.ext_cols = cols;
+    bcoo.nnzb = nnzb;
+    bcoo.nrows = nrows;
+    bcoo.row_ptr_valid = false;
+    return 0;
+}
+
+int Solver::prepare_spmv()
+{
+    cudaStream_t s = stream;
+    const int nnzb = bcoo.nnzb, nrows = bcoo.nrows;
+    if(nrows < 1) return 0;
+    STG_TRY(bcoo.row_ptr.resize(nrows + 1));
+    STG_TRY(bcoo.t_ptr.resize(nrows + 1));
+    STG_TRY(bcoo.t_cnt.resize(nrows + 1));
+    STG_TRY(bcoo.t_ent.resize(std::max(nnzb, 1)));
+    STG_TRY(cv.scratch.resize(4));
+    const int g = std::max(1, std::min(div_up(nnzb + 1, 256), kSMs * 16));
+    if(!bcoo.row_ptr_valid)
+    {
+        k_row_ptr<<<g, 256, 0, s>>>(bcoo.R(), nnzb, nrows, bcoo.row_ptr.data());
+        STG_LAUNCH_CHECK();
+        launches++;
+        bcoo.row_ptr_valid = true;
+    }
+    STG_CUDA_TRY(cudaMemsetAsync(bcoo.t_cnt.data(), 0, sizeof(int) * (nrows + 1), s));
+    k_t_count<<<g, 256, 0, s>>>(bcoo.R(), bcoo.C(), nnzb, bcoo.t_cnt.data());
+    STG_LAUNCH_CHECK();
+    k_scan_exclusive<<<1, 1024, 0, s>>>(bcoo.t_cnt.data(), bcoo.t_ptr.data(), nullptr, nrows + 1, cv.scratch.data() + 2);
+    STG_LAUNCH_CHECK();
+    STG_CUDA_TRY(cudaMemsetAsync(bcoo.t_cnt.data(), 0, sizeof(int) * (nrows + 1), s));
+    k_t_fill<<<g, 256, 0, s>>>(bcoo.R(), bcoo.C(), nnzb, bcoo.t_ptr.data(), bcoo.t_cnt.data(), bcoo.t_ent.data());
+    STG_LAUNCH_CHECK();
+    k_t_sort<<<std::max(1, std::min(div_up(nrows, 256), kSMs * 16)), 256, 0, s>>>(bcoo.t_ptr.data(), bcoo.t_ent.data(), nrows);
+    STG_LAUNCH_CHECK();
+    launches += 4;
+    if(cfg.precision == STG_PREC_FP32)
+    {
+        STG_TRY(bcoo.blocks32.resize((size_t)nnzb * 9));
+        k_to_f32<<<std::max(1, std::min(div_up((long)nnzb * 9, 256), kSMs * 16)), 256, 0, s>>>(bcoo.B(), bcoo.blocks32.data(),
+                                                                                           (size_t)nnzb * 9);
+        STG_LAUNCH_CHECK();
+        launches++;
+    }
+    if(cfg.preconditioner == STG_PRECOND_DIAG)
+    {
+        STG_TRY(bcoo.diag_inv.resize((size_t)nrows * 9));
+        STG_CUDA_TRY(cudaMemsetAsync(bcoo.diag_inv.data(), 0, sizeof(double) * 9 * nrows, s));
+        k_diag_inv<<<g, 256, 0, s>>>(bcoo.R(), bcoo.C(), bcoo.B(), nnzb, bcoo.diag_inv.data());
+        STG_LAUNCH_CHECK();
+        launches++;
+    }
+    bcoo.offdiag = -1;  // not needed on the host
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// the standalone SpMV kernel (stg_spmv): y = a A x + b y
+// ---------------------------------------------------------------------------------------
+template <typename T, int LPR>
+__global__ void __launch_bounds__(256) k_spmv_sym(const int* __restrict__ row_ptr, const int* __restrict__ cols,
+                                                  const T* __restrict__ blocks, const int* __restrict__ t_ptr,
+                                                  const int2* __restrict__ t_ent, const T* __restrict__ x, T* y, double a,
+                                                  double b, int nrows)
+{
+    constexpr int RPW = 32 / LPR;  // rows per warp
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31, sub = lane & (LPR - 1);
+    for(int base = warp * RPW; base < nrows; base += nwarps * RPW)
+    {
+        const int i = base + lane / LPR;
+        const bool valid = i < nrows;
+        T a0, a1, a2;
+        row_spmv<T, LPR>(i, valid, sub, row_ptr, cols, blocks, t_ptr, t_ent, x, a0, a1, a2);
+        if(valid && sub < 3)
+        {
+            T v = sub == 0 ? a0 : (sub == 1 ? a1 : a2);
+            double out = a * (double)v;
+            if(b != 0.0) out += b * (double)y[3 * i + sub];
+            y[3 * i + sub] = (T)out;
+        }
+    }
+}
+
+int Solver::spmv(double a, const double* x, double b, double* y)
+{
+    const int nrows = bcoo.nrows;
+    if(nrows < 1) return 0;
+    const int grid = std::max(1, std::min(div_up(nrows, 256 / 16), kSMs * 8));
+    k_spmv_sym<double, 16><<<grid, 256, 0, stream>>>(bcoo.row_ptr.data(), bcoo.C(), bcoo.B(), bcoo.t_ptr.data(),
+                                                     bcoo.t_ent.data(), x, y, a, b, nrows);
+    STG_LAUNCH_CHECK();
+    launches++;
+    return 0;
+}
+
+}  // namespace stg

@@ -1,0 +1,450 @@
+"""Seeded synthetic Newton systems in the layout StiffGIPC hands to its linear solver.
+
+The reference assembles, every Newton iteration, a triplet buffer (``GIPCTripletMatrix``,
+StiffGIPC/linear_system/linear_system/global_matrix.h:52-253) in this order
+(StiffGIPC/GIPC.cu:10258-10493):
+
+1. contact / ground barrier blocks, one 3x3 ``n n^T`` block per active vertex
+   (``_computeGroundGradientAndHessian``, GIPC.cu:6506-6557);
+2. FEM tetrahedra, 10 upper blocks per tet in (ii <= jj) order with the row <= col swap
+   (``_calculate_fem_gradient_hessian``, femEnergy.cu:1832-1854);
+3. one mass block ``m_i I`` per FEM vertex (GIPC.cu:10466-10482).
+
+Blocks are 3x3 FP64 stored column-major (Eigen ``Matrix3d``), rows/cols are int32 block
+indices (vertex id + 4 * abd_body_num).  The right-hand side is the gradient
+(fem_linear_subsystem.cu:56-84).
+
+This module only produces inputs for the solver (the Hessian producer sits upstream of the
+hot path); it is plain numpy, deterministic for a given seed.
+
+Meshes: an n x n x n hex grid split into 6 tets per hex along the main diagonal
+(Kuhn/Freudenthal), vertices renumbered by the reference's 30-bit Morton code
+(``hash_code(type=-1)`` / ``_calcVertMChash``, GIPC.cu:183-241, 453-502) so that
+consecutive vertices form the MAS partitions ("GPU MAS, Morton ordered").
+"""
+from __future__ import annotations
+
+import dataclasses
+import os
+from typing import Optional
+
+import numpy as np
+
+# ----------------------------------------------------------------------------------------
+# Morton code (GIPC.cu:183-241)
+# ----------------------------------------------------------------------------------------
+
+
+def expand_bits(v: np.ndarray) -> np.ndarray:
+    """Spread the low 10 bits of ``v`` three apart (GIPC.cu:183-190), uint32 arithmetic."""
+    v = v.astype(np.uint64)
+    m = np.uint64(0xFFFFFFFF)
+    v = ((v * np.uint64(0x00010001)) & m) & np.uint64(0xFF0000FF)
+    v = ((v * np.uint64(0x00000101)) & m) & np.uint64(0x0F00F00F)
+    v = ((v * np.uint64(0x00000011)) & m) & np.uint64(0xC30C30C3)
+    v = ((v * np.uint64(0x00000005)) & m) & np.uint64(0x49249249)
+    return v.astype(np.uint32)
+
+
+def morton_hash(pos: np.ndarray, resolution: float = 1024.0) -> np.ndarray:
+    """Per-vertex 64-bit key ``(mc32 << 32) | idx`` of ``_calcVertMChash`` (GIPC.cu:453-502).
+
+    Positions are normalised per axis to the scene AABB, scaled to ``resolution`` cells,
+    clamped to ``[0, resolution-1]`` and truncated (``hash_code`` type -1, GIPC.cu:192-208).
+    """
+    lower = pos.min(axis=0)
+    upper = pos.max(axis=0)
+    size = upper - lower
+    off = (pos - lower) / size
+    q = np.clip(off * resolution, 0.0, resolution - 1.0).astype(np.uint32)
+    xx, yy, zz = expand_bits(q[:, 0]), expand_bits(q[:, 1]), expand_bits(q[:, 2])
+    mc32 = ((xx.astype(np.uint64) << np.uint64(2)) + (yy.astype(np.uint64) << np.uint64(1))
+            + zz.astype(np.uint64)) & np.uint64(0xFFFFFFFF)
+    idx = np.arange(pos.shape[0], dtype=np.uint64)
+    return (mc32 << np.uint64(32)) | idx
+
+
+# ----------------------------------------------------------------------------------------
+# Mesh
+# ----------------------------------------------------------------------------------------
+
+
+def cube_mesh(n: int, size: float = 1.0, origin=(0.0, 0.0, 0.0)):
+    """(n+1)^3 grid vertices and 6 n^3 Kuhn tets (all sharing each hex's main diagonal)."""
+    m = n + 1
+    g = np.arange(m, dtype=np.float64) * (size / n)
+    z, y, x = np.meshgrid(g, g, g, indexing="ij")
+    pos = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1) + np.asarray(origin, dtype=np.float64)
+
+    def vid(i, j, k):
+        return i + m * (j + m * k)
+
+    ii, jj, kk = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    ii, jj, kk = ii.ravel(), jj.ravel(), kk.ravel()
+    e = [(1, 0, 0), (0, 1, 0), (0, 0, 1)]
+    perms = [(0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)]
+    tets = []
+    for p in perms:
+        a = e[p[0]]
+        b = tuple(e[p[0]][t] + e[p[1]][t] for t in range(3))
+        v0 = vid(ii, jj, kk)
+        v1 = vid(ii + a[0], jj + a[1], kk + a[2])
+        v2 = vid(ii + b[0], jj + b[1], kk + b[2])
+        v3 = vid(ii + 1, jj + 1, kk + 1)
+        tets.append(np.stack([v0, v1, v2, v3], axis=1))
+    # hex-major order: the 6 tets of a hex are consecutive
+    tets = np.stack(tets, axis=1).reshape(-1, 4).astype(np.int64)
+    # positive orientation
+    d = pos[tets[:, 1:]] - pos[tets[:, :1]]
+    det = np.linalg.det(np.transpose(d, (0, 2, 1)))
+    neg = det < 0
+    tets[neg, 1], tets[neg, 2] = tets[neg, 2].copy(), tets[neg, 1].copy()
+    return pos, tets
+
+
+def morton_renumber(pos: np.ndarray, tets: np.ndarray):
+    """Renumber vertices by ascending Morton key; returns (pos', tets', old_of_new)."""
+    key = morton_hash(pos)
+    order = np.argsort(key, kind="stable")
+    new_of_old = np.empty_like(order)
+    new_of_old[order] = np.arange(order.size)
+    return pos[order], new_of_old[tets], order
+
+
+def vert_neighbors(num_verts: int, tets: np.ndarray):
+    """CSR vertex neighbour lists with the ordering of ``getVertNeighbors``.
+
+    load_mesh.cpp:934-1040: every tet edge is inserted into a ``std::set<pair>`` in the
+    orientation it is first met (tet order, edge order 01,02,03,12,13,23), the set is walked
+    in lexicographic order and each edge (a, b) appends b to a's list and a to b's list.
+    Returns (start, num, list) as uint32 arrays.
+    """
+    pairs = np.stack([tets[:, [0, 0, 0, 1, 1, 2]], tets[:, [1, 2, 3, 2, 3, 3]]], axis=2).reshape(-1, 2)
+    lo = np.minimum(pairs[:, 0], pairs[:, 1])
+    hi = np.maximum(pairs[:, 0], pairs[:, 1])
+    ukey = lo.astype(np.int64) * num_verts + hi
+    # first occurrence of each undirected edge keeps its orientation
+    _, first = np.unique(ukey, return_index=True)
+    edges = pairs[np.sort(first)]
+    # std::set order: lexicographic on (first, second)
+    order = np.lexsort((edges[:, 1], edges[:, 0]))
+    edges = edges[order]
+    a, b = edges[:, 0], edges[:, 1]
+    # append order: walk edges; for edge e, a gets b, then b gets a
+    src = np.empty(2 * a.size, dtype=np.int64)
+    dst = np.empty(2 * a.size, dtype=np.int64)
+    src[0::2], dst[0::2] = a, b
+    src[1::2], dst[1::2] = b, a
+    order = np.argsort(src, kind="stable")
+    nlist = dst[order].astype(np.uint32)
+    num = np.bincount(src, minlength=num_verts).astype(np.uint32)
+    start = np.zeros(num_verts, dtype=np.uint32)
+    start[1:] = np.cumsum(num[:-1], dtype=np.int64).astype(np.uint32)
+    return start, num, nlist
+
+
+def mas_partition_morton(num_verts: int, bank: int):
+    """Slot maps of ``set_mas_partition`` (app/common/sim_bootstrap.cpp:90-113) for a
+    Morton-ordered mesh where partition p = vertices [p*bank, (p+1)*bank)."""
+    part_id = np.arange(num_verts) // bank
+    return slot_maps_from_parts(part_id, bank)
+
+
+def slot_maps_from_parts(part_id: np.ndarray, bank: int):
+    """``set_mas_partition`` (sim_bootstrap.cpp:90-113): partId_map_real (size
+    part_offset*bank, -1 padding) and real_map_partId, for vertices grouped by part id."""
+    part_id = np.asarray(part_id, dtype=np.int64)
+    nparts = int(part_id[-1]) + 1
+    part_map = np.full(nparts * bank, -1, dtype=np.int32)
+    index = 0
+    for i in range(part_id.size):
+        part_map[bank * part_id[i] + index] = i
+        index += 1
+        if i <= part_id.size - 2 and part_id[i + 1] != part_id[i]:
+            index = 0
+    inv = np.zeros(part_id.size, dtype=np.int32)
+    index = 0
+    for i in range(part_map.size):
+        if part_map[i] == index:
+            inv[index] = i
+            index += 1
+    return part_map, inv
+
+
+# ----------------------------------------------------------------------------------------
+# Energies (FP64, PSD projected)
+# ----------------------------------------------------------------------------------------
+
+_EPS = np.zeros((3, 3, 3))
+_EPS[0, 1, 2] = _EPS[1, 2, 0] = _EPS[2, 0, 1] = 1.0
+_EPS[0, 2, 1] = _EPS[2, 1, 0] = _EPS[1, 0, 2] = -1.0
+# _HJ_OP[(m,n), (i,j,k,l)] = eps_ikm eps_jln (row-major vec indices)
+_HJ_OP = np.einsum("ikm,jln->mnijkl", _EPS, _EPS).reshape(9, 81)
+
+
+def _dFdx(dm_inv: np.ndarray) -> np.ndarray:
+    """(T, 9, 12) Jacobian of vec_rowmajor(F) w.r.t. the 4 vertex positions."""
+    t = dm_inv.shape[0]
+    d = np.empty((t, 4, 3))
+    d[:, 1:, :] = dm_inv
+    d[:, 0, :] = -dm_inv.sum(axis=1)
+    P = np.zeros((t, 9, 12))
+    for i in range(3):
+        for j in range(3):
+            for a in range(4):
+                P[:, 3 * i + j, 3 * a + i] = d[:, a, j]
+    return P
+
+
+def snh_gradient_hessian(F, mu, lam):
+    """Stable Neo-Hookean (Smith et al. 2018, no log term):
+    psi = mu/2 (|F|^2 - 3) + lam/2 (J - alpha)^2, alpha = 1 + mu/lam.
+    Returns (dpsi/dF as (T,9) row-major, PSD-projected d2psi/dF2 (T,9,9))."""
+    t = F.shape[0]
+    J = np.linalg.det(F)
+    alpha = 1.0 + mu / lam
+    # d2J/dF_ij dF_kl = eps_ikm eps_jln F_mn: a linear map of vec(F) (one matmul)
+    HJ = (F.reshape(t, 9) @ _HJ_OP).reshape(t, 9, 9)
+    # cof(F) = dJ/dF = 1/2 HJ : F
+    g = 0.5 * np.matmul(HJ, F.reshape(t, 9, 1)).reshape(t, 9)
+    P = mu[:, None] * F.reshape(t, 9) + (lam * (J - alpha))[:, None] * g
+    H = (mu[:, None, None] * np.eye(9)[None] + lam[:, None, None] * g[:, :, None] * g[:, None, :]
+         + (lam * (J - alpha))[:, None, None] * HJ)
+    H = 0.5 * (H + np.transpose(H, (0, 2, 1)))
+    w, V = np.linalg.eigh(H)
+    if (w < 0).any():
+        w = np.maximum(w, 0.0)
+        H = np.matmul(V * w[:, None, :], np.transpose(V, (0, 2, 1)))
+    return P, H
+
+
+def ground_barrier(dist, dhat, kappa):
+    """IPC plane barrier on squared distance (GIPC.cu:6524-6551).
+
+    Returns (dE/dd along the normal, scalar s such that the 3x3 Hessian is s * n n^T)."""
+    dist2 = dist * dist
+    dh2 = dhat * dhat
+    t = dist2 - dh2
+    g_b = t * np.log(dist2 / dh2) * -2.0 - (t * t) / dist2
+    H_b = (np.log(dist2 / dh2) * -2.0 - t * 4.0 / dist2) + 1.0 / (dist2 * dist2) * (t * t)
+    grad = kappa * g_b * 2.0 * dist
+    param = 4.0 * H_b * dist2 + 2.0 * g_b
+    return grad, kappa * param
+
+
+# ----------------------------------------------------------------------------------------
+# System container
+# ----------------------------------------------------------------------------------------
+
+
+@dataclasses.dataclass
+class NewtonSystem:
+    """One Newton linear system: triplets (pre-convert), RHS and MAS inputs."""
+    name: str
+    num_verts: int
+    rows: np.ndarray          # int32 [T]
+    cols: np.ndarray          # int32 [T]
+    blocks: np.ndarray        # float64 [T, 9] column-major 3x3
+    b: np.ndarray             # float64 [3V]
+    pos: np.ndarray           # float64 [V, 3]
+    tets: np.ndarray          # int64 [Tet, 4]
+    neighbor_start: np.ndarray
+    neighbor_num: np.ndarray
+    neighbor_list: np.ndarray
+    contacts: np.ndarray      # int32 [C, 4] (sign-encoded collision pairs, may be empty)
+    fem_block_offset: int = 0
+    abd_bodies: int = 0
+
+    @property
+    def n(self) -> int:
+        return 3 * self.num_verts
+
+    def slot_maps(self, bank: int):
+        return mas_partition_morton(self.num_verts, bank)
+
+
+def _assemble(name, pos_rest, pos, tets, E, nu, rho, dt, vel, barriers, rng_contacts=None):
+    """Build triplets + gradient of one implicit-Euler Newton iteration at ``pos``."""
+    V = pos.shape[0]
+    T = tets.shape[0]
+    mu_all = E / (2.0 * (1.0 + nu))
+    lam_all = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+
+    grad = np.zeros((V, 3))
+    mass = np.zeros(V)
+    tet_blocks = np.empty((T, 10, 9))
+    tet_rows = np.empty((T, 10), dtype=np.int32)
+    tet_cols = np.empty((T, 10), dtype=np.int32)
+    chunk = 1 << 15
+    pairs = [(ii, jj) for ii in range(4) for jj in range(ii, 4)]
+    for s in range(0, T, chunk):
+        tt = tets[s:s + chunk]
+        nt = tt.shape[0]
+        Dm = np.transpose(pos_rest[tt[:, 1:]] - pos_rest[tt[:, :1]], (0, 2, 1))
+        vol = np.abs(np.linalg.det(Dm)) / 6.0
+        Dminv = np.linalg.inv(Dm)
+        Ds = np.transpose(pos[tt[:, 1:]] - pos[tt[:, :1]], (0, 2, 1))
+        F = Ds @ Dminv
+        Pf, H9 = snh_gradient_hessian(F, mu_all[s:s + chunk], lam_all[s:s + chunk])
+        Jx = _dFdx(Dminv)
+        w = vol * dt * dt
+        JxT = np.transpose(Jx, (0, 2, 1))
+        f12 = w[:, None] * np.matmul(JxT, Pf[:, :, None])[:, :, 0]
+        H12 = w[:, None, None] * np.matmul(np.matmul(JxT, H9), Jx)
+        for a in range(4):
+            np.add.at(grad, tt[:, a], f12[:, 3 * a:3 * a + 3])
+            np.add.at(mass, tt[:, a], rho * vol / 4.0)
+        for kk, (ii, jj) in enumerate(pairs):
+            r = tt[:, ii]
+            c = tt[:, jj]
+            blk = H12[:, 3 * ii:3 * ii + 3, 3 * jj:3 * jj + 3]
+            swap = r > c
+            blk = np.where(swap[:, None, None], np.transpose(blk, (0, 2, 1)), blk)
+            tet_rows[s:s + nt, kk] = np.where(swap, c, r)
+            tet_cols[s:s + nt, kk] = np.where(swap, r, c)
+            # column-major 3x3 (Eigen Matrix3d)
+            tet_blocks[s:s + nt, kk] = np.transpose(blk, (0, 2, 1)).reshape(nt, 9)
+
+    # kinetic gradient: M (x - x_tilde), x_tilde = x_n + dt v + dt^2 g with x_n = pos_rest path
+    x_tilde = pos + dt * vel + dt * dt * np.array([0.0, -9.8, 0.0])
+    grad += mass[:, None] * (pos - x_tilde)
+
+    bar_rows, bar_blocks = [], []
+    for (normal, offset, dhat, kappa) in barriers:
+        normal = np.asarray(normal, dtype=np.float64)
+        dist = pos @ normal - offset
+        act = np.nonzero(dist < dhat)[0]
+        if act.size == 0:
+            continue
+        g, s_ = ground_barrier(dist[act], dhat, kappa)
+        grad[act] += g[:, None] * normal[None, :]
+        nn = np.outer(normal, normal).T.reshape(9)  # symmetric: layout irrelevant
+        bar_rows.append(act.astype(np.int32))
+        bar_blocks.append(s_[:, None] * nn[None, :])
+    if bar_rows:
+        bar_rows = np.concatenate(bar_rows)
+        bar_blocks = np.concatenate(bar_blocks)
+    else:
+        bar_rows = np.zeros(0, dtype=np.int32)
+        bar_blocks = np.zeros((0, 9))
+
+    mass_blocks = np.zeros((V, 9))
+    mass_blocks[:, 0] = mass_blocks[:, 4] = mass_blocks[:, 8] = mass
+    vids = np.arange(V, dtype=np.int32)
+
+    rows = np.concatenate([bar_rows, tet_rows.reshape(-1), vids])
+    cols = np.concatenate([bar_rows, tet_cols.reshape(-1), vids])
+    blocks = np.concatenate([bar_blocks, tet_blocks.reshape(-1, 9), mass_blocks])
+    start, num, nlist = vert_neighbors(V, tets)
+    return NewtonSystem(name=name, num_verts=V, rows=rows.astype(np.int32), cols=cols.astype(np.int32),
+                        blocks=np.ascontiguousarray(blocks), b=grad.reshape(-1).copy(), pos=pos, tets=tets,
+                        neighbor_start=start, neighbor_num=num, neighbor_list=nlist,
+                        contacts=np.zeros((0, 4), dtype=np.int32))
+
+
+def make_cube_drop(n: int = 16, seed: int = 1001, E: float = 1e5, nu: float = 0.45,
+                   rho: float = 1000.0, dt: float = 1.0 / 60.0, v0: float = -2.0,
+                   jitter: float = 1e-3, gap: float = 5e-4, dhat: float = 1e-3,
+                   kappa: float = 1e5) -> NewtonSystem:
+    """Plain FP64 MAS-PCG workload, one Newton step: a 1 m cube of n^3 hexes (6 tets each),
+    vertices jittered U(+-jitter) from ``seed``, falling at ``v0`` m/s in y, resting ``gap``
+    above a ground plane with an IPC barrier (d_hat, kappa).  n=16: 4,913 vertices,
+    24,576 tets, 14,739 DOF."""
+    rng = np.random.default_rng(seed)
+    pos, tets = cube_mesh(n, 1.0, origin=(0.0, gap, 0.0))
+    pos = pos + rng.uniform(-jitter, jitter, size=pos.shape)
+    bottom = np.isclose(pos[:, 1], gap, atol=2 * jitter)
+    pos[bottom, 1] = gap  # the resting face sits exactly gap above the ground
+    pos, tets, _ = morton_renumber(pos, tets)
+    E_t = np.full(tets.shape[0], E)
+    vel = np.zeros_like(pos)
+    vel[:, 1] = v0
+    return _assemble(f"cube{n}_drop", pos, pos, tets, E_t, nu, rho, dt, vel,
+                     barriers=[((0.0, 1.0, 0.0), 0.0, dhat, kappa)])
+
+
+def make_heterogeneous_cube(n: int = 48, seed: int = 1005, nu: float = 0.45, rho: float = 1000.0,
+                            dt: float = 1.0 / 60.0, e_lo: float = 1e4, e_hi: float = 1e8,
+                            regions: int = 8, squash: float = 0.08, jitter: float = 1e-3,
+                            dhat: float = 1e-3, kappa: float = 1e5, slab_speed: float = 1.0) -> NewtonSystem:
+    """Heterogeneous cube under a rigid slab: n^3 hexes (6 tets each), per-tet Young's modulus
+    log-uniform in [e_lo, e_hi] from ``regions`` seeded Voronoi sites, nu=0.45; one Newton
+    iteration of a step where the slab (moving down at ``slab_speed``) has squashed the top by
+    ``squash`` m.  The slab and the ground act through IPC plane barriers.  n=48: 117,649
+    vertices, 663,552 tets, 352,947 DOF."""
+    rng = np.random.default_rng(seed)
+    rest, tets = cube_mesh(n, 1.0, origin=(0.0, 0.0, 0.0))
+    rest = rest + rng.uniform(-jitter, jitter, size=rest.shape)
+    sites = rng.uniform(0.0, 1.0, size=(regions, 3))
+    site_E = np.exp(rng.uniform(np.log(e_lo), np.log(e_hi), size=regions))
+    rest, tets, _ = morton_renumber(rest, tets)
+    cent = rest[tets].mean(axis=1)
+    d2 = ((cent[:, None, :] - sites[None, :, :]) ** 2).sum(axis=2)
+    E_t = site_E[np.argmin(d2, axis=1)]
+    # deformed state: top squashed down non-uniformly, bottom resting just above the ground
+    pos = rest.copy()
+    y = rest[:, 1]
+    bulge = 1.0 + 0.3 * np.sin(np.pi * rest[:, 0]) * np.sin(np.pi * rest[:, 2])
+    pos[:, 1] = y - squash * y * y * bulge
+    pos[:, 0] += 0.02 * squash * (rest[:, 0] - 0.5) * y
+    pos[:, 2] += 0.02 * squash * (rest[:, 2] - 0.5) * y
+    pos += rng.uniform(-0.05 * jitter, 0.05 * jitter, size=pos.shape)
+    pos[:, 1] += 4e-4 - pos[:, 1].min()
+    top = pos[:, 1].max() + 4e-4
+    vel = np.zeros_like(pos)
+    vel[:, 1] = -slab_speed * (rest[:, 1])
+    return _assemble(f"hetcube{n}", rest, pos, tets, E_t, nu, rho, dt, vel,
+                     barriers=[((0.0, 1.0, 0.0), 0.0, dhat, kappa), ((0.0, -1.0, 0.0), -top, dhat, kappa)])
+
+
+def make_batched_cubes(count: int = 256, seed: int = 1004, n_lo: int = 4, n_hi: int = 24,
+                       e_lo: float = 1e4, e_hi: float = 1e7, nu: float = 0.45, rho: float = 1000.0,
+                       dt: float = 1.0 / 60.0, press: float = 5e-4, dhat: float = 1e-3,
+                       kappa: float = 1e5, max_dof: Optional[int] = None):
+    """Independent Neo-Hookean cubes, n x n x n hexes with n log-uniform in [n_lo, n_hi]
+    and E log-uniform in [e_lo, e_hi], each pressed ``press`` into a ground barrier."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for c in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi)))))
+        E = float(np.exp(rng.uniform(np.log(e_lo), np.log(e_hi))))
+        sub = int(rng.integers(0, 2**31 - 1))
+        r2 = np.random.default_rng(sub)
+        rest, tets = cube_mesh(n, 0.1 * n / n_hi + 0.02, origin=(0.0, 0.0, 0.0))
+        rest = rest + r2.uniform(-1e-5, 1e-5, size=rest.shape)
+        rest, tets, _ = morton_renumber(rest, tets)
+        pos = rest.copy()
+        # pressed into the ground: bottom at dhat - press (inside the barrier zone)
+        pos[:, 1] += (dhat - press) - pos[:, 1].min() + 1e-6
+        pos[:, 1] *= 1.0
+        E_t = np.full(tets.shape[0], E)
+        vel = np.zeros_like(pos)
+        sysm = _assemble(f"batch{c}_n{n}", rest, pos, tets, E_t, nu, rho, dt, vel,
+                         barriers=[((0.0, 1.0, 0.0), 0.0, dhat, kappa)])
+        out.append(sysm)
+        if max_dof is not None and sum(s.n for s in out) >= max_dof:
+            break
+    return out
+
+
+_CACHE_ENV = "STGIPC_SCENE_CACHE"
+
+
+def cached(builder, key: str, **kw) -> NewtonSystem:
+    """Build a system, memoised as an .npz under $STGIPC_SCENE_CACHE (if set)."""
+    root = os.environ.get(_CACHE_ENV)
+    if not root:
+        return builder(**kw)
+    os.makedirs(root, exist_ok=True)
+    path = os.path.join(root, key + ".npz")
+    if os.path.exists(path):
+        z = np.load(path)
+        return NewtonSystem(name=str(z["name"]), num_verts=int(z["num_verts"]), rows=z["rows"], cols=z["cols"],
+                            blocks=z["blocks"], b=z["b"], pos=z["pos"], tets=z["tets"],
+                            neighbor_start=z["neighbor_start"], neighbor_num=z["neighbor_num"],
+                            neighbor_list=z["neighbor_list"], contacts=z["contacts"])
+    s = builder(**kw)
+    np.savez(path, name=s.name, num_verts=s.num_verts, rows=s.rows, cols=s.cols, blocks=s.blocks, b=s.b,
+             pos=s.pos, tets=s.tets, neighbor_start=s.neighbor_start, neighbor_num=s.neighbor_num,
+             neighbor_list=s.neighbor_list, contacts=s.contacts)
+    return s

@@ -1,0 +1,74 @@
+"""Regenerate the golden fixtures from the reference's shipped assets.
+
+    python tests/golden/make_golden.py /root/reference
+
+Reads Assets/sorted_mesh/{cube,bunny2}_sorted.16.{msh,part} and cloth_high_sorted.16.{obj,part}
+(the METIS-partitioned, partition-sorted meshes the reference ships; produced by
+MeshProcess/metis_partition/src/metis_sort.cpp) and stores their element connectivity,
+vertex positions and per-vertex partition ids as compressed .npz files next to this script.
+These pin the CEMAS ordering inputs (partId per vertex, vertices grouped by part) for the
+MAS hierarchy tests; nothing else is taken from the reference.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def read_msh(path):
+    """gmsh 2.2 ASCII: $Nodes (id x y z), $Elements (id type ntags [tags] v...), tets are type 4."""
+    with open(path) as f:
+        lines = f.read().split("\n")
+    i = lines.index("$Nodes")
+    nn = int(lines[i + 1])
+    pos = np.array([[float(t) for t in lines[i + 2 + k].split()[1:4]] for k in range(nn)])
+    j = lines.index("$Elements")
+    ne = int(lines[j + 1])
+    tets = []
+    for k in range(ne):
+        t = lines[j + 2 + k].split()
+        if int(t[1]) == 4:
+            ntag = int(t[2])
+            tets.append([int(v) - 1 for v in t[3 + ntag:3 + ntag + 4]])
+    return pos, np.array(tets, dtype=np.int32)
+
+
+def read_obj(path):
+    pos, tris = [], []
+    with open(path) as f:
+        for line in f:
+            t = line.split()
+            if not t:
+                continue
+            if t[0] == "v":
+                pos.append([float(a) for a in t[1:4]])
+            elif t[0] == "f":
+                tris.append([int(a.split("/")[0]) - 1 for a in t[1:4]])
+    return np.array(pos), np.array(tris, dtype=np.int32)
+
+
+def read_part(path):
+    return np.loadtxt(path, dtype=np.int32).reshape(-1)
+
+
+def main(ref_root):
+    sm = os.path.join(ref_root, "Assets", "sorted_mesh")
+    for name in ("cube", "bunny2"):
+        pos, tets = read_msh(os.path.join(sm, f"{name}_sorted.16.msh"))
+        part = read_part(os.path.join(sm, f"{name}_sorted.16.part"))
+        assert part.size == pos.shape[0], (name, part.size, pos.shape)
+        np.savez_compressed(os.path.join(HERE, f"{name}_sorted16.npz"), pos=pos.astype(np.float32), tets=tets, part=part)
+        print(name, pos.shape[0], "verts", tets.shape[0], "tets")
+    pos, tris = read_obj(os.path.join(sm, "cloth_high_sorted.16.obj"))
+    part = read_part(os.path.join(sm, "cloth_high_sorted.16.part"))
+    assert part.size == pos.shape[0]
+    np.savez_compressed(os.path.join(HERE, "cloth_high_sorted16.npz"), pos=pos.astype(np.float32), tris=tris, part=part)
+    print("cloth_high", pos.shape[0], "verts", tris.shape[0], "tris")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

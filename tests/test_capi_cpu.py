@@ -1,0 +1,70 @@
+"""CPU: the C-ABI library loads and exports every symbol include/stgipc.h declares; calls
+that need no GPU behave (defaults, no-device error)."""
+import ctypes as C
+import os
+import subprocess
+
+import pytest
+
+from conftest import ROOT, have_gpu
+
+
+@pytest.fixture(scope="module")
+def L():
+    from stgipc import _lib
+    if not os.path.exists(_lib.LIB_PATH):
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("stg_build", os.path.join(ROOT, "stiff-gipc_b200", "build.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.build()
+    return _lib.lib()
+
+
+def test_exports_every_header_symbol(L):
+    from stgipc import _lib
+    syms = _lib.header_symbols()
+    assert len(syms) >= 14
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    missing = [s for s in syms if s not in exported]
+    assert not missing, missing
+    for s in syms:
+        assert hasattr(L, s)
+
+
+def test_config_default(L):
+    from stgipc import _lib
+    c = _lib.Config()
+    L.stg_config_default(C.byref(c))
+    assert c.bank_size == 16 and c.tol == 1e-4 and abs(c.max_iter_ratio - 0.3) < 1e-15
+    assert c.precision == 0 and c.preconditioner == 1 and c.stop_rule == 0
+
+
+@pytest.mark.skipif(have_gpu(), reason="checks the no-device path")
+def test_create_without_device_reports_error(L):
+    from stgipc import _lib
+    h = C.c_void_p()
+    c = _lib.Config()
+    L.stg_config_default(C.byref(c))
+    assert L.stg_create(C.byref(c), C.byref(h)) == _lib.STG_ERR_NO_DEVICE
+    assert b"device" in L.stg_last_error()
+
+
+def test_invalid_config_rejected_before_device(L):
+    from stgipc import _lib
+    h = C.c_void_p()
+    c = _lib.Config()
+    L.stg_config_default(C.byref(c))
+    c.bank_size = 24
+    assert L.stg_create(C.byref(c), C.byref(h)) == _lib.STG_ERR_INVALID
+    assert L.stg_destroy(None) == _lib.STG_OK
+    assert L.stg_convert(None, 0, None, None, None, None) == _lib.STG_ERR_INVALID
+
+
+def test_missing_library_fails_loudly(tmp_path, monkeypatch):
+    from stgipc import _lib
+    monkeypatch.setattr(_lib, "_lib", None)
+    monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "libstgipc.so"))
+    with pytest.raises(ImportError):
+        _lib.lib()

@@ -1,0 +1,285 @@
+"""GPU parity: libstgipc (sm_100a) against the CPU oracle, through the C ABI.
+
+Tolerances:
+  * integer work (convert indices, MAS masks / coarse ids / tables): bit-exact;
+  * convert block sums: bit-exact (both sum duplicates in input order);
+  * FP64 SpMV: 1e-13 relative (different summation order);
+  * MAS Galerkin matrices (FP64 atomics at coarse levels): 1e-12 relative;
+  * MAS FP32 inverses and apply: 2e-5 relative to the bank's / vector's max magnitude;
+  * PCG, all-FP64 preconditioner (block Jacobi): x within 1e-8 relative of the oracle;
+  * PCG with MAS (FP32 apply, as the reference): same iteration count +-2 and x within
+    1e-4 relative (the preconditioner is a float operator; both solutions satisfy the
+    reference stopping rule).
+"""
+import numpy as np
+import pytest
+
+from conftest import cube_system, fixture_system, random_contacts
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(a, dev):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+def _solver(**kw):
+    from stgipc import PCGSolverConfig, Solver
+    return Solver(PCGSolverConfig(**kw))
+
+
+def _converted(sysm):
+    from oracle import oracle as orc
+    return orc.convert(sysm.rows, sysm.cols, sysm.blocks)
+
+
+# ------------------------------------------------------------------------------------------
+def test_convert_bit_exact(dev):
+    from oracle import oracle as orc
+    s = cube_system(16)
+    rng = np.random.default_rng(7)
+    perm = rng.permutation(s.rows.size)
+    extra = rng.integers(0, s.rows.size, size=5000)   # duplicate some triplets
+    rows = np.concatenate([s.rows[perm], s.rows[extra]])
+    cols = np.concatenate([s.cols[perm], s.cols[extra]])
+    blocks = np.concatenate([s.blocks[perm], s.blocks[extra] * 0.5])
+    er, ec, eb = orc.convert(rows, cols, blocks)
+    R, Cc, Bk = _t(rows, dev), _t(cols, dev), _t(blocks.reshape(-1), dev)
+    u = _solver().convert(R, Cc, Bk)
+    assert u == er.size
+    assert np.array_equal(R[:u].cpu().numpy(), er)
+    assert np.array_equal(Cc[:u].cpu().numpy(), ec)
+    assert np.array_equal(Bk[:9 * u].cpu().numpy().reshape(-1, 9), eb)
+
+
+def test_convert_edge_cases(dev):
+    from oracle import oracle as orc
+    solver = _solver()
+    # single triplet
+    R, Cc, Bk = _t(np.array([3], np.int32), dev), _t(np.array([5], np.int32), dev), _t(np.arange(9.0), dev)
+    assert solver.convert(R, Cc, Bk) == 1
+    # all duplicates of one key, and a row with no entries in between
+    rows = np.array([0, 0, 0, 2, 2], np.int32)
+    cols = np.array([1, 1, 1, 2, 2], np.int32)
+    blocks = np.random.default_rng(1).standard_normal((5, 9))
+    er, ec, eb = orc.convert(rows, cols, blocks)
+    R, Cc, Bk = _t(rows, dev), _t(cols, dev), _t(blocks.reshape(-1), dev)
+    u = solver.convert(R, Cc, Bk)
+    assert u == 2 and np.array_equal(R[:u].cpu().numpy(), er) and np.array_equal(Cc[:u].cpu().numpy(), ec)
+    assert np.array_equal(Bk[:9 * u].cpu().numpy().reshape(-1, 9), eb)
+
+
+# ------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("a,b", [(1.0, 0.0), (-0.5, 2.0)])
+def test_spmv(dev, a, b):
+    from oracle import oracle as orc
+    s = cube_system(16)
+    r, c, bl = _converted(s)
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(s.n)
+    y0 = rng.standard_normal(s.n)
+    ye = orc.spmv(r, c, bl, x, a=a, b=b, y=y0)
+    Y = _t(y0, dev)
+    _solver().spmv(a, _t(bl.reshape(-1), dev), _t(r, dev), _t(c, dev), r.size, _t(x, dev), b, Y)
+    yg = Y.cpu().numpy()
+    assert np.max(np.abs(yg - ye)) <= 1e-13 * np.max(np.abs(ye))
+
+
+def test_spmv_deterministic(dev):
+    s = cube_system(16)
+    r, c, bl = _converted(s)
+    x = np.random.default_rng(4).standard_normal(s.n)
+    solver = _solver()
+    outs = []
+    for _ in range(3):
+        Y = _t(np.zeros(s.n), dev)
+        solver.spmv(1.0, _t(bl.reshape(-1), dev), _t(r, dev), _t(c, dev), r.size, _t(x, dev), 0.0, Y)
+        outs.append(Y.cpu().numpy())
+    assert all(np.array_equal(outs[0], o) for o in outs[1:])
+
+
+# ------------------------------------------------------------------------------------------
+def _mas_pair(sysm, bank, part=None, contacts=None, dev=None):
+    from stgipc import scenes
+    from oracle import oracle as orc
+    if part is None:
+        pm, rm = sysm.slot_maps(bank)
+    else:
+        pm, rm = scenes.slot_maps_from_parts(part, bank)
+    om = orc.Mas(bank, sysm.num_verts, sysm.neighbor_start, sysm.neighbor_num, sysm.neighbor_list, pm, rm)
+    om.build(contacts)
+    solver = _solver(bank_size=bank)
+    solver.mas_init(sysm.num_verts, sysm.neighbor_start, sysm.neighbor_num, sysm.neighbor_list, pm, rm)
+    r, c, bl = _converted(sysm)
+    om.assemble(r, c, bl)
+    C = None if contacts is None else _t(contacts, dev)
+    solver.mas_assemble(_t(bl.reshape(-1), dev), _t(r, dev), _t(c, dev), r.size, 0, C)
+    return om, solver, pm, (r, c, bl)
+
+
+def _compare_hierarchy(om, solver, pm):
+    e = om.hierarchy()
+    g = solver.export_hierarchy(pm.size)
+    L, T, ls = solver.mas_info()
+    assert L == om.L and T == om.total
+    assert np.array_equal(ls, e["level_size"])
+    assert np.array_equal(g["fine_mask"], e["fine_mask"])
+    assert np.array_equal(g["prefix_orig"], e["prefix_orig"])
+    assert np.array_equal(g["coarse_tables"], e["coarse_tables"])
+    V = om.V
+    assert np.array_equal(g["going_next"][:V], e["going_next"][:V])
+    assert np.array_equal(g["going_next"][om.M:T], e["going_next"][om.M:T])
+    if L > 1:
+        assert np.array_equal(g["coarse_table"], e["coarse_table"])
+
+
+@pytest.mark.parametrize("bank", [16, 32])
+@pytest.mark.parametrize("with_contacts", [False, True])
+def test_mas_hierarchy_bit_exact_morton(dev, bank, with_contacts):
+    s = cube_system(16)
+    cp = random_contacts(s.num_verts, 600, seed=11) if with_contacts else None
+    om, solver, pm, _ = _mas_pair(s, bank, contacts=cp, dev=dev)
+    _compare_hierarchy(om, solver, pm)
+
+
+@pytest.mark.parametrize("with_contacts", [False, True])
+def test_mas_hierarchy_bit_exact_metis_fixture(dev, with_contacts):
+    """bunny2 as the reference ships it: METIS 16-vertex partitions, partition-sorted."""
+    s, part = fixture_system("bunny2")
+    cp = random_contacts(s.num_verts, 2000, seed=12) if with_contacts else None
+    om, solver, pm, _ = _mas_pair(s, 16, part=part, contacts=cp, dev=dev)
+    _compare_hierarchy(om, solver, pm)
+
+
+@pytest.mark.parametrize("bank", [16, 32])
+def test_mas_matrices_and_inverse(dev, bank):
+    s = cube_system(16)
+    om, solver, pm, _ = _mas_pair(s, bank, dev=dev)
+    em, ei = om.matrices()
+    gm, gi = solver.export_matrices()
+    assert gm.shape == em.shape
+    scale = np.abs(em).max(axis=(1, 2), keepdims=True) + 1e-300
+    assert np.max(np.abs(gm - em) / scale) <= 1e-12
+    iscale = np.abs(ei).max(axis=(1, 2), keepdims=True) + 1e-30
+    assert np.max(np.abs(gi - ei) / iscale) <= 2e-5
+
+
+@pytest.mark.parametrize("bank", [16, 32])
+def test_mas_apply(dev, bank):
+    s = cube_system(16)
+    om, solver, pm, _ = _mas_pair(s, bank, dev=dev)
+    rvec = np.random.default_rng(5).standard_normal(s.n)
+    ze = om.apply(rvec)
+    Z = _t(np.zeros(s.n), dev)
+    solver.mas_apply(_t(rvec, dev), Z)
+    zg = Z.cpu().numpy()
+    assert np.max(np.abs(zg - ze)) <= 2e-5 * np.max(np.abs(ze))
+
+
+def test_mas_apply_metis_fixture_with_contacts(dev):
+    s, part = fixture_system("bunny2")
+    cp = random_contacts(s.num_verts, 2000, seed=13)
+    om, solver, pm, _ = _mas_pair(s, 16, part=part, contacts=cp, dev=dev)
+    rvec = np.random.default_rng(6).standard_normal(s.n)
+    ze = om.apply(rvec)
+    Z = _t(np.zeros(s.n), dev)
+    solver.mas_apply(_t(rvec, dev), Z)
+    assert np.max(np.abs(Z.cpu().numpy() - ze)) <= 2e-5 * np.max(np.abs(ze))
+
+
+# ------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("loop", ["host", "graph"])
+def test_pcg_block_jacobi_fp64(dev, loop):
+    """All-FP64 path (global 3x3 block-Jacobi = DiagPreconditioner): x within 1e-8."""
+    from oracle import oracle as orc
+    s = cube_system(16)
+    r, c, bl = _converted(s)
+    xe, st_e = orc.pcg(r, c, bl, s.b, use_diag=True)
+    solver = _solver(preconditioner="diag", loop=loop)
+    X = _t(np.zeros(s.n), dev)
+    st = solver.pcg_solve(_t(bl.reshape(-1), dev), _t(r, dev), _t(c, dev), r.size, _t(s.b, dev), X)
+    assert st["iterations"] == st_e["iterations"]
+    xg = X.cpu().numpy()
+    assert np.linalg.norm(xg - xe) <= 1e-8 * np.linalg.norm(xe)
+    assert abs(st["rel_residual"] - st_e["rel_residual"]) <= 1e-6 * max(st_e["rel_residual"], 1e-30)
+
+
+@pytest.mark.parametrize("bank", [16, 32])
+def test_pcg_mas_vs_oracle(dev, bank):
+    from oracle import oracle as orc
+    s = cube_system(16)
+    om, _, pm, (r, c, bl) = _mas_pair(s, bank, dev=dev)
+    xe, st_e = orc.pcg(r, c, bl, s.b, mas=om)
+    G = _t(bl.reshape(-1), dev), _t(r, dev), _t(c, dev)
+    solver = _solver(bank_size=bank)
+    solver.mas_init(s.num_verts, s.neighbor_start, s.neighbor_num, s.neighbor_list, *s.slot_maps(bank))
+    solver.mas_assemble(G[0], G[1], G[2], r.size, 0, None)
+    X = _t(np.zeros(s.n), dev)
+    st = solver.pcg_solve(G[0], G[1], G[2], r.size, _t(s.b, dev), X)
+    assert abs(st["iterations"] - st_e["iterations"]) <= 2
+    xg = X.cpu().numpy()
+    assert np.linalg.norm(xg - xe) <= 1e-4 * np.linalg.norm(xe)
+
+
+def test_loop_modes_identical(dev):
+    s = cube_system(16)
+    r, c, bl = _converted(s)
+    res = []
+    for loop in ("host", "graph"):
+        from stgipc import GlobalLinearSystem, PCGSolverConfig
+        gls = GlobalLinearSystem(s, PCGSolverConfig(loop=loop, preconditioner="diag"), device=dev)
+        st = gls.solve_linear_system()
+        res.append((st["iterations"], gls.x.cpu().numpy()))
+    assert res[0][0] == res[1][0] and np.array_equal(res[0][1], res[1][1])
+
+
+@pytest.mark.parametrize("bank", [16, 32])
+def test_solve_linear_system_end_to_end(dev, bank):
+    """Triplets -> convert -> MAS build/assemble -> PCG, against the oracle pipeline."""
+    from oracle import oracle as orc
+    from stgipc import GlobalLinearSystem, PCGSolverConfig
+    s = cube_system(16)
+    r, c, bl = _converted(s)
+    om = orc.Mas(bank, s.num_verts, s.neighbor_start, s.neighbor_num, s.neighbor_list, *s.slot_maps(bank))
+    om.build()
+    om.assemble(r, c, bl)
+    xe, st_e = orc.pcg(r, c, bl, s.b, mas=om)
+    gls = GlobalLinearSystem(s, PCGSolverConfig(bank_size=bank), device=dev)
+    st = gls.solve_linear_system()
+    assert st["nnzb"] == r.size == 35937
+    assert abs(st["iterations"] - st_e["iterations"]) <= 2
+    assert np.linalg.norm(gls.x.cpu().numpy() - xe) <= 1e-4 * np.linalg.norm(xe)
+
+
+def test_fp32_mode_relative_residual(dev):
+    """FP32 SpMV/MAS storage, FP64 dots + residual replacement: FP64 residual <= 1e-4."""
+    from oracle import oracle as orc
+    from stgipc import GlobalLinearSystem, PCGSolverConfig
+    s = cube_system(16)
+    r, c, bl = _converted(s)
+    om = orc.Mas(16, s.num_verts, s.neighbor_start, s.neighbor_num, s.neighbor_list, *s.slot_maps(16))
+    om.build()
+    om.assemble(r, c, bl)
+    xe, _ = orc.pcg(r, c, bl, s.b, mas=om, tol=1e-10)
+    gls = GlobalLinearSystem(s, PCGSolverConfig(precision="fp32", stop_rule="relative_residual", refine_interval=8),
+                             device=dev)
+    st = gls.solve_linear_system()
+    assert st["status"] == 0
+    assert st["rel_residual"] <= 1.5e-4
+    err = np.linalg.norm(gls.x.cpu().numpy() - xe) / np.linalg.norm(xe)
+    assert err <= 1e-2
+
+
+def test_invalid_arguments_raise(dev):
+    from stgipc import StgError
+    solver = _solver()
+    import torch
+    x = torch.zeros(5, dtype=torch.float64, device=dev)
+    with pytest.raises(StgError):
+        solver.spmv(1.0, x, x.int(), x.int(), 1, x, 0.0, x)   # n = 5 not a multiple of 3
+    with pytest.raises(StgError):
+        solver.mas_apply(x, x)                                 # MAS not initialised
+    with pytest.raises(StgError):
+        bad = np.array([0, 1, 99], np.int32)                  # part map entry out of range
+        solver.mas_init(2, np.zeros(2), np.zeros(2), np.zeros(0), bad, np.array([0, 1]))

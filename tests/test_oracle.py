@@ -1,0 +1,189 @@
+"""CPU: the oracle against independent restatements, the reference's fixtures and invariants."""
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from conftest import GOLDEN, cube_system, fixture_system, random_contacts
+
+
+def _dense_sym(rows, cols, blocks, n):
+    """Full symmetric sparse matrix from unique upper blocks (column-major 3x3)."""
+    B = blocks.reshape(-1, 3, 3).transpose(0, 2, 1)  # row-major
+    r, c, v = [], [], []
+    for a in range(3):
+        for b in range(3):
+            r.append(3 * rows + a)
+            c.append(3 * cols + b)
+            v.append(B[:, a, b])
+            off = rows != cols
+            r.append(3 * cols[off] + b)
+            c.append(3 * rows[off] + a)
+            v.append(B[off, a, b])
+    return sp.coo_matrix((np.concatenate(v), (np.concatenate(r), np.concatenate(c))), shape=(n, n)).tocsr()
+
+
+def test_convert_matches_numpy():
+    from oracle import oracle as orc
+    s = cube_system(8)
+    r, c, b = orc.convert(s.rows, s.cols, s.blocks)
+    key = s.rows.astype(np.int64) * (1 << 32) + s.cols
+    uk, inv = np.unique(key, return_inverse=True)
+    sums = np.zeros((uk.size, 9))
+    np.add.at(sums, inv, s.blocks)
+    assert np.array_equal(r, (uk >> 32).astype(np.int32))
+    assert np.array_equal(c, (uk & 0xffffffff).astype(np.int32))
+    assert np.allclose(b, sums, rtol=1e-14, atol=0)
+
+
+def test_spmv_matches_scipy():
+    from oracle import oracle as orc
+    s = cube_system(8)
+    r, c, b = orc.convert(s.rows, s.cols, s.blocks)
+    A = _dense_sym(r, c, b, s.n)
+    x = np.random.default_rng(0).standard_normal(s.n)
+    y = orc.spmv(r, c, b, x)
+    assert np.allclose(y, A @ x, rtol=1e-12, atol=1e-12 * np.abs(A @ x).max())
+    y2 = orc.spmv(r, c, b, x, a=-2.0, b=0.5, y=np.ones(s.n))
+    assert np.allclose(y2, -2.0 * (A @ x) + 0.5, rtol=1e-12, atol=1e-12 * np.abs(A @ x).max())
+
+
+def test_system_counts_match_configs():
+    s = cube_system(16)
+    assert s.num_verts == 4913 and s.tets.shape[0] == 24576 and s.n == 14739
+    key = s.rows.astype(np.int64) * (1 << 32) + s.cols
+    assert np.unique(key).size == 35937
+    assert (s.rows <= s.cols).all()
+
+
+def test_morton_code_known_answers():
+    from stgipc import scenes
+    # interleave by hand: code = sum over bits of x<<(3i+2) | y<<(3i+1) | z<<(3i)
+    rng = np.random.default_rng(1)
+    q = rng.integers(0, 1024, size=(200, 3)).astype(np.uint32)
+    got = ((scenes.expand_bits(q[:, 0]).astype(np.uint64) << 2) + (scenes.expand_bits(q[:, 1]).astype(np.uint64) << 1)
+           + scenes.expand_bits(q[:, 2]).astype(np.uint64))
+    want = np.zeros(200, np.uint64)
+    for i in range(10):
+        for a, sh in ((0, 2), (1, 1), (2, 0)):
+            want |= ((q[:, a].astype(np.uint64) >> np.uint64(i)) & np.uint64(1)) << np.uint64(3 * i + sh)
+    assert np.array_equal(got, want)
+    assert int(scenes.expand_bits(np.array([1023], np.uint32))[0]) == 0x09249249
+
+
+def test_neighbor_lists_symmetric_and_complete():
+    s = cube_system(8)
+    V = s.num_verts
+    nb = [set(s.neighbor_list[s.neighbor_start[v]:s.neighbor_start[v] + s.neighbor_num[v]].tolist()) for v in range(V)]
+    for v in range(V):
+        for u in nb[v]:
+            assert v in nb[u]
+    edges = set()
+    for t in s.tets:
+        for a in range(4):
+            for b in range(a + 1, 4):
+                edges.add((min(t[a], t[b]), max(t[a], t[b])))
+    assert sum(len(x) for x in nb) == 2 * len(edges)
+
+
+def test_fixture_partitions_are_mas_ready():
+    """The reference's METIS fixtures: parts of <= 16 vertices, vertices grouped by part,
+    and set_mas_partition's maps are mutually inverse."""
+    from stgipc import scenes
+    for name in ("cube", "bunny2", "cloth_high"):
+        z = np.load(os.path.join(GOLDEN, f"{name}_sorted16.npz"))
+        part = z["part"]
+        assert (np.diff(part) >= 0).all()
+        assert np.bincount(part).max() <= 16
+        pm, rm = scenes.slot_maps_from_parts(part, 16)
+        assert pm.size == 16 * (part.max() + 1)
+        assert np.array_equal(pm[rm], np.arange(part.size))
+        assert (rm // 16 == part).all()
+
+
+def test_mas_hierarchy_invariants():
+    from oracle import oracle as orc
+    s, part = fixture_system("bunny2")
+    from stgipc import scenes
+    pm, rm = scenes.slot_maps_from_parts(part, 16)
+    cp = random_contacts(s.num_verts, 500, seed=2)
+    m = orc.Mas(16, s.num_verts, s.neighbor_start, s.neighbor_num, s.neighbor_list, pm, rm)
+    total = m.build(cp)
+    h = m.hierarchy()
+    L, V = m.L, s.num_verts
+    ls = h["level_size"]
+    assert ls[L, 1] == total and total % 16 == 0
+    # level sizes shrink and begins are bank aligned
+    for l in range(1, L):
+        assert ls[l + 1, 0] <= ls[l, 0]
+        assert ls[l, 1] % 16 == 0
+    # every vertex's closed mask contains its own lane; coarse ids are in range
+    lanes = rm % 16
+    assert ((h["fine_mask"] >> lanes) & 1).all()
+    for l in range(L):
+        assert (h["coarse_tables"][l] >= 0).all() and (h["coarse_tables"][l] < ls[l + 1, 0]).all()
+    # components at level 0 never span two banks
+    g1 = h["coarse_tables"][0]
+    for cid in np.unique(g1)[:200]:
+        members = np.nonzero(g1 == cid)[0]
+        assert np.unique(rm[members] // 16).size == 1
+    # the coarse table follows going_next
+    if L > 1:
+        assert np.array_equal(h["coarse_table"][:, 0], h["going_next"][:V])
+
+
+def test_mas_inverse_is_inverse():
+    from oracle import oracle as orc
+    s = cube_system(8)
+    r, c, b = orc.convert(s.rows, s.cols, s.blocks)
+    m = orc.Mas(16, s.num_verts, s.neighbor_start, s.neighbor_num, s.neighbor_list, *s.slot_maps(16))
+    m.build()
+    m.assemble(r, c, b)
+    mat, inv = m.matrices()
+
+    def dense(P, B=16):
+        N = 3 * B
+        D = np.zeros((N, N))
+        k = 0
+        for a in range(B):
+            for cc in range(a, B):
+                blk = P[k].reshape(3, 3).T  # column-major -> row-major
+                D[3 * a:3 * a + 3, 3 * cc:3 * cc + 3] = blk
+                if cc != a:
+                    D[3 * cc:3 * cc + 3, 3 * a:3 * a + 3] = blk.T
+                k += 1
+        return D
+
+    for bk in range(0, mat.shape[0], max(1, mat.shape[0] // 8)):
+        A = dense(mat[bk])
+        d = np.diag(A).copy()
+        A[np.arange(48), np.arange(48)] = np.where(d == 0, 1.0, d)
+        P = dense(inv[bk].astype(np.float64))
+        err = np.abs(P @ A - np.eye(48)).max()
+        assert err < 1e-3, (bk, err)
+
+
+def test_pcg_matches_scipy_solution():
+    from oracle import oracle as orc
+    s = cube_system(8)
+    r, c, b = orc.convert(s.rows, s.cols, s.blocks)
+    A = _dense_sym(r, c, b, s.n)
+    m = orc.Mas(16, s.num_verts, s.neighbor_start, s.neighbor_num, s.neighbor_list, *s.slot_maps(16))
+    m.build()
+    m.assemble(r, c, b)
+    x, st = orc.pcg(r, c, b, s.b, mas=m, tol=1e-12, max_iter_ratio=1.0)
+    xs = sp.linalg.spsolve(A.tocsc(), s.b)
+    assert np.linalg.norm(x - xs) <= 1e-5 * np.linalg.norm(xs)
+    assert st["rel_residual"] < 1e-5
+
+
+def test_pcg_reference_stop_rule_and_max_iter():
+    from oracle import oracle as orc
+    s = cube_system(8)
+    r, c, b = orc.convert(s.rows, s.cols, s.blocks)
+    x, st = orc.pcg(r, c, b, s.b, use_diag=True)
+    assert abs(st["rz_final"]) <= 1e-4 * st["rz0"] * 1e4  # sanity: finite
+    # a tiny max_iter_ratio stops at max_iter = (long)(ratio * n)
+    x, st = orc.pcg(r, c, b, s.b, use_diag=True, max_iter_ratio=3.0 / s.n)
+    assert st["iterations"] == 3
