@@ -21,6 +21,7 @@ namespace stg
 Solver::~Solver()
 {
     if(pcg.graph) cudaGraphExecDestroy(pcg.graph);
+    if(capture_stream) cudaStreamDestroy(capture_stream);
     for(auto& e : ev)
         if(e) cudaEventDestroy(e);
 }

@@ -16,28 +16,39 @@
 namespace stg
 {
 
-__global__ void k_conv_max_row(const int* rows, int count, int* max_row)
+// largest block index among rows and cols (the block dimension when the caller gives none)
+__global__ void k_conv_max_row(const int* rows, const int* cols, int count, int* max_row)
 {
     int m = -1;
     for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
-        m = max(m, rows[i]);
+        m = max(m, max(rows[i], cols[i]));
 #pragma unroll
     for(int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
     if((threadIdx.x & 31) == 0) atomicMax(max_row, m);
 }
 
-__global__ void k_conv_hist(const int* rows, int count, int* row_cnt)
-{
-    for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
-        atomicAdd(row_cnt + rows[i], 1);
-}
-
-__global__ void k_conv_scatter(const int* rows, int count, const int* row_start, int* cursor, int* perm)
+// Row histogram.  Triplets whose row or col lies outside [0, nrows) are counted in *bad
+// (the caller gets STG_ERR_INVALID) and never used as an index.
+__global__ void k_conv_hist(const int* rows, const int* cols, int count, int nrows, int* row_cnt, int* bad)
 {
     for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
     {
-        int r = rows[i];
-        int pos = row_start[r] + atomicAdd(cursor + r, 1);
+        const int r = rows[i], c = cols[i];
+        if(r < 0 || r >= nrows || c < 0 || c >= nrows)
+            atomicAdd(bad, 1);
+        else
+            atomicAdd(row_cnt + r, 1);
+    }
+}
+
+__global__ void k_conv_scatter(const int* rows, const int* cols, int count, int nrows, const int* row_start, int* cursor,
+                               int* perm)
+{
+    for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    {
+        const int r = rows[i], c = cols[i];
+        if(r < 0 || r >= nrows || c < 0 || c >= nrows) continue;
+        const int pos = row_start[r] + atomicAdd(cursor + r, 1);
         perm[pos] = i;
     }
 }
@@ -126,9 +137,9 @@ int Solver::convert(int count, const int* rows, const int* cols, const double* b
     int nrows = nrows_hint;
     if(nrows <= 0)
     {
-        STG_TRY(cv.scratch.resize(1));
+        STG_TRY(cv.scratch.resize(4));
         STG_CUDA_TRY(cudaMemsetAsync(cv.scratch.data(), 0xff, sizeof(int), s));
-        k_conv_max_row<<<std::min(div_up(count, 256), 1184), 256, 0, s>>>(rows, count, cv.scratch.data());
+        k_conv_max_row<<<std::min(div_up(count, 256), 1184), 256, 0, s>>>(rows, cols, count, cv.scratch.data());
         STG_LAUNCH_CHECK();
         int mr = -1;
         STG_CUDA_TRY(cudaMemcpyAsync(&mr, cv.scratch.data(), sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -151,12 +162,13 @@ int Solver::convert(int count, const int* rows, const int* cols, const double* b
 
     STG_CUDA_TRY(cudaMemsetAsync(cv.row_cnt.data(), 0, sizeof(int) * (nrows + 1), s));
     STG_CUDA_TRY(cudaMemsetAsync(cv.cursor.data(), 0, sizeof(int) * (nrows + 1), s));
+    STG_CUDA_TRY(cudaMemsetAsync(cv.scratch.data() + 2, 0, sizeof(int), s));
     const int g = std::min(div_up(count, 256), 148 * 16);
-    k_conv_hist<<<g, 256, 0, s>>>(rows, count, cv.row_cnt.data());
+    k_conv_hist<<<g, 256, 0, s>>>(rows, cols, count, nrows, cv.row_cnt.data(), cv.scratch.data() + 2);
     STG_LAUNCH_CHECK();
     k_scan_exclusive<<<1, 1024, 0, s>>>(cv.row_cnt.data(), cv.row_start.data(), nullptr, nrows + 1, cv.scratch.data());
     STG_LAUNCH_CHECK();
-    k_conv_scatter<<<g, 256, 0, s>>>(rows, count, cv.row_start.data(), cv.cursor.data(), cv.perm.data());
+    k_conv_scatter<<<g, 256, 0, s>>>(rows, cols, count, nrows, cv.row_start.data(), cv.cursor.data(), cv.perm.data());
     STG_LAUNCH_CHECK();
     const int gw = std::min(div_up((long)nrows * 32, 256), 148 * 16);
     k_conv_sort_rows<<<gw, 256, 0, s>>>(cols, cv.row_start.data(), cv.perm.data(), cv.perm2.data(), cv.scol.data(),
@@ -169,9 +181,17 @@ int Solver::convert(int count, const int* rows, const int* cols, const double* b
                                    bcoo.rows.data(), bcoo.cols.data(), bcoo.blocks.data(), nrows);
     STG_LAUNCH_CHECK();
     launches += 6;
-    int total = 0;
-    STG_CUDA_TRY(cudaMemcpyAsync(&total, cv.scratch.data() + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    int h[2] = {0, 0};
+    STG_CUDA_TRY(cudaMemcpyAsync(h, cv.scratch.data() + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     STG_CUDA_TRY(cudaStreamSynchronize(s));
+    if(h[1] != 0)
+    {
+        set_error("convert: " + std::to_string(h[1]) + " triplets have a row or col outside [0, " +
+                  std::to_string(nrows) + ")");
+        bcoo.nnzb = 0;
+        return STG_ERR_INVALID;
+    }
+    const int total = h[0];
     bcoo.nnzb = total;
     bcoo.nrows = nrows;
     bcoo.external = false;

@@ -729,7 +729,7 @@ int Solver::mas_init(int V, int node_offset, const uint32_t* ns, const uint32_t*
     STG_TRY(m.next_prefix.resize(V / B + 2));
     STG_TRY(m.next_prefix_sum.resize(V / B + 2));
     STG_TRY(m.coarse_tables.resize((size_t)L * V));
-    m.gn_size = L * V + pms + B;
+    m.gn_size = pms + L * (V + B);  // >= total clusters: level l >= 1 holds <= V nodes, rounded to B
     STG_TRY(m.going_next.resize(m.gn_size));
     STG_TRY(m.closed.resize(m.gn_size));
     STG_TRY(m.coarse_table.resize((size_t)V * std::max(L - 1, 1)));

@@ -465,15 +465,29 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
                 cudaGraphExecDestroy(P.graph);
                 P.graph = nullptr;
             }
+            // the legacy default stream cannot be captured: record the kernels on a private
+            // stream; the instantiated graph is then launched on the caller's stream
+            if(!capture_stream) STG_CUDA_TRY(cudaStreamCreateWithFlags(&capture_stream, cudaStreamNonBlocking));
             cudaGraph_t g = nullptr;
-            STG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            stream = capture_stream;
+            cudaError_t cb = cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal);
+            if(cb != cudaSuccess)
+            {
+                stream = s;
+                STG_CUDA_TRY(cb);
+            }
             int rc = 0;
             const int l0 = launches;
             for(int it = 0; it < batch && rc == 0; it++) rc = launch_iteration(L);
-            cudaError_t ce = cudaStreamEndCapture(s, &g);
+            cudaError_t ce = cudaStreamEndCapture(capture_stream, &g);
+            stream = s;
             launches_per_batch = launches - l0;
             launches = l0;
-            if(rc) return rc;
+            if(rc)
+            {
+                if(g) cudaGraphDestroy(g);
+                return rc;
+            }
             STG_CUDA_TRY(ce);
             STG_CUDA_TRY(cudaGraphInstantiate(&P.graph, g, 0));
             cudaGraphDestroy(g);

@@ -103,6 +103,7 @@ struct Solver
 {
     stg_config cfg{};
     cudaStream_t stream = nullptr;
+    cudaStream_t capture_stream = nullptr;  // private stream used only to record graphs
     int launches = 0;
     Bcoo bcoo;
     ConvertScratch cv;

@@ -22,6 +22,48 @@ namespace stg
 // ---------------------------------------------------------------------------------------
 // structure preparation
 // ---------------------------------------------------------------------------------------
+// Caller-provided BCOO must be sorted by (row, col), unique, upper (row <= col) and inside
+// [0, nrows) when nrows > 0 (the converter's output contract); counts violations.
+__global__ void k_bcoo_validate(const int* rows, const int* cols, int nnzb, int nrows, int* bad)
+{
+    int cnt = 0;
+    for(int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnzb; k += gridDim.x * blockDim.x)
+    {
+        const int r = rows[k], c = cols[k];
+        bool ok = r >= 0 && c >= r && (nrows <= 0 || c < nrows);
+        if(k > 0)
+        {
+            const int rp = rows[k - 1], cp = cols[k - 1];
+            ok = ok && (rp < r || (rp == r && cp < c));
+        }
+        cnt += !ok;
+    }
+    if(cnt) atomicAdd(bad, cnt);
+}
+
+int validate_bcoo(Solver& S)
+{
+    const int nnzb = S.bcoo.nnzb;
+    if(nnzb < 1) return 0;
+    STG_TRY(S.cv.scratch.resize(4));
+    int* bad = S.cv.scratch.data() + 3;
+    STG_CUDA_TRY(cudaMemsetAsync(bad, 0, sizeof(int), S.stream));
+    k_bcoo_validate<<<std::max(1, std::min(div_up(nnzb, 256), kSMs * 8)), 256, 0, S.stream>>>(S.bcoo.R(), S.bcoo.C(), nnzb,
+                                                                                            S.bcoo.nrows, bad);
+    STG_LAUNCH_CHECK();
+    S.launches++;
+    int h = 0;
+    STG_CUDA_TRY(cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, S.stream));
+    STG_CUDA_TRY(cudaStreamSynchronize(S.stream));
+    if(h)
+    {
+        set_error("BCOO input: " + std::to_string(h) +
+                  " entries are out of range, lower-triangular, unsorted or duplicated (run stg_convert first)");
+        return STG_ERR_INVALID;
+    }
+    return 0;
+}
+
 __global__ void k_row_ptr(const int* rows, int nnzb, int nrows, int* row_ptr)
 {
     for(int k = blockIdx.x * blockDim.x + threadIdx.x; k <= nnzb; k += gridDim.x * blockDim.x)
@@ -110,7 +152,7 @@ int Solver::bind_bcoo(const double* blocks, const int* rows, const int* cols, in
     bcoo.nnzb = nnzb;
     bcoo.nrows = nrows;
     bcoo.row_ptr_valid = false;
-    return 0;
+    return validate_bcoo(*this);
 }
 
 int Solver::prepare_spmv()
