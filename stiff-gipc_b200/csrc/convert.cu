@@ -29,11 +29,13 @@ __global__ void k_conv_max_row(const int* rows, const int* cols, int count, int*
 
 // Row histogram.  Triplets whose row or col lies outside [0, nrows) are counted in *bad
 // (the caller gets STG_ERR_INVALID) and never used as an index.
-__global__ void k_conv_hist(const int* rows, const int* cols, int count, int nrows, int* row_cnt, int* bad)
+__global__ void k_conv_hist(const int* rows, const int* cols, int count, int nrows, bool skip_negative, int* row_cnt,
+                            int* bad)
 {
     for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
     {
         const int r = rows[i], c = cols[i];
+        if(skip_negative && r < 0) continue;
         if(r < 0 || r >= nrows || c < 0 || c >= nrows)
             atomicAdd(bad, 1);
         else
@@ -126,14 +128,73 @@ __global__ void k_conv_emit(const double* blocks, const int* row_start, const in
     }
 }
 
+// Sort/merge `count` triplets into unique (row, col) blocks written to out_* (row_ptr gets the
+// CSR offsets).  Triplets with row < 0 are skipped when skip_negative is set (used to mask
+// entries); any other row or col outside [0, nrows) is an error.  Returns the unique count
+// through *unique (one device->host read).
+int convert_into(Solver& S, ConvertScratch& cv, int count, const int* rows, const int* cols, const double* blocks,
+                 int nrows, bool skip_negative, DBuf<int>& out_rows, DBuf<int>& out_cols, DBuf<double>& out_blocks,
+                 DBuf<int>& row_ptr, int* unique)
+{
+    cudaStream_t s = S.stream;
+    *unique = 0;
+    STG_TRY(row_ptr.resize(nrows + 1));
+    STG_TRY(cv.scratch.resize(4));
+    if(count < 1 || nrows < 1)
+    {
+        STG_CUDA_TRY(cudaMemsetAsync(row_ptr.data(), 0, sizeof(int) * (nrows + 1), s));
+        return 0;
+    }
+    STG_TRY(cv.row_cnt.resize(nrows + 1));
+    STG_TRY(cv.row_start.resize(nrows + 1));
+    STG_TRY(cv.cursor.resize(nrows + 1));
+    STG_TRY(cv.perm.resize(count));
+    STG_TRY(cv.perm2.resize(count));
+    STG_TRY(cv.scol.resize(count));
+    STG_TRY(cv.uniq.resize(nrows + 1));
+    STG_TRY(out_rows.resize(count));
+    STG_TRY(out_cols.resize(count));
+    STG_TRY(out_blocks.resize((size_t)count * 9));
+
+    STG_CUDA_TRY(cudaMemsetAsync(cv.row_cnt.data(), 0, sizeof(int) * (nrows + 1), s));
+    STG_CUDA_TRY(cudaMemsetAsync(cv.cursor.data(), 0, sizeof(int) * (nrows + 1), s));
+    STG_CUDA_TRY(cudaMemsetAsync(cv.scratch.data() + 2, 0, sizeof(int), s));
+    const int g = std::min(div_up(count, 256), kSMs * 16);
+    k_conv_hist<<<g, 256, 0, s>>>(rows, cols, count, nrows, skip_negative, cv.row_cnt.data(), cv.scratch.data() + 2);
+    STG_LAUNCH_CHECK();
+    k_scan_exclusive<<<1, 1024, 0, s>>>(cv.row_cnt.data(), cv.row_start.data(), nullptr, nrows + 1, cv.scratch.data());
+    STG_LAUNCH_CHECK();
+    k_conv_scatter<<<g, 256, 0, s>>>(rows, cols, count, nrows, cv.row_start.data(), cv.cursor.data(), cv.perm.data());
+    STG_LAUNCH_CHECK();
+    const int gw = std::min(div_up((long)nrows * 32, 256), kSMs * 16);
+    k_conv_sort_rows<<<gw, 256, 0, s>>>(cols, cv.row_start.data(), cv.perm.data(), cv.perm2.data(), cv.scol.data(),
+                                        cv.uniq.data(), nrows);
+    STG_LAUNCH_CHECK();
+    STG_CUDA_TRY(cudaMemsetAsync(cv.uniq.data() + nrows, 0, sizeof(int), s));
+    k_scan_exclusive<<<1, 1024, 0, s>>>(cv.uniq.data(), row_ptr.data(), nullptr, nrows + 1, cv.scratch.data() + 1);
+    STG_LAUNCH_CHECK();
+    k_conv_emit<<<gw, 256, 0, s>>>(blocks, cv.row_start.data(), cv.perm2.data(), cv.scol.data(), row_ptr.data(),
+                                   out_rows.data(), out_cols.data(), out_blocks.data(), nrows);
+    STG_LAUNCH_CHECK();
+    S.launches += 6;
+    int h[2] = {0, 0};
+    STG_CUDA_TRY(cudaMemcpyAsync(h, cv.scratch.data() + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    STG_CUDA_TRY(cudaStreamSynchronize(s));
+    if(h[1] != 0)
+    {
+        set_error("convert: " + std::to_string(h[1]) + " triplets have a row or col outside [0, " + std::to_string(nrows) +
+                  ")");
+        return STG_ERR_INVALID;
+    }
+    *unique = h[0];
+    return 0;
+}
+
 int Solver::convert(int count, const int* rows, const int* cols, const double* blocks, int nrows_hint)
 {
     cudaStream_t s = stream;
-    if(count < 1)
-    {
-        bcoo.nnzb = 0;
-        return 0;
-    }
+    bcoo.nnzb = 0;
+    if(count < 1) return 0;
     int nrows = nrows_hint;
     if(nrows <= 0)
     {
@@ -147,51 +208,9 @@ int Solver::convert(int count, const int* rows, const int* cols, const double* b
         nrows = mr + 1;
         launches += 1;
     }
-    STG_TRY(cv.row_cnt.resize(nrows + 1));
-    STG_TRY(cv.row_start.resize(nrows + 1));
-    STG_TRY(cv.cursor.resize(nrows + 1));
-    STG_TRY(cv.perm.resize(count));
-    STG_TRY(cv.perm2.resize(count));
-    STG_TRY(cv.scol.resize(count));
-    STG_TRY(cv.uniq.resize(nrows + 1));
-    STG_TRY(bcoo.row_ptr.resize(nrows + 1));
-    STG_TRY(bcoo.rows.resize(count));
-    STG_TRY(bcoo.cols.resize(count));
-    STG_TRY(bcoo.blocks.resize((size_t)count * 9));
-    STG_TRY(cv.scratch.resize(4));
-
-    STG_CUDA_TRY(cudaMemsetAsync(cv.row_cnt.data(), 0, sizeof(int) * (nrows + 1), s));
-    STG_CUDA_TRY(cudaMemsetAsync(cv.cursor.data(), 0, sizeof(int) * (nrows + 1), s));
-    STG_CUDA_TRY(cudaMemsetAsync(cv.scratch.data() + 2, 0, sizeof(int), s));
-    const int g = std::min(div_up(count, 256), 148 * 16);
-    k_conv_hist<<<g, 256, 0, s>>>(rows, cols, count, nrows, cv.row_cnt.data(), cv.scratch.data() + 2);
-    STG_LAUNCH_CHECK();
-    k_scan_exclusive<<<1, 1024, 0, s>>>(cv.row_cnt.data(), cv.row_start.data(), nullptr, nrows + 1, cv.scratch.data());
-    STG_LAUNCH_CHECK();
-    k_conv_scatter<<<g, 256, 0, s>>>(rows, cols, count, nrows, cv.row_start.data(), cv.cursor.data(), cv.perm.data());
-    STG_LAUNCH_CHECK();
-    const int gw = std::min(div_up((long)nrows * 32, 256), 148 * 16);
-    k_conv_sort_rows<<<gw, 256, 0, s>>>(cols, cv.row_start.data(), cv.perm.data(), cv.perm2.data(), cv.scol.data(),
-                                        cv.uniq.data(), nrows);
-    STG_LAUNCH_CHECK();
-    STG_CUDA_TRY(cudaMemsetAsync(cv.uniq.data() + nrows, 0, sizeof(int), s));
-    k_scan_exclusive<<<1, 1024, 0, s>>>(cv.uniq.data(), bcoo.row_ptr.data(), nullptr, nrows + 1, cv.scratch.data() + 1);
-    STG_LAUNCH_CHECK();
-    k_conv_emit<<<gw, 256, 0, s>>>(blocks, cv.row_start.data(), cv.perm2.data(), cv.scol.data(), bcoo.row_ptr.data(),
-                                   bcoo.rows.data(), bcoo.cols.data(), bcoo.blocks.data(), nrows);
-    STG_LAUNCH_CHECK();
-    launches += 6;
-    int h[2] = {0, 0};
-    STG_CUDA_TRY(cudaMemcpyAsync(h, cv.scratch.data() + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
-    STG_CUDA_TRY(cudaStreamSynchronize(s));
-    if(h[1] != 0)
-    {
-        set_error("convert: " + std::to_string(h[1]) + " triplets have a row or col outside [0, " +
-                  std::to_string(nrows) + ")");
-        bcoo.nnzb = 0;
-        return STG_ERR_INVALID;
-    }
-    const int total = h[0];
+    int total = 0;
+    STG_TRY(convert_into(*this, cv, count, rows, cols, blocks, nrows, false, bcoo.rows, bcoo.cols, bcoo.blocks,
+                         bcoo.row_ptr, &total));
     bcoo.nnzb = total;
     bcoo.nrows = nrows;
     bcoo.external = false;

@@ -16,7 +16,8 @@
 //     atomicOr on the node mask (OR is order independent);
 //   * component leaders and counts use ballots instead of racy shared atomics.
 // Restriction sums are computed per bank in lane order (deterministic) instead of float
-// atomics; the coarse-level Galerkin accumulation uses FP64 atomics like the reference.
+// atomics, and the coarse-level Galerkin blocks are formed level by level with the
+// deterministic sort/merge of convert.cu instead of FP64 atomics (see the assembly section).
 #include "solver.hpp"
 
 namespace stg
@@ -301,135 +302,123 @@ __global__ void k_set_level1(int* ls, const int* total, int M)
 // ---------------------------------------------------------------------------------------
 // assembly (PrepareHessian_bcoo) and inverse
 // ---------------------------------------------------------------------------------------
-__device__ __forceinline__ void atomic_add_block(double* D, const double* H, bool transpose, bool both)
-{
-#pragma unroll
-    for(int i = 0; i < 3; i++)
-#pragma unroll
-        for(int j = 0; j < 3; j++)
-        {
-            // column-major element (i,j) at [j*3+i]
-            double v = transpose ? H[i * 3 + j] : H[j * 3 + i];
-            if(both) v += H[i * 3 + j];
-            atomicAdd(D + j * 3 + i, v);
-        }
-}
+// PrepareHessian_bcoo (MASPreconditioner.cu:1829-2075) accumulates, for every level l, the
+// bank-diagonal blocks of the Galerkin operator P_l^T A P_l: block (a, b) of a level-l bank
+// is the sum of A(u, v) over all fine pairs with coarse_l(u) = a, coarse_l(v) = b.  The
+// reference walks every BCOO entry and every in-bank level-0 pair up the levels with FP64
+// atomics, which serialise on the few coarse blocks every pair reaches.  Here the same sums
+// are formed level by level: A_1 = aggregate(A_0), A_{l+1} = aggregate(A_l) (aggregate =
+// map both indices to the coarse node and merge duplicates with the deterministic sorter of
+// convert.cu), and each level's bank blocks are read off A_l.  Level-0 in-bank entries with
+// slot(col) < slot(row) are not stored by the reference (lambda 1 only stores col >= row
+// slots, and lambda 2 propagates the stored bank matrix); they are left out here too.
 
-// lambda 1 of PrepareHessian_bcoo (MASPreconditioner.cu:1849-1944), one thread per BCOO entry
-// of the FEM range.
+// level-0 bank blocks (lambda 1, level-0 branch): direct stores, entries are unique
 template <int B>
-__global__ void k_mas_scatter_bcoo(const int* __restrict__ rows, const int* __restrict__ cols,
-                                   const double* __restrict__ blocks, int nnzb, int offset, int V,
-                                   const int* __restrict__ real_map, const int* __restrict__ going_next, int L,
-                                   double* mat)
+__global__ void k_mas_store_l0(const int* __restrict__ rows, const int* __restrict__ cols,
+                               const double* __restrict__ blocks, int nnzb, int offset, int V,
+                               const int* __restrict__ real_map, double* mat)
 {
     const int NS = nsym(B);
     for(int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnzb; k += gridDim.x * blockDim.x)
     {
         const int rr = rows[k] - offset, cc = cols[k] - offset;
         if(rr < 0 || rr >= V || cc < 0 || cc >= V) continue;
-        const double* H = blocks + 9 * (size_t)k;
         const int sc = real_map[cc], sr = real_map[rr];
-        if(sc / B == sr / B)
-        {
-            if(sc >= sr)
-            {
-                double* D = mat + ((size_t)(sc / B) * NS + upper_index(B, sr % B, sc % B)) * 9;
+        if(sc / B != sr / B || sc < sr) continue;
+        const double* H = blocks + 9 * (size_t)k;
+        double* D = mat + ((size_t)(sc / B) * NS + upper_index(B, sr % B, sc % B)) * 9;
 #pragma unroll
-                for(int e = 0; e < 9; e++) D[e] = H[e];
-            }
-            continue;
-        }
-        int gc = cc, gr = rr;
-        for(int level = 1; level < L; level++)
-        {
-            gc = going_next[gc];
-            gr = going_next[gr];
-            if(gc / B != gr / B) continue;
-            if(gc >= gr)
-                atomic_add_block(mat + ((size_t)(gc / B) * NS + upper_index(B, gr % B, gc % B)) * 9, H, false, gc == gr);
-            else
-                atomic_add_block(mat + ((size_t)(gc / B) * NS + upper_index(B, gc % B, gr % B)) * 9, H, true, false);
-        }
+        for(int e = 0; e < 9; e++) D[e] = H[e];
     }
 }
 
-// lambda 2 of PrepareHessian_bcoo (MASPreconditioner.cu:1946-2075): level-0 bank blocks added
-// into the coarse levels.  One CTA per level-0 bank, B*B threads (row lane, col lane).
-template <int B>
-__global__ void __launch_bounds__(B * B) k_mas_scatter_l0(const int* __restrict__ part_map, const int* __restrict__ prefix_orig,
-                                                          const int* __restrict__ going_next, int L, double* mat)
+// Map an upper block (u <= v) with value H to coarse nodes (a, b) and orient it upper:
+// a < b: H; a > b: H^T at (b, a); a == b: H (u == v) or H + H^T (u < v).
+__device__ __forceinline__ void coarse_triplet(int u, int v, int a, int b, const double* __restrict__ H, int* orow,
+                                               int* ocol, double* oblk)
 {
-    const int NS = nsym(B);
-    __shared__ double red[B * B / 32][9];
-    const int bank = blockIdx.x;
-    const int LR = threadIdx.x / B, LC = threadIdx.x % B;
-    int rdx = part_map[bank * B + LR], cdx = part_map[bank * B + LC];
-    const bool real = rdx >= 0 && cdx >= 0;
-    double m3[9];
-    if(LC >= LR)
-    {
-        const double* S = mat + ((size_t)bank * NS + upper_index(B, LR, LC)) * 9;
+    double h[9];
 #pragma unroll
-        for(int e = 0; e < 9; e++) m3[e] = S[e];
-    }
-    else
+    for(int e = 0; e < 9; e++) h[e] = H[e];
+    if(a < b || (a == b && u == v))
     {
-        const double* S = mat + ((size_t)bank * NS + upper_index(B, LC, LR)) * 9;
+#pragma unroll
+        for(int e = 0; e < 9; e++) oblk[e] = h[e];
+    }
+    else if(a > b)
+    {
 #pragma unroll
         for(int i = 0; i < 3; i++)
 #pragma unroll
-            for(int j = 0; j < 3; j++) m3[j * 3 + i] = S[i * 3 + j];
+            for(int j = 0; j < 3; j++) oblk[j * 3 + i] = h[i * 3 + j];
+        const int t = a;
+        a = b;
+        b = t;
     }
-    if(prefix_orig[bank] == 1)
+    else
     {
-        // the whole bank is one component: sum all real pairs (fixed tree order), add once
-        // to the single coarse node's diagonal block at every coarser level
 #pragma unroll
-        for(int e = 0; e < 9; e++)
-        {
-            double v = real ? m3[e] : 0.0;
-            v = warp_sum(v);
-            if((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][e] = v;
-        }
-        __syncthreads();
-        if(threadIdx.x == 0)
-        {
-            double S[9];
+        for(int i = 0; i < 3; i++)
 #pragma unroll
-            for(int e = 0; e < 9; e++)
-            {
-                double a = 0;
-                for(int w = 0; w < B * B / 32; w++) a += red[w][e];
-                S[e] = a;
-            }
-            int lead = -1;
-            for(int l = 0; l < B && lead < 0; l++) lead = part_map[bank * B + l];
-            if(lead >= 0)
-            {
-                int nid = going_next[lead];
-                for(int level = 1; level < L; level++)
-                {
-                    double* D = mat + ((size_t)(nid / B) * NS + upper_index(B, nid % B, nid % B)) * 9;
-#pragma unroll
-                    for(int e = 0; e < 9; e++) atomicAdd(D + e, S[e]);
-                    nid = going_next[nid];
-                }
-            }
-        }
-        return;
+            for(int j = 0; j < 3; j++) oblk[j * 3 + i] = h[j * 3 + i] + h[i * 3 + j];
     }
-    if(!real) return;
-    for(int level = 1; level < L; level++)
+    *orow = a;
+    *ocol = b;
+}
+
+// A_0 (FEM range of the BCOO) -> level-1 triplets; masked entries get row -1
+template <int B>
+__global__ void k_mas_agg_l0(const int* __restrict__ rows, const int* __restrict__ cols, const double* __restrict__ blocks,
+                             int nnzb, int offset, int V, const int* __restrict__ real_map, const int* __restrict__ c1,
+                             int* orow, int* ocol, double* oblk)
+{
+    for(int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnzb; k += gridDim.x * blockDim.x)
     {
-        rdx = going_next[rdx];
-        cdx = going_next[cdx];
-        if(rdx / B == cdx / B && cdx >= rdx)
+        const int rr = rows[k] - offset, cc = cols[k] - offset;
+        bool use = rr >= 0 && rr < V && cc >= 0 && cc < V;
+        if(use)
         {
-            double* D = mat + ((size_t)(cdx / B) * NS + upper_index(B, rdx % B, cdx % B)) * 9;
-#pragma unroll
-            for(int e = 0; e < 9; e++) atomicAdd(D + e, m3[e]);
+            const int sc = real_map[cc], sr = real_map[rr];
+            use = !(sc / B == sr / B && sc < sr);
         }
+        if(!use)
+        {
+            orow[k] = -1;
+            ocol[k] = 0;
+            continue;
+        }
+        coarse_triplet(rr, cc, c1[rr], c1[cc], blocks + 9 * (size_t)k, orow + k, ocol + k, oblk + 9 * (size_t)k);
+    }
+}
+
+// A_l -> level-(l+1) triplets through going_next (global ids) of level-l nodes
+__global__ void k_mas_agg_lx(const int* __restrict__ rows, const int* __restrict__ cols, const double* __restrict__ blocks,
+                             int nnz, const int* __restrict__ going_next, int begin, int begin_next, int* orow, int* ocol,
+                             double* oblk)
+{
+    for(int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += gridDim.x * blockDim.x)
+    {
+        const int u = rows[k], v = cols[k];
+        coarse_triplet(u, v, going_next[begin + u] - begin_next, going_next[begin + v] - begin_next,
+                       blocks + 9 * (size_t)k, orow + k, ocol + k, oblk + 9 * (size_t)k);
+    }
+}
+
+// bank-diagonal blocks of A_l (level-local ids, upper) into the packed bank matrices
+template <int B>
+__global__ void k_mas_extract(const int* __restrict__ rows, const int* __restrict__ cols, const double* __restrict__ blocks,
+                              int nnz, int begin, double* mat)
+{
+    const int NS = nsym(B);
+    for(int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += gridDim.x * blockDim.x)
+    {
+        const int ga = begin + rows[k], gb = begin + cols[k];
+        if(ga / B != gb / B) continue;
+        double* D = mat + ((size_t)(ga / B) * NS + upper_index(B, ga % B, gb % B)) * 9;
+        const double* H = blocks + 9 * (size_t)k;
+#pragma unroll
+        for(int e = 0; e < 9; e++) D[e] = H[e];
     }
 }
 
@@ -838,6 +827,10 @@ int Solver::mas_build(const int* contacts, int ncp)
     return mas_build_t<16>(*this, contacts, ncp);
 }
 
+int convert_into(Solver& S, ConvertScratch& cv, int count, const int* rows, const int* cols, const double* blocks,
+                 int nrows, bool skip_negative, DBuf<int>& out_rows, DBuf<int>& out_cols, DBuf<double>& out_blocks,
+                 DBuf<int>& row_ptr, int* unique);
+
 template <int B>
 static int mas_assemble_t(Solver& S, int offset)
 {
@@ -852,19 +845,59 @@ static int mas_assemble_t(Solver& S, int offset)
     STG_CUDA_TRY(cudaMemsetAsync(m.mat.data(), 0, nvals * sizeof(double), s));
     STG_CUDA_TRY(cudaMemsetAsync(m.R.data(), 0, sizeof(float) * 3 * m.total_clusters, s));
     const int nnzb = S.bcoo.nnzb;
+    const int g = std::max(1, std::min(div_up(nnzb, 256), kSMs * 16));
     if(nnzb > 0)
     {
-        k_mas_scatter_bcoo<B><<<std::min(div_up(nnzb, 256), kSMs * 16), 256, 0, s>>>(
-            S.bcoo.R(), S.bcoo.C(), S.bcoo.B(), nnzb, offset, m.V, m.real_map.data(), m.going_next.data(), m.L, m.mat.data());
+        k_mas_store_l0<B><<<g, 256, 0, s>>>(S.bcoo.R(), S.bcoo.C(), S.bcoo.B(), nnzb, offset, m.V, m.real_map.data(),
+                                            m.mat.data());
         STG_LAUNCH_CHECK();
         S.launches++;
     }
-    if(m.L > 1)
+    if(m.L > 1 && nnzb > 0)
     {
-        k_mas_scatter_l0<B><<<m.nb0, B * B, 0, s>>>(m.part_map.data(), m.prefix_orig.data(), m.going_next.data(), m.L,
-                                                    m.mat.data());
+        // level 1 from the fine matrix
+        STG_TRY(m.tr_rows.resize(nnzb));
+        STG_TRY(m.tr_cols.resize(nnzb));
+        STG_TRY(m.tr_blocks.resize((size_t)nnzb * 9));
+        k_mas_agg_l0<B><<<g, 256, 0, s>>>(S.bcoo.R(), S.bcoo.C(), S.bcoo.B(), nnzb, offset, m.V, m.real_map.data(),
+                                          m.coarse_tables.data(), m.tr_rows.data(), m.tr_cols.data(), m.tr_blocks.data());
         STG_LAUNCH_CHECK();
         S.launches++;
+        int nnz = 0;
+        STG_TRY(convert_into(S, m.gcv, nnzb, m.tr_rows.data(), m.tr_cols.data(), m.tr_blocks.data(), m.level_size[2],
+                             true, m.ga_rows, m.ga_cols, m.ga_blocks, m.g_rowptr, &nnz));
+        for(int level = 1;; level++)
+        {
+            const int begin = m.level_size[2 * level + 1];
+            if(nnz > 0)
+            {
+                k_mas_extract<B><<<std::max(1, std::min(div_up(nnz, 256), kSMs * 16)), 256, 0, s>>>(
+                    m.ga_rows.data(), m.ga_cols.data(), m.ga_blocks.data(), nnz, begin, m.mat.data());
+                STG_LAUNCH_CHECK();
+                S.launches++;
+            }
+            if(level + 1 >= m.L || nnz == 0) break;
+            const int begin_next = m.level_size[2 * (level + 1) + 1];
+            STG_TRY(m.tr_rows.resize(nnz));
+            STG_TRY(m.tr_cols.resize(nnz));
+            STG_TRY(m.tr_blocks.resize((size_t)nnz * 9));
+            k_mas_agg_lx<<<std::max(1, std::min(div_up(nnz, 256), kSMs * 16)), 256, 0, s>>>(
+                m.ga_rows.data(), m.ga_cols.data(), m.ga_blocks.data(), nnz, m.going_next.data(), begin, begin_next,
+                m.tr_rows.data(), m.tr_cols.data(), m.tr_blocks.data());
+            STG_LAUNCH_CHECK();
+            S.launches++;
+            int nnz2 = 0;
+            STG_TRY(convert_into(S, m.gcv, nnz, m.tr_rows.data(), m.tr_cols.data(), m.tr_blocks.data(),
+                                 m.level_size[2 * (level + 1)], false, m.gb_rows, m.gb_cols, m.gb_blocks, m.g_rowptr,
+                                 &nnz2));
+            std::swap(m.ga_rows.ptr, m.gb_rows.ptr);
+            std::swap(m.ga_rows.cap, m.gb_rows.cap);
+            std::swap(m.ga_cols.ptr, m.gb_cols.ptr);
+            std::swap(m.ga_cols.cap, m.gb_cols.cap);
+            std::swap(m.ga_blocks.ptr, m.gb_blocks.ptr);
+            std::swap(m.ga_blocks.cap, m.gb_blocks.cap);
+            nnz = nnz2;
+        }
     }
     const size_t smem = sizeof(double) * (3 * B * 3 * B + 3 * B);
     if(smem > 48 * 1024)

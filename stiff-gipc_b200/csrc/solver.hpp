@@ -68,6 +68,10 @@ struct MasState
     DBuf<double> mat;             // [nbanks * NS * 9]
     DBuf<float> inv;              // [nbanks * NS * 9]
     DBuf<float> R, Z;             // [total_clusters * 3]
+    // Galerkin assembly: coarse triplets and the current / next level operator (upper BCOO)
+    ConvertScratch gcv;
+    DBuf<int> tr_rows, tr_cols, ga_rows, ga_cols, gb_rows, gb_cols, g_rowptr;
+    DBuf<double> tr_blocks, ga_blocks, gb_blocks;
 };
 
 struct PcgState

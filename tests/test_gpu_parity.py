@@ -4,7 +4,8 @@ Tolerances:
   * integer work (convert indices, MAS masks / coarse ids / tables): bit-exact;
   * convert block sums: bit-exact (both sum duplicates in input order);
   * FP64 SpMV: 1e-13 relative (different summation order);
-  * MAS Galerkin matrices (FP64 atomics at coarse levels): 1e-12 relative;
+  * MAS Galerkin matrices (coarse levels summed in a different order than the oracle's
+    direct walk): 1e-11 relative to each bank's largest entry;
   * MAS FP32 inverses and apply: 2e-5 relative to the bank's / vector's max magnitude;
   * PCG, all-FP64 preconditioner (block Jacobi): x within 1e-8 relative of the oracle;
   * PCG with MAS (FP32 apply, as the reference): same iteration count +-2 and x within
@@ -160,7 +161,7 @@ def test_mas_matrices_and_inverse(dev, bank):
     gm, gi = solver.export_matrices()
     assert gm.shape == em.shape
     scale = np.abs(em).max(axis=(1, 2), keepdims=True) + 1e-300
-    assert np.max(np.abs(gm - em) / scale) <= 1e-12
+    assert np.max(np.abs(gm - em) / scale) <= 1e-11
     iscale = np.abs(ei).max(axis=(1, 2), keepdims=True) + 1e-30
     assert np.max(np.abs(gi - ei) / iscale) <= 2e-5
 
