@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--bank", type=int, default=16)
     ap.add_argument("--refine", type=int, default=32)
     ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--loop", choices=["host", "graph", "persistent"], default="graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     return ap.parse_args()
@@ -207,7 +208,7 @@ def main():
 
     def make(precision):
         cfg = PCGSolverConfig(bank_size=args.bank, precision=precision, stop_rule="relative_residual",
-                              global_tol_rate=1e-4, refine_interval=args.refine, loop="graph",
+                              global_tol_rate=1e-4, refine_interval=args.refine, loop=args.loop,
                               graph_batch=args.batch, max_iter_ratio=0.3)
         s = Solver(cfg, stream=stream)
         s.mas_init(sysm.num_verts, sysm.neighbor_start, sysm.neighbor_num, sysm.neighbor_list, pm, rm)
@@ -321,7 +322,7 @@ def main():
             "vs_baseline": None, "dtype": "f32 (FP64 dots, FP64 residual replacement)", "data": "synthetic",
             "config": {"workload": args.workload, "desc": desc, "dof": sysm.n, "nnzb": st_fast["nnzb"],
                        "triplets": int(sysm.rows.size), "bank": args.bank, "ordering": "Morton",
-                       "stop": "||b-Ax||/||b|| <= 1e-4", "refine_interval": args.refine, "graph_batch": args.batch,
+                       "stop": "||b-Ax||/||b|| <= 1e-4", "refine_interval": args.refine, "loop": args.loop,
                        "l2": "inputs larger than L2 (triplets 540 MB); no flush",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "iterations": st_fast["iterations"], "rel_residual": st_fast["rel_residual"],

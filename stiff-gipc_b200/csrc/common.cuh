@@ -94,6 +94,42 @@ __device__ __forceinline__ unsigned lanemask_lt(int lane)
     return lane >= 32 ? 0xffffffffu : ((1u << lane) - 1u);
 }
 
+// Value of lane `bb` of this lane's group of B lanes, as a full-width shuffle with an explicit
+// source lane.  With CUDA 12.9 for sm_100a, a fully unrolled loop of width-B shuffles inside a
+// grid-stride loop made ptxas abort with a register-allocation error in some kernels; this
+// form (plus partial unrolling where the abort persisted) compiles.
+template <int B>
+__device__ __forceinline__ float group_shfl(float v, int bb)
+{
+    return __shfl_sync(0xffffffffu, v, ((threadIdx.x & 31) & ~(B - 1)) + bb);
+}
+
+// 4-wide per-node vector slots {v0 v1 v2 0}: one 16-byte access (FP32) or two (FP64)
+__device__ __forceinline__ void ld4(const float* p, float& a, float& b, float& c)
+{
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    a = v.x;
+    b = v.y;
+    c = v.z;
+}
+__device__ __forceinline__ void ld4(const double* p, double& a, double& b, double& c)
+{
+    const double2 v0 = *reinterpret_cast<const double2*>(p);
+    const double2 v1 = *reinterpret_cast<const double2*>(p + 2);
+    a = v0.x;
+    b = v0.y;
+    c = v1.x;
+}
+__device__ __forceinline__ void st4(float* p, float a, float b, float c)
+{
+    *reinterpret_cast<float4*>(p) = make_float4(a, b, c, 0.f);
+}
+__device__ __forceinline__ void st4(double* p, double a, double b, double c)
+{
+    *reinterpret_cast<double2*>(p) = make_double2(a, b);
+    *reinterpret_cast<double2*>(p + 2) = make_double2(c, 0.0);
+}
+
 __device__ __forceinline__ double warp_sum(double v)
 {
 #pragma unroll

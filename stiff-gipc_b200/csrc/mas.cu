@@ -502,19 +502,14 @@ __global__ void k_mas_restrict0(const double* __restrict__ r, const int* __restr
         r2 = (float)r[3 * v + 2];
         msk = fine_mask[v];
     }
-    if(s < M)
-    {
-        R[3 * s] = r0;
-        R[3 * s + 1] = r1;
-        R[3 * s + 2] = r2;
-    }
+    if(s < M) st4(R + 4 * (size_t)s, r0, r1, r2);
     float a0 = 0.f, a1 = 0.f, a2 = 0.f;
 #pragma unroll
     for(int b = 0; b < B; b++)
     {
-        const float x0 = __shfl_sync(0xffffffffu, r0, b, B);
-        const float x1 = __shfl_sync(0xffffffffu, r1, b, B);
-        const float x2 = __shfl_sync(0xffffffffu, r2, b, B);
+        const float x0 = group_shfl<B>(r0, b);
+        const float x1 = group_shfl<B>(r1, b);
+        const float x2 = group_shfl<B>(r2, b);
         if(msk & (1u << b))
         {
             a0 += x0;
@@ -525,9 +520,7 @@ __global__ void k_mas_restrict0(const double* __restrict__ r, const int* __restr
     if(v >= 0 && __popc(msk & lanemask_lt(lane)) == 0)
     {
         const int g = going_next[v];
-        R[3 * g] = a0;
-        R[3 * g + 1] = a1;
-        R[3 * g + 2] = a2;
+        st4(R + 4 * (size_t)g, a0, a1, a2);
     }
 }
 
@@ -544,18 +537,16 @@ __global__ void k_mas_restrict_lx(float* R, const unsigned* __restrict__ closed,
     unsigned msk = 0;
     if(valid)
     {
-        r0 = R[3 * (begin + i)];
-        r1 = R[3 * (begin + i) + 1];
-        r2 = R[3 * (begin + i) + 2];
+        ld4(R + 4 * (size_t)(begin + i), r0, r1, r2);
         msk = closed[begin + i];
     }
     float a0 = 0.f, a1 = 0.f, a2 = 0.f;
 #pragma unroll
     for(int b = 0; b < B; b++)
     {
-        const float x0 = __shfl_sync(0xffffffffu, r0, b, B);
-        const float x1 = __shfl_sync(0xffffffffu, r1, b, B);
-        const float x2 = __shfl_sync(0xffffffffu, r2, b, B);
+        const float x0 = group_shfl<B>(r0, b);
+        const float x1 = group_shfl<B>(r1, b);
+        const float x2 = group_shfl<B>(r2, b);
         if(msk & (1u << b))
         {
             a0 += x0;
@@ -566,9 +557,7 @@ __global__ void k_mas_restrict_lx(float* R, const unsigned* __restrict__ closed,
     if(valid && __popc(msk & lanemask_lt(lane)) == 0)
     {
         const int g = going_next[begin + i];
-        R[3 * g] = a0;
-        R[3 * g + 1] = a1;
-        R[3 * g + 2] = a2;
+        st4(R + 4 * (size_t)g, a0, a1, a2);
     }
 }
 
@@ -588,7 +577,7 @@ __global__ void __launch_bounds__(B * B) k_mas_schwarz(const float* __restrict__
     const float4* src = reinterpret_cast<const float4*>(inv + (size_t)bk * NS * 9);
     float4* dst = reinterpret_cast<float4*>(P);
     for(int t = threadIdx.x; t < NS * 9 / 4; t += B * B) dst[t] = __ldg(src + t);
-    if(threadIdx.x < 3 * B) r[threadIdx.x] = R[(size_t)bk * 3 * B + threadIdx.x];
+    if(threadIdx.x < B) ld4(R + 4 * ((size_t)bk * B + threadIdx.x), r[3 * threadIdx.x], r[3 * threadIdx.x + 1], r[3 * threadIdx.x + 2]);
     __syncthreads();
     const int a = threadIdx.x / B, c = threadIdx.x % B;
     const float x0 = r[3 * c], x1 = r[3 * c + 1], x2 = r[3 * c + 2];
@@ -614,13 +603,7 @@ __global__ void __launch_bounds__(B * B) k_mas_schwarz(const float* __restrict__
         z1 += __shfl_xor_sync(0xffffffffu, z1, o);
         z2 += __shfl_xor_sync(0xffffffffu, z2, o);
     }
-    if(c == 0)
-    {
-        float* zo = Z + ((size_t)bk * B + a) * 3;
-        zo[0] = z0;
-        zo[1] = z1;
-        zo[2] = z2;
-    }
+    if(c == 0) st4(Z + ((size_t)bk * B + a) * 4, z0, z1, z2);
 }
 
 // __collectFinalZ_new (MASPreconditioner.cu:850-879): Z_v = sum over levels (FP32) -> FP64.
@@ -630,13 +613,16 @@ __global__ void k_mas_prolong(const float* __restrict__ Z, const int* __restrict
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if(v >= V) return;
     const int s = real_map[v];
-    float c0 = Z[3 * s], c1 = Z[3 * s + 1], c2 = Z[3 * s + 2];
+    float c0, c1, c2;
+    ld4(Z + 4 * (size_t)s, c0, c1, c2);
     for(int l = 1; l < L; l++)
     {
         const int now = coarse_table[(size_t)v * (L - 1) + l - 1];
-        c0 += Z[3 * now];
-        c1 += Z[3 * now + 1];
-        c2 += Z[3 * now + 2];
+        float t0, t1, t2;
+        ld4(Z + 4 * (size_t)now, t0, t1, t2);
+        c0 += t0;
+        c1 += t1;
+        c2 += t2;
     }
     z[3 * v] = c0;
     z[3 * v + 1] = c1;
@@ -698,6 +684,8 @@ int Solver::mas_init(int V, int node_offset, const uint32_t* ns, const uint32_t*
     m.bank = B;
     m.V = V;
     m.M = pms;
+    m.identity = true;
+    for(int s = 0; s < pms && m.identity; s++) m.identity = pm[s] == (s < V ? s : -1);
     m.nb0 = pms / B;
     m.node_offset = node_offset;
     m.nlist_size = nls;
@@ -840,10 +828,11 @@ static int mas_assemble_t(Solver& S, int offset)
     const size_t nvals = (size_t)m.nbanks * NS * 9;
     STG_TRY(m.mat.resize(nvals));
     STG_TRY(m.inv.resize(nvals));
-    STG_TRY(m.R.resize((size_t)m.total_clusters * 3));
-    STG_TRY(m.Z.resize((size_t)m.total_clusters * 3));
+    // R, Z: one {x y z 0} float4 slot per node of every level
+    STG_TRY(m.R.resize((size_t)m.total_clusters * 4));
+    STG_TRY(m.Z.resize((size_t)m.total_clusters * 4));
     STG_CUDA_TRY(cudaMemsetAsync(m.mat.data(), 0, nvals * sizeof(double), s));
-    STG_CUDA_TRY(cudaMemsetAsync(m.R.data(), 0, sizeof(float) * 3 * m.total_clusters, s));
+    STG_CUDA_TRY(cudaMemsetAsync(m.R.data(), 0, sizeof(float) * 4 * m.total_clusters, s));
     const int nnzb = S.bcoo.nnzb;
     const int g = std::max(1, std::min(div_up(nnzb, 256), kSMs * 16));
     if(nnzb > 0)

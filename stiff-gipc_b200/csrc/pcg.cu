@@ -8,344 +8,1377 @@
 //       q = A p; alpha = rz / p.q; x += alpha p; r -= alpha q
 //       if |rz| <= tol * rz0: break          (rz from before the update)
 //       z = M^-1 r; rz_new = r.z; beta = rz_new / rz; p = z + beta p; rz = rz_new
-// The reference copies every dot product to the host (pcg_solver.cu:148) and synchronises
-// six times per iteration; here all scalars stay on the device, each reduction is finished
-// by the last CTA (reduce.cuh), the dot products are fused into the kernels that produce
-// their operands (SpMV -> p.q, axpy -> r.r, preconditioner -> r.z), and a device flag ends
-// the loop.  The iteration body is launched from the host (LOOP_HOST, one flag read per
-// iteration) or captured once into a CUDA graph that runs `graph_batch` iterations per
-// launch (LOOP_GRAPH, one flag read per batch; iterations past convergence are no-ops).
+//
+// The reference runs ~8 kernels per iteration, copies each dot product to the host
+// (pcg_solver.cu:148) and synchronises six times per iteration.  Here one iteration is five
+// fused phases with every scalar on the device:
+//   A  q = A p_new with p_new = z + beta p_old formed on the fly from the gathered z / p_old
+//      (p is double-buffered, so the p update costs no pass), p.q -> alpha
+//   B  x += alpha p; r -= alpha q per MAS level-0 bank, restricting r to level 0 and summing
+//      each level-0 component into level 1 in the same pass; r.r -> stop test
+//   C  restriction of levels >= 2 from level 1 (one CTA, level by level)
+//   D  bank solves z_b = P_b r_b for every bank of every level
+//   E  prolongation z = sum_l P_l z_l (+ ABD 12x12 block-Jacobi), r.z -> beta
+// (non-MAS preconditioners: B is a plain axpy, C/D vanish, E applies block-Jacobi/identity).
+// Every reduction is finished by the last CTA in a fixed order (deterministic).  In FP32 mode
+// every `refine` iterations r is recomputed as b - A x with the FP64 blocks and restricted
+// again (residual replacement).
+//
+// Three drivers share these phases:
+//   LOOP_HOST   one launch per phase, a flag read after every iteration;
+//   LOOP_GRAPH  the iteration is captured once as the body of a device-side WHILE node of a
+//               CUDA graph (the replacement as an IF node); one graph launch runs the whole
+//               solve, the loop condition is set by the stop test on the device;
+//   LOOP_PERSISTENT  one cooperative kernel runs all iterations; phases are separated by a
+//               bounded grid barrier that also finishes the reductions.
 #include "solver.hpp"
 #include "reduce.cuh"
-#include "spmv_core.cuh"
 
 namespace stg
 {
-int mas_restrict_solve(Solver& S, const double* r);
-int mas_restrict_solve_guarded(Solver& S, const double* r, const int* done);
 
-constexpr int PB = 256;  // PCG kernel block size
+constexpr int PB = 256;  // threads per CTA in every PCG kernel
 
-struct RedArgs
+enum Site : int
 {
-    double* partials;
-    unsigned* counter;
-    double* scal;
-    int* flags;
-    PcgParams p;
+    SITE_A = 0,
+    SITE_B = 1,
+    SITE_R = 2,
+    SITE_E = 3,
+    SITE_INIT = 4,
+    SITE_INIT_RZ = 5
 };
 
-// r = b, x = 0, p = 0; b.b -> SS_BB
-__global__ void __launch_bounds__(PB) k_pcg_init(const double* __restrict__ b, double* r, double* x, double* p64,
-                                                 float* p32, int n, RedArgs ra)
+// ---------------------------------------------------------------------------------------
+// reductions: last CTA finishes, optionally drives the graph's conditional nodes
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void set_conditionals(const PcgDev& c, int op)
 {
-    double acc = 0;
-    for(int i = blockIdx.x * PB + threadIdx.x; i < n; i += gridDim.x * PB)
+    if(!c.use_cond) return;
+    const bool done = c.flags[F_DONE] != 0;
+    if(op == POST_CHECK || op == POST_RECHECK || op == POST_ALPHA) cudaGraphSetConditional(c.h_while, done ? 0u : 1u);
+    if(op == POST_CHECK && c.use_cond == 2)
     {
-        const double bi = b[i];
-        r[i] = bi;
-        x[i] = 0.0;
-        if(p64) p64[i] = 0.0;
-        if(p32) p32[i] = 0.f;
-        acc += bi * bi;
+        const long k = (long)c.scal[SS_ITER];
+        const bool repl = !done && c.prm.refine > 0 && k % c.prm.refine == 0;
+        cudaGraphSetConditional(c.h_if, repl ? 1u : 0u);
     }
-    grid_reduce_finish<PB>(acc, ra.partials, ra.counter, POST_STORE, SS_BB, ra.scal, ra.flags, ra.p);
 }
 
-// q = A p and p.q (-> alpha)
-template <typename T>
-__global__ void __launch_bounds__(PB) k_pcg_spmv(const int* __restrict__ row_ptr, const int* __restrict__ cols,
-                                                 const T* __restrict__ blocks, const int* __restrict__ t_ptr,
-                                                 const int2* __restrict__ t_ent, const T* __restrict__ p, T* q, int nrows,
-                                                 RedArgs ra)
+__device__ __forceinline__ void finish_reduction(const PcgDev& c, double v, int site, int op, int slot = 0)
 {
-    if(ra.flags[F_DONE]) return;
-    constexpr int LPR = 16, RPW = 32 / LPR;
-    const int warp = (blockIdx.x * PB + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * PB) >> 5;
-    const int lane = threadIdx.x & 31, sub = lane & (LPR - 1);
-    double acc = 0;
-    for(int base = warp * RPW; base < nrows; base += nwarps * RPW)
+    __shared__ double red[PB / 32];
+    __shared__ bool last;
+    double* partials = c.partials + (size_t)site * c.slots;
+    unsigned* counter = c.counters + site;
+    const double bs = block_sum<PB>(v, red);
+    if(threadIdx.x == 0)
     {
-        const int i = base + lane / LPR;
-        const bool valid = i < nrows;
-        T a0, a1, a2;
-        row_spmv<T, LPR>(i, valid, sub, row_ptr, cols, blocks, t_ptr, t_ent, p, a0, a1, a2);
-        if(valid && sub < 3)
+        partials[blockIdx.x] = bs;
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if(!last) return;
+    __threadfence();
+    double acc = 0;
+    for(int i = threadIdx.x; i < (int)gridDim.x; i += PB) acc += __ldcg(partials + i);
+    const double tot = block_sum<PB>(acc, red);
+    if(threadIdx.x == 0)
+    {
+        post_op(op, slot, tot, c.scal, c.flags, c.prm);
+        set_conditionals(c, op);
+        *counter = 0u;
+        __threadfence();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// block loads (16-byte vector loads of the padded layouts)
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void load_block(const float* base, size_t k, float h[9])
+{
+    const float4* p = reinterpret_cast<const float4*>(base) + 3 * k;
+    const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+    h[0] = a.x; h[1] = a.y; h[2] = a.z; h[3] = a.w;
+    h[4] = b.x; h[5] = b.y; h[6] = b.z; h[7] = b.w;
+    h[8] = c.x;
+}
+
+__device__ __forceinline__ void load_block(const double* base, size_t k, double h[9])
+{
+    const double2* p = reinterpret_cast<const double2*>(base) + 5 * k;
+    const double2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3), e = __ldg(p + 4);
+    h[0] = a.x; h[1] = a.y; h[2] = b.x; h[3] = b.y; h[4] = c.x; h[5] = c.y; h[6] = d.x; h[7] = d.y;
+    h[8] = e.x;
+}
+
+// acc += H x (trans: H^T x); h column-major
+template <typename T>
+__device__ __forceinline__ void mv3(const T h[9], bool trans, T x0, T x1, T x2, T& a0, T& a1, T& a2)
+{
+    const T h01 = trans ? h[1] : h[3], h10 = trans ? h[3] : h[1];
+    const T h02 = trans ? h[2] : h[6], h20 = trans ? h[6] : h[2];
+    const T h12 = trans ? h[5] : h[7], h21 = trans ? h[7] : h[5];
+    a0 += h[0] * x0 + h01 * x1 + h02 * x2;
+    a1 += h10 * x0 + h[4] * x1 + h12 * x2;
+    a2 += h20 * x0 + h21 * x1 + h[8] * x2;
+}
+
+// Row i of A * v with v_j = z_j + beta p_j gathered from the interleaved zp slots (x_plain:
+// a plain [3n] FP64 vector instead, for the residual replacement).  LPR lanes per row,
+// warp-wide shuffles: every lane of the warp must call it.
+template <typename T, int LPR>
+__device__ __forceinline__ void row_spmv_zp(const PcgDev& c, const T* blk, int i, bool valid, int sub, const T* zp,
+                                            T beta, const double* x_plain, T& a0, T& a1, T& a2)
+{
+    a0 = a1 = a2 = T(0);
+    int u0 = 0, nu = 0, t0 = 0, nt = 0;
+    if(valid)
+    {
+        u0 = __ldg(c.row_ptr + i);
+        nu = __ldg(c.row_ptr + i + 1) - u0;
+        t0 = __ldg(c.t_ptr + i);
+        nt = __ldg(c.t_ptr + i + 1) - t0;
+    }
+    for(int e = sub; e < nu + nt; e += LPR)
+    {
+        int k, j;
+        const bool trans = e >= nu;
+        if(!trans)
         {
-            const T v = sub == 0 ? a0 : (sub == 1 ? a1 : a2);
-            q[3 * i + sub] = v;
-            acc += (double)p[3 * i + sub] * (double)v;
+            k = u0 + e;
+            j = __ldg(c.cols + k);
         }
-    }
-    grid_reduce_finish<PB>(acc, ra.partials, ra.counter, POST_ALPHA, 0, ra.scal, ra.flags, ra.p);
-}
-
-// x += alpha p; r -= alpha q; r.r (-> stop test)
-template <typename T>
-__global__ void __launch_bounds__(PB) k_pcg_axpy(double* x, double* r, const T* __restrict__ p, const T* __restrict__ q,
-                                                 int n, RedArgs ra)
-{
-    if(ra.flags[F_DONE]) return;
-    const double alpha = ra.scal[SS_ALPHA];
-    double acc = 0;
-    for(int i = blockIdx.x * PB + threadIdx.x; i < n; i += gridDim.x * PB)
-    {
-        x[i] += alpha * (double)p[i];
-        const double ri = r[i] - alpha * (double)q[i];
-        r[i] = ri;
-        acc += ri * ri;
-    }
-    grid_reduce_finish<PB>(acc, ra.partials, ra.counter, POST_CHECK, 0, ra.scal, ra.flags, ra.p);
-}
-
-// FP32 mode residual replacement: every `refine` iterations r = b - A x in FP64, r.r, stop test.
-__global__ void __launch_bounds__(PB) k_pcg_replace(const int* __restrict__ row_ptr, const int* __restrict__ cols,
-                                                    const double* __restrict__ blocks, const int* __restrict__ t_ptr,
-                                                    const int2* __restrict__ t_ent, const double* __restrict__ x,
-                                                    const double* __restrict__ b, double* r, int nrows, RedArgs ra)
-{
-    if(ra.flags[F_DONE]) return;
-    const long k = (long)ra.scal[SS_ITER];
-    if(ra.p.refine <= 0 || k % ra.p.refine != 0) return;
-    constexpr int LPR = 16, RPW = 32 / LPR;
-    const int warp = (blockIdx.x * PB + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * PB) >> 5;
-    const int lane = threadIdx.x & 31, sub = lane & (LPR - 1);
-    double acc = 0;
-    for(int base = warp * RPW; base < nrows; base += nwarps * RPW)
-    {
-        const int i = base + lane / LPR;
-        const bool valid = i < nrows;
-        double a0, a1, a2;
-        row_spmv<double, LPR>(i, valid, sub, row_ptr, cols, blocks, t_ptr, t_ent, x, a0, a1, a2);
-        if(valid && sub < 3)
+        else
         {
-            const double v = sub == 0 ? a0 : (sub == 1 ? a1 : a2);
-            const double ri = b[3 * i + sub] - v;
-            r[3 * i + sub] = ri;
-            acc += ri * ri;
+            const int2 te = __ldg(c.t_ent + t0 + e - nu);
+            k = te.x;
+            j = te.y;
         }
+        T h[9];
+        load_block(blk, (size_t)k, h);
+        T x0, x1, x2;
+        if(x_plain)
+        {
+            x0 = (T)x_plain[3 * j];
+            x1 = (T)x_plain[3 * j + 1];
+            x2 = (T)x_plain[3 * j + 2];
+        }
+        else
+        {
+            T p0, p1, p2;
+            ld4(zp + 8 * (size_t)j, x0, x1, x2);
+            ld4(zp + 8 * (size_t)j + 4, p0, p1, p2);
+            x0 += beta * p0;
+            x1 += beta * p1;
+            x2 += beta * p2;
+        }
+        mv3<T>(h, trans, x0, x1, x2, a0, a1, a2);
     }
-    if(blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(ra.flags + F_REPL, 1);
-    grid_reduce_finish<PB>(acc, ra.partials, ra.counter, POST_RECHECK, 0, ra.scal, ra.flags, ra.p);
-}
-
-// ABD 12x12 block-Jacobi (abd_preconditioner.cu:20-38) on the first 12*bodies dofs, one thread
-// per body row; returns this thread's share of r.z.
-template <typename T>
-__device__ __forceinline__ double abd_rows(const double* __restrict__ r, T* z, const double* __restrict__ abd_inv,
-                                           int abd_bodies, int gtid, int gthreads)
-{
-    double acc = 0;
-    for(int t = gtid; t < abd_bodies * 12; t += gthreads)
-    {
-        const int body = t / 12, row = t % 12;
-        const double* J = abd_inv + (size_t)body * 144 + row * 12;
-        double s = 0;
 #pragma unroll
-        for(int c = 0; c < 12; c++) s += J[c] * r[body * 12 + c];
-        z[t] = (T)s;
-        acc += r[t] * (double)(T)s;
+    for(int o = LPR / 2; o > 0; o >>= 1)
+    {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    }
+}
+
+// Row i of A * (z + beta p) on the full symmetric SoA copy (phase A).  LPR lanes per row,
+// warp-wide shuffles: every lane of the warp must call it.
+template <typename T, int LPR>
+__device__ __forceinline__ void row_spmv_full(const PcgDev& c, int i, bool valid, int sub, const T* zp, T beta, T& a0,
+                                              T& a1, T& a2)
+{
+    a0 = a1 = a2 = T(0);
+    size_t f0 = 0;
+    int deg = 0;
+    if(valid)
+    {
+        const int r0 = __ldg(c.row_ptr + i), r1 = __ldg(c.row_ptr + i + 1);
+        const int t0 = __ldg(c.t_ptr + i), t1 = __ldg(c.t_ptr + i + 1);
+        f0 = (size_t)r0 + t0;
+        deg = (r1 - r0) + (t1 - t0);
+    }
+    const T* v = reinterpret_cast<const T*>(c.fval);
+    for(int e = sub; e < deg; e += LPR)
+    {
+        const size_t f = f0 + e;
+        const int j = __ldg(c.fcol + f);
+        T h[9];
+#pragma unroll
+        for(int t = 0; t < 9; t++) h[t] = __ldg(v + t * c.fstride + f);
+        T x0, x1, x2, p0, p1, p2;
+        ld4(zp + 8 * (size_t)j, x0, x1, x2);
+        ld4(zp + 8 * (size_t)j + 4, p0, p1, p2);
+        x0 += beta * p0;
+        x1 += beta * p1;
+        x2 += beta * p2;
+        mv3<T>(h, false, x0, x1, x2, a0, a1, a2);
+    }
+#pragma unroll
+    for(int o = LPR / 2; o > 0; o >>= 1)
+    {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// phases (gt / gn: this thread's index and the thread count of the grid)
+// ---------------------------------------------------------------------------------------
+// zp buffer parity: phase A of iteration k runs with ITER = k-1 and reads zp[(k-1)&1]
+// (z_{k-1}, p_{k-1}), writing p_k into zp[k&1]; B reads p_k there; E (ITER = k) writes z_k
+// into zp[k&1] too, which phase A of iteration k+1 reads.
+template <typename T>
+__device__ __forceinline__ T* zpbuf(const PcgDev& c, int parity)
+{
+    return reinterpret_cast<T*>(parity ? c.zp1 : c.zp0);
+}
+// scalars are read with ld.global.cg: in the persistent kernel they change between phases
+__device__ __forceinline__ int iter_parity(const PcgDev& c) { return ((long)__ldcg(c.scal + SS_ITER)) & 1; }
+
+// A: q = A p_new, p_new = z + beta p_old; returns this thread's share of p_new . q
+template <typename T>
+__device__ __forceinline__ double phase_a(const PcgDev& c, int gt, int gn)
+{
+    constexpr int LPR = 16, RPW = 32 / LPR;
+    const int par = iter_parity(c);
+    const T* zp = zpbuf<T>(c, par);
+    T* zpn = zpbuf<T>(c, par ^ 1);
+    T* q = reinterpret_cast<T*>(c.q);
+    const T beta = (T)__ldcg(c.scal + SS_BETA);
+    const int warp = gt >> 5, nwarps = gn >> 5, lane = gt & 31, sub = lane & (LPR - 1);
+    double acc = 0;
+    for(int base = warp * RPW; base < c.nrows; base += nwarps * RPW)
+    {
+        const int i = base + lane / LPR;
+        const bool valid = i < c.nrows;
+        T a0, a1, a2;
+        row_spmv_full<T, LPR>(c, i, valid, sub, zp, beta, a0, a1, a2);
+        if(valid && sub == 0)
+        {
+            T z0, z1, z2, p0, p1, p2;
+            ld4(zp + 8 * (size_t)i, z0, z1, z2);
+            ld4(zp + 8 * (size_t)i + 4, p0, p1, p2);
+            p0 = z0 + beta * p0;
+            p1 = z1 + beta * p1;
+            p2 = z2 + beta * p2;
+            st4(zpn + 8 * (size_t)i + 4, p0, p1, p2);
+            st4(q + 4 * (size_t)i, a0, a1, a2);
+            acc += (double)p0 * (double)a0 + (double)p1 * (double)a1 + (double)p2 * (double)a2;
+        }
     }
     return acc;
 }
 
-// MAS prolongation (__collectFinalZ_new, MASPreconditioner.cu:850-879) over the FEM range +
-// ABD block-Jacobi, fused with r.z.
+// B (MAS): axpy over the FEM range in level-0 slot order + level-0/1 restriction; plain axpy
+// over the ABD range.  Returns this thread's share of r.r.
+// x_i += alpha p_i; r_i -= alpha q_i for block row i (3 dofs); returns the new r_i and adds
+// its squared norm to acc
 template <typename T>
-__global__ void __launch_bounds__(PB) k_pcg_prolong(const float* __restrict__ Z, const int* __restrict__ real_map,
-                                                    const int* __restrict__ coarse_table, int L, int V, int fem_dof,
-                                                    const double* __restrict__ r, T* z, const double* __restrict__ abd_inv,
-                                                    int abd_bodies, int op, RedArgs ra)
+__device__ __forceinline__ void axpy_row(const PcgDev& c, const T* pn, const T* q, double alpha, int i, double& r0,
+                                         double& r1, double& r2, double& acc)
 {
-    if(ra.flags[F_DONE]) return;
-    double acc = 0;
-    const int gt = blockIdx.x * PB + threadIdx.x, gn = gridDim.x * PB;
-    for(int v = gt; v < V; v += gn)
-    {
-        const int s = real_map[v];
-        float c0 = Z[3 * s], c1 = Z[3 * s + 1], c2 = Z[3 * s + 2];
-        for(int l = 1; l < L; l++)
-        {
-            const int now = coarse_table[(size_t)v * (L - 1) + l - 1];
-            c0 += Z[3 * now];
-            c1 += Z[3 * now + 1];
-            c2 += Z[3 * now + 2];
-        }
-        const int d = fem_dof + 3 * v;
-        z[d] = (T)c0;
-        z[d + 1] = (T)c1;
-        z[d + 2] = (T)c2;
-        acc += r[d] * (double)c0 + r[d + 1] * (double)c1 + r[d + 2] * (double)c2;
-    }
-    acc += abd_rows<T>(r, z, abd_inv, abd_bodies, gt, gn);
-    grid_reduce_finish<PB>(acc, ra.partials, ra.counter, op, 0, ra.scal, ra.flags, ra.p);
+    T p0, p1, p2, q0, q1, q2;
+    ld4(pn + 8 * (size_t)i + 4, p0, p1, p2);
+    ld4(q + 4 * (size_t)i, q0, q1, q2);
+    double* x = c.x + 3 * (size_t)i;
+    double* r = c.r + 3 * (size_t)i;
+    x[0] += alpha * (double)p0;
+    x[1] += alpha * (double)p1;
+    x[2] += alpha * (double)p2;
+    r0 = r[0] - alpha * (double)q0;
+    r1 = r[1] - alpha * (double)q1;
+    r2 = r[2] - alpha * (double)q2;
+    r[0] = r0;
+    r[1] = r1;
+    r[2] = r2;
+    acc += r0 * r0 + r1 * r1 + r2 * r2;
 }
 
-// Global block-Jacobi (DiagPreconditioner, diag_preconditioner.cu:35-66) or identity, then the
-// ABD local preconditioner over its range; fused with r.z.
-template <typename T>
-__global__ void __launch_bounds__(PB) k_pcg_diag(const double* __restrict__ diag_inv, const double* __restrict__ r, T* z,
-                                                 int nrows, const double* __restrict__ abd_inv, int abd_bodies, int op,
-                                                 RedArgs ra)
+template <typename T, int B>
+__device__ __forceinline__ double phase_b_mas(const PcgDev& c, int gt, int gn)
 {
-    if(ra.flags[F_DONE]) return;
+    const double alpha = __ldcg(c.scal + SS_ALPHA);
+    const T* pn = zpbuf<T>(c, iter_parity(c) ^ 1);
+    const T* q = reinterpret_cast<const T*>(c.q);
     double acc = 0;
-    const int gt = blockIdx.x * PB + threadIdx.x, gn = gridDim.x * PB;
-    const int first = abd_bodies * 4;  // ABD block rows are overwritten by the local preconditioner
-    for(int bi = first + gt; bi < nrows; bi += gn)
+    const int span = (c.M + 31) / 32 * 32;
+    const int fem_row = c.fem_dof / 3;
+    for(int s = gt; s < span; s += gn)
     {
-        const double r0 = r[3 * bi], r1 = r[3 * bi + 1], r2 = r[3 * bi + 2];
-        double z0 = r0, z1 = r1, z2 = r2;
-        if(diag_inv)
+        const int v = c.identity ? (s < c.V ? s : -1) : (s < c.M ? c.part_map[s] : -1);
+        float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+        unsigned msk = 0;
+        if(v >= 0)
         {
-            const double* D = diag_inv + 9 * (size_t)bi;
+            double d0, d1, d2;
+            axpy_row<T>(c, pn, q, alpha, fem_row + v, d0, d1, d2, acc);
+            r0 = (float)d0;
+            r1 = (float)d1;
+            r2 = (float)d2;
+            msk = c.fine_mask[v];
+        }
+        if(s < c.M)
+        {
+            st4(c.R + 4 * (size_t)s, r0, r1, r2);
+        }
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+        for(int bb = 0; bb < B; bb++)
+        {
+            const float x0 = group_shfl<B>(r0, bb);
+            const float x1 = group_shfl<B>(r1, bb);
+            const float x2 = group_shfl<B>(r2, bb);
+            if(msk & (1u << bb))
+            {
+                a0 += x0;
+                a1 += x1;
+                a2 += x2;
+            }
+        }
+        const int lane = s % B;
+        if(v >= 0 && __popc(msk & lanemask_lt(lane)) == 0)
+        {
+            const int g = c.going_next[v];
+            st4(c.R + 4 * (size_t)g, a0, a1, a2);
+        }
+    }
+    for(int i = gt; i < c.abd_bodies * 4; i += gn)
+    {
+        double d0, d1, d2;
+        axpy_row<T>(c, pn, q, alpha, i, d0, d1, d2, acc);
+    }
+    return acc;
+}
+
+// B (block-Jacobi / identity): plain axpy over all block rows
+template <typename T>
+__device__ __forceinline__ double phase_b_plain(const PcgDev& c, int gt, int gn)
+{
+    const double alpha = __ldcg(c.scal + SS_ALPHA);
+    const T* pn = zpbuf<T>(c, iter_parity(c) ^ 1);
+    const T* q = reinterpret_cast<const T*>(c.q);
+    double acc = 0;
+    for(int i = gt; i < c.nrows; i += gn)
+    {
+        double d0, d1, d2;
+        axpy_row<T>(c, pn, q, alpha, i, d0, d1, d2, acc);
+    }
+    return acc;
+}
+
+// residual replacement: r = b - A x with the FP64 blocks; returns the share of r.r
+__device__ __forceinline__ double phase_replace(const PcgDev& c, int gt, int gn)
+{
+    constexpr int LPR = 16, RPW = 32 / LPR;
+    const int warp = gt >> 5, nwarps = gn >> 5, lane = gt & 31, sub = lane & (LPR - 1);
+    const double* blk = reinterpret_cast<const double*>(c.blk64);
+    double acc = 0;
+    for(int base = warp * RPW; base < c.nrows; base += nwarps * RPW)
+    {
+        const int i = base + lane / LPR;
+        const bool valid = i < c.nrows;
+        double a0, a1, a2;
+        row_spmv_zp<double, LPR>(c, blk, i, valid, sub, nullptr, 0.0, c.x, a0, a1, a2);
+        if(valid && sub < 3)
+        {
+            const int d = 3 * i + sub;
+            const double ri = c.b[d] - (sub == 0 ? a0 : (sub == 1 ? a1 : a2));
+            c.r[d] = ri;
+            acc += ri * ri;
+        }
+    }
+    return acc;
+}
+
+// level 0/1 restriction alone (after a residual replacement)
+template <int B>
+__device__ __forceinline__ void phase_restrict01(const PcgDev& c, int gt, int gn)
+{
+    const int span = (c.M + 31) / 32 * 32;
+    for(int s = gt; s < span; s += gn)
+    {
+        const int v = s < c.M ? c.part_map[s] : -1;
+        float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+        unsigned msk = 0;
+        if(v >= 0)
+        {
+            const int d = c.fem_dof + 3 * v;
+            r0 = (float)c.r[d];
+            r1 = (float)c.r[d + 1];
+            r2 = (float)c.r[d + 2];
+            msk = c.fine_mask[v];
+        }
+        // the bank's values through shared memory (same lane-order sums as the shuffle form in
+        // phase_b_mas); this kernel runs at set-up and after residual replacements only
+        __shared__ float sv[PB * 3];
+        const int w0 = (threadIdx.x & ~(B - 1)) * 3;
+        sv[3 * threadIdx.x] = r0;
+        sv[3 * threadIdx.x + 1] = r1;
+        sv[3 * threadIdx.x + 2] = r2;
+        __syncwarp();
+        if(s < c.M)
+        {
+            st4(c.R + 4 * (size_t)s, r0, r1, r2);
+        }
+        const int lane = s % B;
+        if(v >= 0 && __popc(msk & lanemask_lt(lane)) == 0)
+        {
+            float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+            for(int bb = 0; bb < B; bb++)
+                if(msk & (1u << bb))
+                {
+                    a0 += sv[w0 + 3 * bb];
+                    a1 += sv[w0 + 3 * bb + 1];
+                    a2 += sv[w0 + 3 * bb + 2];
+                }
+            const int g = c.going_next[v];
+            st4(c.R + 4 * (size_t)g, a0, a1, a2);
+        }
+        __syncwarp();
+    }
+}
+
+// C: restriction level l -> l+1 for l in [l0, l1): each component of a level-l bank sums its
+// nodes in lane order.  Threads gt, gt+gn, ... of the caller; the caller separates levels
+// (C1: level 1 -> 2 over the whole grid; C2: levels >= 2 inside one CTA, which passes
+// block_sync = true).
+template <int B>
+__device__ __forceinline__ void restrict_level(const PcgDev& c, int number, int begin, int gt, int gn)
+{
+    const int span = (number + 31) / 32 * 32;
+    for(int i = gt; i < span; i += gn)
+    {
+        const bool valid = i < number;
+        float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+        unsigned msk = 0;
+        if(valid)
+        {
+            ld4(c.R + 4 * (size_t)(begin + i), r0, r1, r2);
+            msk = c.closed[begin + i];
+        }
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+        // partial unroll: full unrolling of this loop makes ptxas 12.9 (sm_100a) abort
+#pragma unroll 4
+        for(int bb = 0; bb < B; bb++)
+        {
+            const float x0 = group_shfl<B>(r0, bb);
+            const float x1 = group_shfl<B>(r1, bb);
+            const float x2 = group_shfl<B>(r2, bb);
+            if(msk & (1u << bb))
+            {
+                a0 += x0;
+                a1 += x1;
+                a2 += x2;
+            }
+        }
+        if(valid && __popc(msk & lanemask_lt(i % B)) == 0)
+        {
+            const int g = c.going_next[begin + i];
+            st4(c.R + 4 * (size_t)g, a0, a1, a2);
+        }
+    }
+}
+
+template <int B>
+__device__ __forceinline__ void phase_c(const PcgDev& c, int l0, int l1, int gt, int gn, bool block_sync)
+{
+    for(int level = l0; level < l1 && level < c.L - 1; level++)
+    {
+        restrict_level<B>(c, __ldg(c.ls_dev + 2 * level), __ldg(c.ls_dev + 2 * level + 1), gt, gn);
+        if(block_sync) __syncthreads();
+    }
+}
+
+// D: bank solves for banks [b0, b1) with stride `bstep`, one bank per pass of the CTA.
+// PB threads = 256: for B = 16 one thread per (row lane, col lane); for B = 32 each thread
+// handles 4 (row, col) pairs.  The packed inverse is staged in shared memory with 16-byte loads.
+template <int B>
+__device__ __forceinline__ void phase_d(const PcgDev& c, int b0, int b1, int bstep)
+{
+    constexpr int NS = B * (B + 1) / 2;
+    __shared__ __align__(16) float P[NS * 9];
+    __shared__ float rr[3 * B];
+    for(int bk = b0; bk < b1; bk += bstep)
+    {
+        const float4* src = reinterpret_cast<const float4*>(c.inv + (size_t)bk * NS * 9);
+        float4* dst = reinterpret_cast<float4*>(P);
+        for(int t = threadIdx.x; t < NS * 9 / 4; t += PB) dst[t] = __ldg(src + t);
+        if(threadIdx.x < B) ld4(c.R + 4 * ((size_t)bk * B + threadIdx.x), rr[3 * threadIdx.x], rr[3 * threadIdx.x + 1],
+                                rr[3 * threadIdx.x + 2]);
+        __syncthreads();
+        constexpr int REP = (B * B + PB - 1) / PB;
+#pragma unroll
+        for(int rep = 0; rep < REP; rep++)
+        {
+            const int pair = threadIdx.x + rep * PB;
+            const int a = pair / B, cc = pair % B;
+            const float x0 = rr[3 * cc], x1 = rr[3 * cc + 1], x2 = rr[3 * cc + 2];
+            float z0, z1, z2;
+            if(cc >= a)
+            {
+                const float* Pb = P + (B * a - a * (a + 1) / 2 + cc) * 9;
+                z0 = Pb[0] * x0 + Pb[3] * x1 + Pb[6] * x2;
+                z1 = Pb[1] * x0 + Pb[4] * x1 + Pb[7] * x2;
+                z2 = Pb[2] * x0 + Pb[5] * x1 + Pb[8] * x2;
+            }
+            else
+            {
+                const float* Pb = P + (B * cc - cc * (cc + 1) / 2 + a) * 9;
+                z0 = Pb[0] * x0 + Pb[1] * x1 + Pb[2] * x2;
+                z1 = Pb[3] * x0 + Pb[4] * x1 + Pb[5] * x2;
+                z2 = Pb[6] * x0 + Pb[7] * x1 + Pb[8] * x2;
+            }
+#pragma unroll
+            for(int o = (B < 32 ? B : 32) / 2; o > 0; o >>= 1)
+            {
+                z0 += __shfl_xor_sync(0xffffffffu, z0, o);
+                z1 += __shfl_xor_sync(0xffffffffu, z1, o);
+                z2 += __shfl_xor_sync(0xffffffffu, z2, o);
+            }
+            if(cc == 0)
+            {
+                st4(c.Z + ((size_t)bk * B + a) * 4, z0, z1, z2);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// D (16-vertex banks): one warp per bank, the bank's packed inverse (136 3x3 FP32 blocks,
+// 4,896 B) and its 16 residual slots (256 B) staged in shared memory by the Tensor Memory
+// Accelerator (cp.async.bulk, completion on an mbarrier), double-buffered so that the copy
+// of the warp's next bank overlaps the solve of the current one.
+// ---------------------------------------------------------------------------------------
+constexpr int D_WARPS = 4;                        // warps per CTA
+constexpr int D_PBYTES = 136 * 9 * 4;             // packed inverse of one bank
+constexpr int D_RBYTES = 16 * 16;                 // 16 float4 residual slots
+constexpr int D_BUF = D_PBYTES + D_RBYTES;        // one stage (16-byte multiple)
+constexpr int D_PART = 16 * 65;                   // partial products, row stride 65 floats
+constexpr int D_WARP_BYTES = 2 * D_BUF + D_PART * 4 + 16;
+constexpr unsigned D_WAIT_LIMIT = 1u << 22;       // bounded mbarrier polling
+
+// (row, col) of packed upper block k of a 16-bank
+__constant__ unsigned char c_upper16[136][2];
+
+__device__ __forceinline__ unsigned smem_u32(const void* p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, unsigned bytes, unsigned bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :
+                 : "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// waits for phase `parity` of the mbarrier; false when the bounded wait gave up
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity)
+{
+    for(unsigned it = 0; it < D_WAIT_LIMIT; it++)
+    {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if(ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void d16_issue(const PcgDev& c, char* stage, unsigned bar, int bk)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"((unsigned)D_BUF) : "memory");
+    tma_load_1d(stage, c.inv + (size_t)bk * 136 * 9, D_PBYTES, bar);
+    tma_load_1d(stage + D_PBYTES, c.R + (size_t)bk * 16 * 4, D_RBYTES, bar);
+}
+
+__global__ void __launch_bounds__(D_WARPS * 32) k_phase_d16(PcgDev c)
+{
+    if(c.flags[F_DONE]) return;
+    extern __shared__ __align__(128) char dsm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    char* base = dsm + (size_t)warp * D_WARP_BYTES;
+    char* const stage0 = base;
+    char* const stage1 = base + D_BUF;
+    float* part = reinterpret_cast<float*>(base + 2 * D_BUF);
+    const unsigned bar0 = smem_u32(base + 2 * D_BUF + D_PART * 4), bar1 = bar0 + 8;
+    const int gw = blockIdx.x * D_WARPS + warp, nw = gridDim.x * D_WARPS;
+    if(gw >= c.nbanks) return;
+    if(lane == 0)
+    {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        d16_issue(c, stage0, bar0, gw);
+    }
+    __syncwarp();
+    unsigned ph0 = 0u, ph1 = 0u;
+    int buf = 0;
+    for(int bk = gw; bk < c.nbanks; bk += nw, buf ^= 1)
+    {
+        char* const cur = buf ? stage1 : stage0;
+        const unsigned bcur = buf ? bar1 : bar0, bnext = buf ? bar0 : bar1;
+        // prefetch the next bank into the other stage (its previous contents are consumed)
+        const int nxt = bk + nw;
+        if(lane == 0 && nxt < c.nbanks)
+        {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            d16_issue(c, buf ? stage0 : stage1, bnext, nxt);
+        }
+        if(!mbar_wait(bcur, buf ? ph1 : ph0))
+        {
+            if(lane == 0)
+            {
+                atomicExch(c.flags + F_STATUS, 6);  // STG_ERR_TIMEOUT
+                atomicExch(c.flags + F_DONE, 1);
+            }
+            // let any copy still in flight land before the CTA's shared memory is released
+            if(nxt < c.nbanks) mbar_wait(bnext, buf ? ph0 : ph1);
+            return;
+        }
+        if(buf)
+            ph1 ^= 1u;
+        else
+            ph0 ^= 1u;
+        const float* P = reinterpret_cast<const float*>(cur);
+        const float* rs = reinterpret_cast<const float*>(cur + D_PBYTES);
+#pragma unroll
+        for(int m = 0; m < 5; m++)
+        {
+            const int k = lane + 32 * m;
+            if(k < 136)
+            {
+                const int a = c_upper16[k][0], cc = c_upper16[k][1];
+                const float* h = P + 9 * k;  // column-major 3x3
+                const float x0 = rs[4 * cc], x1 = rs[4 * cc + 1], x2 = rs[4 * cc + 2];
+                float* pa = part + a * 65 + cc * 4;
+                pa[0] = h[0] * x0 + h[3] * x1 + h[6] * x2;
+                pa[1] = h[1] * x0 + h[4] * x1 + h[7] * x2;
+                pa[2] = h[2] * x0 + h[5] * x1 + h[8] * x2;
+                if(cc != a)
+                {
+                    const float y0 = rs[4 * a], y1 = rs[4 * a + 1], y2 = rs[4 * a + 2];
+                    float* pc = part + cc * 65 + a * 4;  // H^T r_a into row cc
+                    pc[0] = h[0] * y0 + h[1] * y1 + h[2] * y2;
+                    pc[1] = h[3] * y0 + h[4] * y1 + h[5] * y2;
+                    pc[2] = h[6] * y0 + h[7] * y1 + h[8] * y2;
+                }
+            }
+        }
+        __syncwarp();
+        if(lane < 16)
+        {
+            float z0 = 0.f, z1 = 0.f, z2 = 0.f;
+            const float* pr = part + lane * 65;
+#pragma unroll
+            for(int col = 0; col < 16; col++)
+            {
+                z0 += pr[4 * col];
+                z1 += pr[4 * col + 1];
+                z2 += pr[4 * col + 2];
+            }
+            st4(c.Z + ((size_t)bk * 16 + lane) * 4, z0, z1, z2);
+        }
+        __syncwarp();
+    }
+}
+
+// E (MAS): z = sum over levels (FP32) on the FEM range + ABD block-Jacobi; share of r.z
+// ABD 12x12 block-Jacobi (abd_preconditioner.cu:20-38): one thread per dof of the first
+// 12 * bodies dofs, z written into the zp slots; returns the share of r.z
+template <typename T>
+__device__ __forceinline__ double abd_apply(const PcgDev& c, T* zp, int gt, int gn)
+{
+    double acc = 0;
+    for(int t = gt; t < c.abd_bodies * 12; t += gn)
+    {
+        const int body = t / 12, row = t % 12;
+        const double* J = c.abd_inv + (size_t)body * 144 + row * 12;
+        double s = 0;
+#pragma unroll
+        for(int cc = 0; cc < 12; cc++) s += J[cc] * c.r[body * 12 + cc];
+        zp[8 * (size_t)(t / 3) + t % 3] = (T)s;
+        acc += c.r[t] * (double)(T)s;
+    }
+    return acc;
+}
+
+template <typename T>
+__device__ __forceinline__ double phase_e_mas(const PcgDev& c, int gt, int gn)
+{
+    T* zp = zpbuf<T>(c, iter_parity(c));
+    double acc = 0;
+    const int fem_row = c.fem_dof / 3;
+    for(int v = gt; v < c.V; v += gn)
+    {
+        const int s = c.real_map[v];
+        float c0, c1, c2;
+        ld4(c.Z + 4 * (size_t)s, c0, c1, c2);
+        for(int l = 1; l < c.L; l++)
+        {
+            const int now = c.coarse_table[(size_t)v * (c.L - 1) + l - 1];
+            float t0, t1, t2;
+            ld4(c.Z + 4 * (size_t)now, t0, t1, t2);
+            c0 += t0;
+            c1 += t1;
+            c2 += t2;
+        }
+        const int row = fem_row + v;
+        st4(zp + 8 * (size_t)row, (T)c0, (T)c1, (T)c2);
+        const double* r = c.r + 3 * (size_t)row;
+        acc += r[0] * (double)(T)c0 + r[1] * (double)(T)c1 + r[2] * (double)(T)c2;
+    }
+    return acc + abd_apply<T>(c, zp, gt, gn);
+}
+
+// E (global block-Jacobi / identity, then the ABD local preconditioner); share of r.z
+template <typename T>
+__device__ __forceinline__ double phase_e_plain(const PcgDev& c, int gt, int gn)
+{
+    T* zp = zpbuf<T>(c, iter_parity(c));
+    double acc = 0;
+    for(int bi = c.abd_bodies * 4 + gt; bi < c.nrows; bi += gn)
+    {
+        const double r0 = c.r[3 * bi], r1 = c.r[3 * bi + 1], r2 = c.r[3 * bi + 2];
+        double z0 = r0, z1 = r1, z2 = r2;
+        if(c.diag_inv)
+        {
+            const double* D = c.diag_inv + 9 * (size_t)bi;
             z0 = D[0] * r0 + D[3] * r1 + D[6] * r2;
             z1 = D[1] * r0 + D[4] * r1 + D[7] * r2;
             z2 = D[2] * r0 + D[5] * r1 + D[8] * r2;
         }
-        z[3 * bi] = (T)z0;
-        z[3 * bi + 1] = (T)z1;
-        z[3 * bi + 2] = (T)z2;
+        st4(zp + 8 * (size_t)bi, (T)z0, (T)z1, (T)z2);
         acc += r0 * (double)(T)z0 + r1 * (double)(T)z1 + r2 * (double)(T)z2;
     }
-    acc += abd_rows<T>(r, z, abd_inv, abd_bodies, gt, gn);
-    grid_reduce_finish<PB>(acc, ra.partials, ra.counter, op, 0, ra.scal, ra.flags, ra.p);
+    return acc + abd_apply<T>(c, zp, gt, gn);
 }
 
-// p = z + beta p
+// ---------------------------------------------------------------------------------------
+// one kernel per phase (LOOP_HOST / LOOP_GRAPH)
+// ---------------------------------------------------------------------------------------
+#define GT (blockIdx.x * PB + threadIdx.x)
+#define GN (gridDim.x * PB)
+
+// r = b, x = 0, both zp slots = 0 (p_0 = 0 so that p_1 = z_0 + 0 p_0); b.b
 template <typename T>
-__global__ void __launch_bounds__(PB) k_pcg_pupdate(T* p, const T* __restrict__ z, int n, const double* scal,
-                                                    const int* flags)
+__global__ void __launch_bounds__(PB) k_init(PcgDev c)
 {
-    if(flags[F_DONE]) return;
-    const T beta = (T)scal[SS_BETA];
-    for(int i = blockIdx.x * PB + threadIdx.x; i < n; i += gridDim.x * PB) p[i] = z[i] + beta * p[i];
+    double acc = 0;
+    T* zp0 = reinterpret_cast<T*>(c.zp0);
+    T* zp1 = reinterpret_cast<T*>(c.zp1);
+    for(int i = GT; i < c.n; i += GN)
+    {
+        const double bi = c.b[i];
+        c.r[i] = bi;
+        c.x[i] = 0.0;
+        acc += bi * bi;
+    }
+    for(int i = GT; i < 8 * c.nrows; i += GN)
+    {
+        zp0[i] = T(0);
+        zp1[i] = T(0);
+    }
+    finish_reduction(c, acc, SITE_INIT, POST_STORE, SS_BB);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(PB) k_phase_a(PcgDev c)
+{
+    if(c.flags[F_DONE]) return;
+    finish_reduction(c, phase_a<T>(c, GT, GN), SITE_A, POST_ALPHA);
+}
+
+template <typename T, int B>
+__global__ void __launch_bounds__(PB, 8) k_phase_b(PcgDev c)
+{
+    if(c.flags[F_DONE]) return;
+    const double v = B > 0 ? phase_b_mas<T, (B > 0 ? B : 16)>(c, GT, GN) : phase_b_plain<T>(c, GT, GN);
+    finish_reduction(c, v, SITE_B, POST_CHECK);
+}
+
+// guarded: runs only when this iteration is a replacement iteration (host / plain graph),
+// or unconditionally inside the graph's IF node
+__global__ void __launch_bounds__(PB) k_replace(PcgDev c, int guarded)
+{
+    if(c.flags[F_DONE]) return;
+    if(guarded)
+    {
+        const long k = (long)c.scal[SS_ITER];
+        if(c.prm.refine <= 0 || k % c.prm.refine != 0) return;
+    }
+    if(blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(c.flags + F_REPL, 1);
+    finish_reduction(c, phase_replace(c, GT, GN), SITE_R, POST_RECHECK);
+}
+
+template <int B>
+__global__ void __launch_bounds__(PB) k_restrict01(PcgDev c, int guarded)
+{
+    if(c.flags[F_DONE]) return;
+    if(guarded)
+    {
+        const long k = (long)c.scal[SS_ITER];
+        if(c.prm.refine <= 0 || k % c.prm.refine != 0) return;
+    }
+    phase_restrict01<B>(c, GT, GN);
+}
+
+// C1: level 1 -> 2 over the whole grid
+template <int B>
+__global__ void __launch_bounds__(PB) k_phase_c1(PcgDev c)
+{
+    if(c.flags[F_DONE]) return;
+    phase_c<B>(c, 1, 2, GT, GN, false);
+}
+
+// C2: levels 2 -> 3 -> ... (small) by one CTA
+template <int B>
+__global__ void __launch_bounds__(1024) k_phase_c2(PcgDev c)
+{
+    if(c.flags[F_DONE]) return;
+    phase_c<B>(c, 2, c.L - 1, threadIdx.x, blockDim.x, true);
+}
+
+template <int B>
+__global__ void __launch_bounds__(PB) k_phase_d(PcgDev c)
+{
+    if(c.flags[F_DONE]) return;
+    phase_d<B>(c, blockIdx.x, c.nbanks, gridDim.x);
+}
+
+template <typename T, int B>
+__global__ void __launch_bounds__(PB, 8) k_phase_e(PcgDev c, int op)
+{
+    if(c.flags[F_DONE]) return;
+    const double v = B > 0 ? phase_e_mas<T>(c, GT, GN) : phase_e_plain<T>(c, GT, GN);
+    finish_reduction(c, v, op == POST_INIT_RZ ? SITE_INIT_RZ : SITE_E, op);
+}
+
+// ---------------------------------------------------------------------------------------
+// persistent kernel (LOOP_PERSISTENT): all iterations in one cooperative launch
+// ---------------------------------------------------------------------------------------
+// Grid barrier that also finishes a reduction: every CTA deposits its partial, the last CTA
+// to arrive sums them in index order, applies the post-op and releases the others.  Waits
+// are bounded (~2^22 polls with backoff, a few seconds): a CTA that gives up marks the solve
+// STG_ERR_TIMEOUT and every CTA leaves at the next check instead of spinning forever.
+__device__ __forceinline__ void grid_barrier(const PcgDev& c, double v, int site, int op, unsigned& gen)
+{
+    __shared__ double red[PB / 32];
+    __shared__ bool last;
+    const double bs = (op >= 0) ? block_sum<PB>(v, red) : 0.0;
+    if(threadIdx.x == 0)
+    {
+        if(op >= 0) c.partials[(size_t)site * c.slots + blockIdx.x] = bs;
+        __threadfence();
+        last = atomicAdd(c.bar, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if(last)
+    {
+        __threadfence();
+        if(op >= 0)
+        {
+            const double* partials = c.partials + (size_t)site * c.slots;
+            double acc = 0;
+            for(int i = threadIdx.x; i < (int)gridDim.x; i += PB) acc += __ldcg(partials + i);
+            const double tot = block_sum<PB>(acc, red);
+            if(threadIdx.x == 0) post_op(op, 0, tot, c.scal, c.flags, c.prm);
+        }
+        if(threadIdx.x == 0)
+        {
+            c.bar[0] = 0u;
+            __threadfence();
+            atomicExch(c.bar + 1, gen + 1u);
+        }
+    }
+    else if(threadIdx.x == 0)
+    {
+        unsigned polls = 0, ns = 32;
+        while(true)
+        {
+            unsigned g;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(g) : "l"(c.bar + 1) : "memory");
+            if(g != gen) break;
+            if(++polls > (1u << 22))
+            {
+                atomicExch(c.flags + F_DONE, 1);
+                atomicExch(c.flags + F_STATUS, 6);  // STG_ERR_TIMEOUT
+                break;
+            }
+            __nanosleep(ns);
+            if(ns < 256) ns <<= 1;
+        }
+    }
+    gen += 1u;
+    __syncthreads();
+    __threadfence();
+}
+
+__device__ __forceinline__ bool is_done(const PcgDev& c)
+{
+    return *((volatile int*)c.flags + F_DONE) != 0;
+}
+
+template <typename T, int B>
+__global__ void __launch_bounds__(PB) k_pcg_persistent(PcgDev c)
+{
+    unsigned gen = 0;
+    const int gt = GT, gn = GN;
+    constexpr int BB = B > 0 ? B : 16;
+    // banks of levels 0..2 need only R_0..R_2 (ready after C1); the coarser ones wait for C2,
+    // which CTA 0 runs before solving them while the other CTAs solve the finer banks
+    const int split = c.L > 3 ? c.ls[2 * 3 + 1] / BB : c.nbanks;
+    for(long guard = 0; guard < c.prm.max_iter + 2; guard++)
+    {
+        if(is_done(c)) break;
+        grid_barrier(c, phase_a<T>(c, gt, gn), SITE_A, POST_ALPHA, gen);
+        if(is_done(c)) break;
+        const double vb = B > 0 ? phase_b_mas<T, BB>(c, gt, gn) : phase_b_plain<T>(c, gt, gn);
+        grid_barrier(c, vb, SITE_B, POST_CHECK, gen);
+        if(is_done(c)) break;
+        const long k = (long)__ldcg(c.scal + SS_ITER);
+        if(c.prm.refine > 0 && k % c.prm.refine == 0)
+        {
+            if(blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(c.flags + F_REPL, 1);
+            grid_barrier(c, phase_replace(c, gt, gn), SITE_R, POST_RECHECK, gen);
+            if(is_done(c)) break;
+            if(B > 0)
+            {
+                phase_restrict01<BB>(c, gt, gn);
+                grid_barrier(c, 0.0, 0, -1, gen);
+            }
+        }
+        if(B > 0)
+        {
+            phase_c<BB>(c, 1, 2, gt, gn, false);
+            grid_barrier(c, 0.0, 0, -1, gen);
+            if(gridDim.x == 1)
+            {
+                phase_c<BB>(c, 2, c.L - 1, threadIdx.x, blockDim.x, true);
+                phase_d<BB>(c, 0, c.nbanks, 1);
+            }
+            else if(blockIdx.x == 0)
+            {
+                phase_c<BB>(c, 2, c.L - 1, threadIdx.x, blockDim.x, true);
+                phase_d<BB>(c, split, c.nbanks, 1);
+            }
+            else
+                phase_d<BB>(c, blockIdx.x - 1, split, gridDim.x - 1);
+            grid_barrier(c, 0.0, 0, -1, gen);
+        }
+        const double ve = B > 0 ? phase_e_mas<T>(c, gt, gn) : phase_e_plain<T>(c, gt, gn);
+        grid_barrier(c, ve, SITE_E, POST_BETA, gen);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// layout preparation
+// ---------------------------------------------------------------------------------------
+__global__ void k_pack_blocks(const double* __restrict__ src, int nnzb, float* dst32, double* dst64)
+{
+    for(int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnzb; k += gridDim.x * blockDim.x)
+    {
+        const double* s = src + 9 * (size_t)k;
+        if(dst32)
+        {
+            float4* d = reinterpret_cast<float4*>(dst32) + 3 * (size_t)k;
+            d[0] = make_float4((float)s[0], (float)s[1], (float)s[2], (float)s[3]);
+            d[1] = make_float4((float)s[4], (float)s[5], (float)s[6], (float)s[7]);
+            d[2] = make_float4((float)s[8], 0.f, 0.f, 0.f);
+        }
+        if(dst64)
+        {
+            double2* d = reinterpret_cast<double2*>(dst64) + 5 * (size_t)k;
+            d[0] = make_double2(s[0], s[1]);
+            d[1] = make_double2(s[2], s[3]);
+            d[2] = make_double2(s[4], s[5]);
+            d[3] = make_double2(s[6], s[7]);
+            d[4] = make_double2(s[8], 0.0);
+        }
+    }
+}
+
+// Full symmetric row-sliced SoA copy used by the PCG SpMV (phase A): row i holds, sorted by
+// column, its lower blocks (transposes of the upper blocks k with col(k) == i, from the
+// transpose list) followed by its upper blocks; entry e of row i sits at
+// f = row_ptr[i] + t_ptr[i] + e, its column in fcol[f] and component t (column-major) in
+// plane t: fval[t * stride + f].  The 16 lanes of a row read consecutive entries of every
+// plane, so each block component is one coalesced 64-byte access and no block is fetched
+// from a random address.
+template <typename T>
+__global__ void k_build_full(const int* __restrict__ row_ptr, const int* __restrict__ cols,
+                             const int* __restrict__ t_ptr, const int2* __restrict__ t_ent,
+                             const double* __restrict__ blocks, int nrows, size_t stride, int* fcol, T* fval)
+{
+    for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrows; i += gridDim.x * blockDim.x)
+    {
+        size_t f = (size_t)row_ptr[i] + t_ptr[i];
+        for(int e = t_ptr[i]; e < t_ptr[i + 1]; e++, f++)
+        {
+            const int2 te = t_ent[e];
+            const double* H = blocks + 9 * (size_t)te.x;
+            fcol[f] = te.y;
+#pragma unroll
+            for(int a = 0; a < 3; a++)
+#pragma unroll
+                for(int b = 0; b < 3; b++) fval[(size_t)(b * 3 + a) * stride + f] = (T)H[a * 3 + b];  // H^T
+        }
+        for(int k = row_ptr[i]; k < row_ptr[i + 1]; k++, f++)
+        {
+            const double* H = blocks + 9 * (size_t)k;
+            fcol[f] = cols[k];
+#pragma unroll
+            for(int t = 0; t < 9; t++) fval[(size_t)t * stride + f] = (T)H[t];
+        }
+    }
+}
+
+int pack_blocks(Solver& S)
+{
+    Bcoo& A = S.bcoo;
+    const int nnzb = A.nnzb;
+    if(nnzb < 1) return 0;
+    STG_TRY(A.blk64p.resize((size_t)nnzb * 10));
+    const bool fp32 = S.cfg.precision == STG_PREC_FP32;
+    k_pack_blocks<<<std::max(1, std::min(div_up(nnzb, 256), kSMs * 16)), 256, 0, S.stream>>>(A.B(), nnzb, nullptr,
+                                                                                           A.blk64p.data());
+    STG_LAUNCH_CHECK();
+    // full symmetric copy: at most 2 * nnzb entries
+    A.fstride = (size_t)2 * nnzb;
+    STG_TRY(A.fcol.resize(A.fstride));
+    const int g = std::max(1, std::min(div_up(A.nrows, 128), kSMs * 16));
+    if(fp32)
+    {
+        STG_TRY(A.fval32.resize(9 * A.fstride));
+        k_build_full<float><<<g, 128, 0, S.stream>>>(A.row_ptr.data(), A.C(), A.t_ptr.data(), A.t_ent.data(), A.B(),
+                                                     A.nrows, A.fstride, A.fcol.data(), A.fval32.data());
+    }
+    else
+    {
+        STG_TRY(A.fval64.resize(9 * A.fstride));
+        k_build_full<double><<<g, 128, 0, S.stream>>>(A.row_ptr.data(), A.C(), A.t_ptr.data(), A.t_ent.data(), A.B(),
+                                                      A.nrows, A.fstride, A.fcol.data(), A.fval64.data());
+    }
+    STG_LAUNCH_CHECK();
+    S.launches += 2;
+    return 0;
 }
 
 // ---------------------------------------------------------------------------------------
 // host driver
 // ---------------------------------------------------------------------------------------
-struct PcgLaunch
+// MAS levels >= 2 restriction (C1 parallel, C2 one CTA) and the bank solves (D)
+template <int B>
+static int launch_mas_cd(Solver& S, const PcgDev& c)
 {
-    Solver* S;
-    int n, nrows;
-    int grid_vec, grid_rows;
-    RedArgs ra[6];  // one counter per reduction site
-    const double* b;
-    double* x;
-    int abd_bodies;
-    const double* abd_inv;
-};
-
-static int launch_precond(PcgLaunch& L, int op, int site)
-{
-    Solver& S = *L.S;
     cudaStream_t s = S.stream;
-    const bool fp32 = S.cfg.precision == STG_PREC_FP32;
-    PcgState& P = S.pcg;
-    if(S.cfg.preconditioner == STG_PRECOND_MAS)
+    if(c.L > 2)
     {
-        const int fem_dof = 3 * (S.mas_fem_offset);
-        STG_TRY(mas_restrict_solve_guarded(S, P.r.data() + fem_dof, P.flags.data()));
-        const int g = std::max(1, std::min(div_up(S.mas.V, PB), kSMs * 4));
-        if(fp32)
-            k_pcg_prolong<float><<<g, PB, 0, s>>>(S.mas.Z.data(), S.mas.real_map.data(), S.mas.coarse_table.data(), S.mas.L,
-                                                  S.mas.V, fem_dof, P.r.data(), P.z32.data(), L.abd_inv, L.abd_bodies, op,
-                                                  L.ra[site]);
-        else
-            k_pcg_prolong<double><<<g, PB, 0, s>>>(S.mas.Z.data(), S.mas.real_map.data(), S.mas.coarse_table.data(), S.mas.L,
-                                                   S.mas.V, fem_dof, P.r.data(), P.z.data(), L.abd_inv, L.abd_bodies, op,
-                                                   L.ra[site]);
+        const int n1 = (c.ls[2] + 31) / 32 * 32;
+        k_phase_c1<B><<<std::max(1, std::min(div_up(n1, PB), kSMs * 4)), PB, 0, s>>>(c);
         STG_LAUNCH_CHECK();
         S.launches++;
-        return 0;
     }
-    const double* dinv = S.cfg.preconditioner == STG_PRECOND_DIAG ? S.bcoo.diag_inv.data() : nullptr;
-    if(fp32)
-        k_pcg_diag<float><<<L.grid_rows, PB, 0, s>>>(dinv, P.r.data(), P.z32.data(), L.nrows, L.abd_inv, L.abd_bodies, op,
-                                                     L.ra[site]);
+    if(c.L > 3)
+    {
+        k_phase_c2<B><<<1, 1024, 0, s>>>(c);
+        STG_LAUNCH_CHECK();
+        S.launches++;
+    }
+    if(B == 16)
+    {
+        // warp per bank, TMA-staged; one resident wave of CTAs
+        const int smem = D_WARPS * D_WARP_BYTES;
+        static thread_local int attr_done = 0;
+        if(!attr_done)
+        {
+            STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_d16, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            attr_done = 1;
+        }
+        int per_sm = 0;
+        STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase_d16, D_WARPS * 32, smem));
+        const int grid = std::max(1, std::min(div_up(c.nbanks, D_WARPS), std::max(per_sm, 1) * kSMs));
+        k_phase_d16<<<grid, D_WARPS * 32, smem, s>>>(c);
+    }
     else
-        k_pcg_diag<double><<<L.grid_rows, PB, 0, s>>>(dinv, P.r.data(), P.z.data(), L.nrows, L.abd_inv, L.abd_bodies, op,
-                                                      L.ra[site]);
+        k_phase_d<B><<<std::max(1, std::min(c.nbanks, kSMs * 8)), PB, 0, s>>>(c);
     STG_LAUNCH_CHECK();
     S.launches++;
     return 0;
 }
 
-// one PCG iteration (k >= 1)
-static int launch_iteration(PcgLaunch& L)
+// (row, col) of every packed upper block of a 16-bank, for k_phase_d16
+static int upload_upper16(cudaStream_t s)
 {
-    Solver& S = *L.S;
+    static unsigned char tab[136][2];
+    int k = 0;
+    for(int a = 0; a < 16; a++)
+        for(int col = a; col < 16; col++, k++)
+        {
+            tab[k][0] = (unsigned char)a;
+            tab[k][1] = (unsigned char)col;
+        }
+    STG_CUDA_TRY(cudaMemcpyToSymbolAsync(c_upper16, tab, sizeof(tab), 0, cudaMemcpyHostToDevice, s));
+    return 0;
+}
+
+template <typename T, int B>
+static int launch_iteration(Solver& S, const PcgDev& c, int grid_vec, int grid_rows, bool in_graph_cond)
+{
+    cudaStream_t s = S.stream;
+    const bool fp32 = sizeof(T) == 4;
+    k_phase_a<T><<<grid_rows, PB, 0, s>>>(c);
+    STG_LAUNCH_CHECK();
+    k_phase_b<T, B><<<B > 0 ? std::max(1, std::min(div_up(c.M, PB), kSMs * 4)) : grid_vec, PB, 0, s>>>(c);
+    STG_LAUNCH_CHECK();
+    S.launches += 2;
+    if(fp32 && c.prm.refine > 0)
+    {
+        if(in_graph_cond)
+        {
+            // IF node: replacement (+ re-restriction) only on replacement iterations
+            cudaStreamCaptureStatus st;
+            cudaGraph_t capg;
+            const cudaGraphNode_t* deps;
+            size_t ndeps = 0;
+            STG_CUDA_TRY(cudaStreamGetCaptureInfo(s, &st, nullptr, &capg, &deps, &ndeps));
+            cudaGraphNodeParams ip = {};
+            ip.type = cudaGraphNodeTypeConditional;
+            ip.conditional.handle = c.h_if;
+            ip.conditional.type = cudaGraphCondTypeIf;
+            ip.conditional.size = 1;
+            cudaGraphNode_t ifnode;
+            STG_CUDA_TRY(cudaGraphAddNode(&ifnode, capg, deps, ndeps, &ip));
+            STG_CUDA_TRY(cudaStreamUpdateCaptureDependencies(s, &ifnode, 1, cudaStreamSetCaptureDependencies));
+            // the IF body is recorded by the caller (see record_if_body)
+            S.pending_if_body = ip.conditional.phGraph_out[0];
+        }
+        else
+        {
+            k_replace<<<grid_rows, PB, 0, s>>>(c, 1);
+            STG_LAUNCH_CHECK();
+            S.launches++;
+            if(B > 0)
+            {
+                k_restrict01<(B > 0 ? B : 16)><<<std::max(1, std::min(div_up(c.M, PB), kSMs * 4)), PB, 0, s>>>(c, 1);
+                STG_LAUNCH_CHECK();
+                S.launches++;
+            }
+        }
+    }
+    if(B > 0) STG_TRY(launch_mas_cd<(B > 0 ? B : 16)>(S, c));
+    k_phase_e<T, B><<<grid_vec, PB, 0, s>>>(c, POST_BETA);
+    STG_LAUNCH_CHECK();
+    S.launches++;
+    return 0;
+}
+
+template <typename T, int B>
+static int record_if_body(Solver& S, const PcgDev& c, int grid_rows, cudaGraph_t body)
+{
+    cudaStream_t s = S.stream;
+    STG_CUDA_TRY(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    k_replace<<<grid_rows, PB, 0, s>>>(c, 0);
+    cudaError_t e1 = cudaGetLastError();
+    if(B > 0 && e1 == cudaSuccess)
+    {
+        k_restrict01<(B > 0 ? B : 16)><<<std::max(1, std::min(div_up(c.M, PB), kSMs * 4)), PB, 0, s>>>(c, 0);
+        e1 = cudaGetLastError();
+    }
+    cudaGraph_t out = body;
+    cudaError_t e2 = cudaStreamEndCapture(s, &out);
+    STG_CUDA_TRY(e1);
+    STG_CUDA_TRY(e2);
+    return 0;
+}
+
+template <typename T, int B>
+static int pcg_run(Solver& S, PcgDev& c, int& h_done)
+{
     cudaStream_t s = S.stream;
     PcgState& P = S.pcg;
-    Bcoo& A = S.bcoo;
-    const bool fp32 = S.cfg.precision == STG_PREC_FP32;
-    if(fp32)
-    {
-        k_pcg_spmv<float><<<L.grid_rows, PB, 0, s>>>(A.row_ptr.data(), A.C(), A.blocks32.data(), A.t_ptr.data(),
-                                                     A.t_ent.data(), P.p32.data(), P.q32.data(), L.nrows, L.ra[0]);
-        STG_LAUNCH_CHECK();
-        k_pcg_axpy<float><<<L.grid_vec, PB, 0, s>>>(L.x, P.r.data(), P.p32.data(), P.q32.data(), L.n, L.ra[1]);
-        STG_LAUNCH_CHECK();
-        k_pcg_replace<<<L.grid_rows, PB, 0, s>>>(A.row_ptr.data(), A.C(), A.B(), A.t_ptr.data(), A.t_ent.data(), L.x, L.b,
-                                                P.r.data(), L.nrows, L.ra[2]);
-        STG_LAUNCH_CHECK();
-        S.launches += 3;
-    }
-    else
-    {
-        k_pcg_spmv<double><<<L.grid_rows, PB, 0, s>>>(A.row_ptr.data(), A.C(), A.B(), A.t_ptr.data(), A.t_ent.data(),
-                                                      P.p.data(), P.q.data(), L.nrows, L.ra[0]);
-        STG_LAUNCH_CHECK();
-        k_pcg_axpy<double><<<L.grid_vec, PB, 0, s>>>(L.x, P.r.data(), P.p.data(), P.q.data(), L.n, L.ra[1]);
-        STG_LAUNCH_CHECK();
-        S.launches += 2;
-    }
-    STG_TRY(launch_precond(L, POST_BETA, 3));
-    if(fp32)
-        k_pcg_pupdate<float><<<L.grid_vec, PB, 0, s>>>(P.p32.data(), P.z32.data(), L.n, P.scal.data(), P.flags.data());
-    else
-        k_pcg_pupdate<double><<<L.grid_vec, PB, 0, s>>>(P.p.data(), P.z.data(), L.n, P.scal.data(), P.flags.data());
+    const int grid_vec = std::max(1, std::min(div_up(c.n, PB), kSMs * 4));
+    // the SpMV phase runs as exactly one resident wave (grid-stride over the rows)
+    int per_sm_a = 0;
+    STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_a, k_phase_a<T>, PB, 0));
+    const int grid_rows = std::max(1, std::min(div_up(c.nrows, PB / 16), std::max(per_sm_a, 1) * kSMs));
+    const int grid_b = B > 0 ? std::max(1, std::min(div_up(c.M, PB), kSMs * 4)) : grid_vec;
+    // init: r = b, x = 0, p = 0, b.b; z = M^-1 r, rz = rz0 = r.z (beta = 0 so p_new = z)
+    k_init<T><<<grid_vec, PB, 0, s>>>(c);
     STG_LAUNCH_CHECK();
     S.launches++;
+    if(B > 0)
+    {
+        constexpr int BB = B > 0 ? B : 16;
+        k_restrict01<BB><<<grid_b, PB, 0, s>>>(c, 0);
+        STG_LAUNCH_CHECK();
+        S.launches++;
+        STG_TRY(launch_mas_cd<BB>(S, c));
+    }
+    k_phase_e<T, B><<<grid_vec, PB, 0, s>>>(c, POST_INIT_RZ);
+    STG_LAUNCH_CHECK();
+    S.launches++;
+
+    int h_flags[4] = {0, 0, 0, 0};
+    const long max_iter = c.prm.max_iter;
+    if(max_iter <= 1)
+    {
+        h_done = 1;
+        return 0;
+    }
+    const int mode = S.cfg.loop_mode;
+    if(mode == STG_LOOP_HOST)
+    {
+        for(long it = 1; it <= max_iter; it++)
+        {
+            STG_TRY((launch_iteration<T, B>(S, c, grid_vec, grid_rows, false)));
+            STG_CUDA_TRY(cudaMemcpyAsync(h_flags, P.flags.data(), sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
+            STG_CUDA_TRY(cudaStreamSynchronize(s));
+            if(h_flags[F_DONE]) break;
+        }
+    }
+    else if(mode == STG_LOOP_GRAPH)
+    {
+        // graph: WHILE(cond) { iteration }, cond initialised to 1 and set by the stop test
+        if(P.graph)
+        {
+            cudaGraphExecDestroy(P.graph);
+            P.graph = nullptr;
+        }
+        if(!S.capture_stream) STG_CUDA_TRY(cudaStreamCreateWithFlags(&S.capture_stream, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        STG_CUDA_TRY(cudaGraphCreate(&g, 0));
+        int rc = 0;
+        do
+        {
+            // a conditional handle must belong to exactly one conditional node: the IF handle
+            // exists only when the body holds the residual-replacement node (FP32 mode)
+            const bool need_if = sizeof(T) == 4 && c.prm.refine > 0;
+            cudaGraphConditionalHandle hw = 0, hi = 0;
+            if(cudaGraphConditionalHandleCreate(&hw, g, 1, cudaGraphCondAssignDefault) != cudaSuccess ||
+               (need_if && cudaGraphConditionalHandleCreate(&hi, g, 0, cudaGraphCondAssignDefault) != cudaSuccess))
+            {
+                set_error(std::string("cudaGraphConditionalHandleCreate failed: ") + cudaGetErrorString(cudaGetLastError()));
+                rc = STG_ERR_CUDA;
+                break;
+            }
+            c.h_while = hw;
+            c.h_if = hi;
+            c.use_cond = need_if ? 2 : 1;  // 2: the stop test also drives the IF node
+            cudaGraphNodeParams wp = {};
+            wp.type = cudaGraphNodeTypeConditional;
+            wp.conditional.handle = hw;
+            wp.conditional.type = cudaGraphCondTypeWhile;
+            wp.conditional.size = 1;
+            cudaGraphNode_t wnode;
+            if(cudaGraphAddNode(&wnode, g, nullptr, 0, &wp) != cudaSuccess)
+            {
+                set_error(std::string("cudaGraphAddNode(WHILE) failed: ") + cudaGetErrorString(cudaGetLastError()));
+                rc = STG_ERR_CUDA;
+                break;
+            }
+            cudaGraph_t body = wp.conditional.phGraph_out[0];
+            cudaStream_t user = S.stream;
+            S.stream = S.capture_stream;
+            S.pending_if_body = nullptr;
+            cudaError_t cb = cudaStreamBeginCaptureToGraph(S.stream, body, nullptr, nullptr, 0,
+                                                           cudaStreamCaptureModeThreadLocal);
+            if(cb != cudaSuccess)
+            {
+                S.stream = user;
+                set_error(std::string("cudaStreamBeginCaptureToGraph failed: ") + cudaGetErrorString(cb));
+                rc = STG_ERR_CUDA;
+                break;
+            }
+            const int l0 = S.launches;
+            rc = launch_iteration<T, B>(S, c, grid_vec, grid_rows, true);
+            cudaGraph_t out = body;
+            cudaError_t ce = cudaStreamEndCapture(S.stream, &out);
+            if(rc == 0 && ce != cudaSuccess)
+            {
+                set_error(std::string("cudaStreamEndCapture failed: ") + cudaGetErrorString(ce));
+                rc = STG_ERR_CUDA;
+            }
+            if(rc == 0 && S.pending_if_body) rc = record_if_body<T, B>(S, c, grid_rows, S.pending_if_body);
+            S.stream = user;
+            S.launches_per_batch = S.launches - l0;
+            S.launches = l0;
+            if(rc) break;
+            cudaError_t ie = cudaGraphInstantiate(&P.graph, g, 0);
+            if(ie != cudaSuccess)
+            {
+                set_error(std::string("cudaGraphInstantiate failed: ") + cudaGetErrorString(ie));
+                rc = STG_ERR_CUDA;
+            }
+        } while(0);
+        cudaGraphDestroy(g);
+        if(rc) return rc;
+        STG_CUDA_TRY(cudaGraphLaunch(P.graph, s));
+        STG_CUDA_TRY(cudaMemcpyAsync(h_flags, P.flags.data(), sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
+        STG_CUDA_TRY(cudaStreamSynchronize(s));
+        c.use_cond = 0;
+    }
+    else
+    {
+        // persistent cooperative kernel: every CTA must be resident
+        int per_sm = 0;
+        STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_persistent<T, B>, PB, 0));
+        int dev = 0, sms = kSMs;
+        STG_CUDA_TRY(cudaGetDevice(&dev));
+        STG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        const int grid = std::max(1, std::min(per_sm, 4) * sms);
+        if(grid > c.slots)
+        {
+            set_error("persistent grid larger than the reduction slots");
+            return STG_ERR_INVALID;
+        }
+        STG_CUDA_TRY(cudaMemsetAsync(c.bar, 0, sizeof(unsigned) * 2, s));
+        void* args[] = {&c};
+        STG_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_pcg_persistent<T, B>, grid, PB, args, 0, s));
+        S.launches++;
+        STG_CUDA_TRY(cudaMemcpyAsync(h_flags, P.flags.data(), sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
+        STG_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    h_done = h_flags[F_DONE];
     return 0;
 }
 
-// Times `reps` launches of the PCG SpMV (q = A p, p.q fused) on the last solved system.
+// Times `reps` launches of the phase-A SpMV on the last solved system (measurement hook).
 int profile_spmv(Solver& S, int reps, float* avg_ms, double* bytes)
 {
-    const bool fp32 = S.cfg.precision == STG_PREC_FP32;
-    PcgState& P = S.pcg;
-    const int nrows = S.bcoo.nrows, n = 3 * nrows;
-    if(nrows < 1 || P.partials.size == 0 || (fp32 ? P.p32.size : P.p.size) < (size_t)n)
+    if(!S.pcg_ready)
     {
         set_error("stg_profile_spmv: run a solve first");
         return STG_ERR_NOT_READY;
     }
+    const bool fp32 = S.cfg.precision == STG_PREC_FP32;
+    PcgDev c = S.pcg_dev;
     cudaStream_t s = S.stream;
-    const int grid_rows = std::max(1, std::min(div_up(nrows, PB / 16), kSMs * 8));
-    const int slots = (int)(P.partials.size / 6);
-    if(grid_rows > slots)
-    {
-        set_error("stg_profile_spmv: partial buffer too small");
-        return STG_ERR_INVALID;
-    }
-    PcgParams prm{1e-4, 1 << 30, 0, 0};
-    RedArgs ra{P.partials.data(), P.counters.data(), P.scal.data(), P.flags.data(), prm};
-    // the solve left flags[F_DONE] set; clear it so the kernel runs, restore afterwards
+    int per_sm_a = 0;
+    if(fp32)
+        STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_a, k_phase_a<float>, PB, 0));
+    else
+        STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_a, k_phase_a<double>, PB, 0));
+    const int grid_rows = std::max(1, std::min(div_up(c.nrows, PB / 16), std::max(per_sm_a, 1) * kSMs));
     int saved[4];
-    STG_CUDA_TRY(cudaMemcpyAsync(saved, P.flags.data(), sizeof(saved), cudaMemcpyDeviceToHost, s));
-    STG_CUDA_TRY(cudaMemsetAsync(P.flags.data(), 0, sizeof(int) * 4, s));
-    Bcoo& A = S.bcoo;
+    STG_CUDA_TRY(cudaMemcpyAsync(saved, c.flags, sizeof(saved), cudaMemcpyDeviceToHost, s));
+    STG_CUDA_TRY(cudaStreamSynchronize(s));
+    STG_CUDA_TRY(cudaMemsetAsync(c.flags, 0, sizeof(int) * 4, s));
     auto launch = [&]() {
         if(fp32)
-            k_pcg_spmv<float><<<grid_rows, PB, 0, s>>>(A.row_ptr.data(), A.C(), A.blocks32.data(), A.t_ptr.data(),
-                                                       A.t_ent.data(), P.p32.data(), P.q32.data(), nrows, ra);
+            k_phase_a<float><<<grid_rows, PB, 0, s>>>(c);
         else
-            k_pcg_spmv<double><<<grid_rows, PB, 0, s>>>(A.row_ptr.data(), A.C(), A.B(), A.t_ptr.data(), A.t_ent.data(),
-                                                        P.p.data(), P.q.data(), nrows, ra);
+            k_phase_a<double><<<grid_rows, PB, 0, s>>>(c);
     };
     for(int i = 0; i < 3; i++) launch();
     STG_LAUNCH_CHECK();
@@ -357,11 +1390,11 @@ int profile_spmv(Solver& S, int reps, float* avg_ms, double* bytes)
     float ms = 0;
     STG_CUDA_TRY(cudaEventElapsedTime(&ms, S.ev[4], S.ev[5]));
     S.launches += reps + 3;
-    STG_CUDA_TRY(cudaMemcpyAsync(P.flags.data(), saved, sizeof(saved), cudaMemcpyHostToDevice, s));
+    STG_CUDA_TRY(cudaMemcpyAsync(c.flags, saved, sizeof(saved), cudaMemcpyHostToDevice, s));
     STG_CUDA_TRY(cudaStreamSynchronize(s));
     if(avg_ms) *avg_ms = ms / std::max(reps, 1);
     const double blk = fp32 ? 36.0 : 72.0, vec = fp32 ? 4.0 : 8.0;
-    if(bytes) *bytes = (double)A.nnzb * (blk + 8.0) + 3.0 * n * vec;
+    if(bytes) *bytes = (double)S.bcoo.nnzb * (blk + 8.0) + 3.0 * c.n * vec;
     return 0;
 }
 
@@ -369,147 +1402,124 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
 {
     cudaStream_t s = stream;
     const bool fp32 = cfg.precision == STG_PREC_FP32;
+    const bool use_mas = cfg.preconditioner == STG_PRECOND_MAS;
     if(n != 3 * bcoo.nrows)
     {
         set_error("stg_pcg_solve: n must be 3 * block rows of the BCOO");
         return STG_ERR_INVALID;
     }
-    if(cfg.preconditioner == STG_PRECOND_MAS && !mas.assembled)
+    if(use_mas && !mas.assembled)
     {
         set_error("stg_pcg_solve: MAS preconditioner not assembled");
         return STG_ERR_NOT_READY;
     }
+    if(use_mas && 3 * (mas_fem_offset + mas.V) > n)
+    {
+        set_error("stg_pcg_solve: MAS range exceeds the system");
+        return STG_ERR_INVALID;
+    }
     PcgState& P = pcg;
+    const size_t es = fp32 ? sizeof(float) : sizeof(double);
     STG_TRY(P.r.resize(n));
-    if(fp32)
-    {
-        STG_TRY(P.p32.resize(n));
-        STG_TRY(P.q32.resize(n));
-        STG_TRY(P.z32.resize(n));
-    }
-    else
-    {
-        STG_TRY(P.p.resize(n));
-        STG_TRY(P.q.resize(n));
-        STG_TRY(P.z.resize(n));
-    }
-    const int nrows = bcoo.nrows;
-    PcgLaunch L;
-    L.S = this;
-    L.n = n;
-    L.nrows = nrows;
-    L.grid_vec = std::max(1, std::min(div_up(n, PB), kSMs * 4));
-    L.grid_rows = std::max(1, std::min(div_up(nrows, PB / 16), kSMs * 8));
-    const int slots = std::max(L.grid_vec, std::max(L.grid_rows, kSMs * 4));
+    const size_t nr = (size_t)bcoo.nrows;
+    // zp0, zp1 (8 slots per block row), q (4 slots), each region 256-byte aligned
+    const size_t zp_bytes = (8 * nr * es + 255) / 256 * 256, q_bytes = (4 * nr * es + 255) / 256 * 256;
+    STG_TRY(P.vbuf.resize((2 * zp_bytes + q_bytes) / sizeof(double) + 32));
+    STG_TRY(pack_blocks(*this));
+    if(use_mas && cfg.bank_size == 16) STG_TRY(upload_upper16(s));
+    const int slots = kSMs * 8;
     STG_TRY(P.partials.resize((size_t)slots * 6));
     STG_TRY(P.scal.resize(S_COUNT));
     STG_TRY(P.counters.resize(8));
     STG_TRY(P.flags.resize(4));
+    STG_TRY(P.bar.resize(2));
     STG_CUDA_TRY(cudaMemsetAsync(P.counters.data(), 0, sizeof(unsigned) * 8, s));
     STG_CUDA_TRY(cudaMemsetAsync(P.flags.data(), 0, sizeof(int) * 4, s));
     STG_CUDA_TRY(cudaMemsetAsync(P.scal.data(), 0, sizeof(double) * S_COUNT, s));
-    PcgParams prm;
-    prm.tol = cfg.tol;
-    prm.max_iter = (long)(cfg.max_iter_ratio * (double)n);
-    prm.stop_rule = cfg.stop_rule;
-    prm.refine = fp32 ? cfg.refine_interval : 0;
-    for(int i = 0; i < 6; i++)
-        L.ra[i] = RedArgs{P.partials.data() + (size_t)i * slots, P.counters.data() + i, P.scal.data(), P.flags.data(), prm};
-    L.b = b;
-    L.x = x;
-    L.abd_bodies = abd_bodies;
-    L.abd_inv = abd_inv;
 
-    k_pcg_init<<<L.grid_vec, PB, 0, s>>>(b, P.r.data(), x, fp32 ? nullptr : P.p.data(), fp32 ? P.p32.data() : nullptr, n,
-                                         L.ra[4]);
-    STG_LAUNCH_CHECK();
-    launches++;
-    STG_TRY(launch_precond(L, POST_INIT_RZ, 5));
-    // p = z (beta = 0, p = 0)
+    PcgDev c = {};
+    c.row_ptr = bcoo.row_ptr.data();
+    c.cols = bcoo.C();
+    c.t_ptr = bcoo.t_ptr.data();
+    c.t_ent = bcoo.t_ent.data();
+    c.blk64 = reinterpret_cast<const double2*>(bcoo.blk64p.data());
+    c.fcol = bcoo.fcol.data();
+    c.fval = fp32 ? (const void*)bcoo.fval32.data() : (const void*)bcoo.fval64.data();
+    c.fstride = bcoo.fstride;
+    c.nrows = bcoo.nrows;
+    c.n = n;
+    char* vb = reinterpret_cast<char*>(P.vbuf.data());
+    c.zp0 = vb;
+    c.zp1 = vb + zp_bytes;
+    c.q = vb + 2 * zp_bytes;
+    c.x = x;
+    c.r = P.r.data();
+    c.b = b;
+    if(use_mas)
+    {
+        c.part_map = mas.part_map.data();
+        c.fine_mask = mas.fine_mask.data();
+        c.going_next = mas.going_next.data();
+        c.closed = mas.closed.data();
+        c.R = mas.R.data();
+        c.Z = mas.Z.data();
+        c.inv = mas.inv.data();
+        c.real_map = mas.real_map.data();
+        c.coarse_table = mas.coarse_table.data();
+        c.M = mas.M;
+        c.V = mas.V;
+        c.L = mas.L;
+        c.nbanks = mas.nbanks;
+        c.fem_dof = 3 * mas_fem_offset;
+        c.identity = mas.identity ? 1 : 0;
+        for(int i = 0; i < 2 * (kMaxLevels + 1); i++) c.ls[i] = mas.level_size[i];
+        c.ls_dev = reinterpret_cast<const int*>(mas.level_size_d.data());
+    }
+    c.diag_inv = cfg.preconditioner == STG_PRECOND_DIAG ? bcoo.diag_inv.data() : nullptr;
+    c.abd_bodies = abd_bodies;
+    c.abd_inv = abd_inv;
+    c.partials = P.partials.data();
+    c.counters = P.counters.data();
+    c.scal = P.scal.data();
+    c.flags = P.flags.data();
+    c.slots = slots;
+    c.prm.tol = cfg.tol;
+    c.prm.max_iter = (long)(cfg.max_iter_ratio * (double)n);
+    c.prm.stop_rule = cfg.stop_rule;
+    c.prm.refine = fp32 ? cfg.refine_interval : 0;
+    c.bar = P.bar.data();
+
+    int done = 0;
     if(fp32)
-        k_pcg_pupdate<float><<<L.grid_vec, PB, 0, s>>>(P.p32.data(), P.z32.data(), n, P.scal.data(), P.flags.data());
+    {
+        if(!use_mas)
+            STG_TRY((pcg_run<float, 0>(*this, c, done)));
+        else if(cfg.bank_size == 32)
+            STG_TRY((pcg_run<float, 32>(*this, c, done)));
+        else
+            STG_TRY((pcg_run<float, 16>(*this, c, done)));
+    }
     else
-        k_pcg_pupdate<double><<<L.grid_vec, PB, 0, s>>>(P.p.data(), P.z.data(), n, P.scal.data(), P.flags.data());
-    STG_LAUNCH_CHECK();
-    launches++;
+    {
+        if(!use_mas)
+            STG_TRY((pcg_run<double, 0>(*this, c, done)));
+        else if(cfg.bank_size == 32)
+            STG_TRY((pcg_run<double, 32>(*this, c, done)));
+        else
+            STG_TRY((pcg_run<double, 16>(*this, c, done)));
+    }
+    pcg_dev = c;
+    pcg_ready = true;
 
-    int h_flags[4] = {0, 0, 0, 0};
-    const long max_iter = prm.max_iter;
-    if(max_iter <= 1)
-    {
-        // the loop body never runs; the reference returns k = 1
-        h_flags[F_DONE] = 1;
-    }
-    else if(cfg.loop_mode == STG_LOOP_HOST)
-    {
-        for(long it = 1; it < max_iter + 1; it++)
-        {
-            STG_TRY(launch_iteration(L));
-            STG_CUDA_TRY(cudaMemcpyAsync(h_flags, P.flags.data(), sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
-            STG_CUDA_TRY(cudaStreamSynchronize(s));
-            if(h_flags[F_DONE]) break;
-        }
-    }
-    else
-    {
-        const int batch = std::max(1, cfg.graph_batch);
-        // capture `batch` iterations once per problem shape
-        const long long key[8] = {n, nrows, bcoo.nnzb, mas.total_clusters, generation, (long long)(intptr_t)x,
-                                  (long long)(intptr_t)b, batch};
-        bool same = P.graph != nullptr;
-        for(int i = 0; i < 8 && same; i++) same = P.graph_key[i] == key[i];
-        if(!same || graph_dirty)
-        {
-            if(P.graph)
-            {
-                cudaGraphExecDestroy(P.graph);
-                P.graph = nullptr;
-            }
-            // the legacy default stream cannot be captured: record the kernels on a private
-            // stream; the instantiated graph is then launched on the caller's stream
-            if(!capture_stream) STG_CUDA_TRY(cudaStreamCreateWithFlags(&capture_stream, cudaStreamNonBlocking));
-            cudaGraph_t g = nullptr;
-            stream = capture_stream;
-            cudaError_t cb = cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal);
-            if(cb != cudaSuccess)
-            {
-                stream = s;
-                STG_CUDA_TRY(cb);
-            }
-            int rc = 0;
-            const int l0 = launches;
-            for(int it = 0; it < batch && rc == 0; it++) rc = launch_iteration(L);
-            cudaError_t ce = cudaStreamEndCapture(capture_stream, &g);
-            stream = s;
-            launches_per_batch = launches - l0;
-            launches = l0;
-            if(rc)
-            {
-                if(g) cudaGraphDestroy(g);
-                return rc;
-            }
-            STG_CUDA_TRY(ce);
-            STG_CUDA_TRY(cudaGraphInstantiate(&P.graph, g, 0));
-            cudaGraphDestroy(g);
-            for(int i = 0; i < 8; i++) P.graph_key[i] = key[i];
-            graph_dirty = false;
-        }
-        const long max_batches = max_iter / batch + 2;
-        for(long bt = 0; bt < max_batches; bt++)
-        {
-            STG_CUDA_TRY(cudaGraphLaunch(P.graph, s));
-            launches += launches_per_batch;
-            STG_CUDA_TRY(cudaMemcpyAsync(h_flags, P.flags.data(), sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
-            STG_CUDA_TRY(cudaStreamSynchronize(s));
-            if(h_flags[F_DONE]) break;
-        }
-    }
     double h_scal[S_COUNT];
+    int h_flags[4];
     STG_CUDA_TRY(cudaMemcpyAsync(h_scal, P.scal.data(), sizeof(double) * S_COUNT, cudaMemcpyDeviceToHost, s));
     STG_CUDA_TRY(cudaMemcpyAsync(h_flags, P.flags.data(), sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
     STG_CUDA_TRY(cudaStreamSynchronize(s));
+    const long max_iter = c.prm.max_iter;
     int status = h_flags[F_DONE] ? h_flags[F_STATUS] : STG_MAX_ITER;
-    long iters = max_iter <= 1 ? 1 : (long)h_scal[S_ITER];
+    if(status == STG_ERR_TIMEOUT) set_error("persistent PCG: a grid barrier wait gave up");
+    const long iters = max_iter <= 1 ? 1 : (long)h_scal[S_ITER];
     if(st)
     {
         st->iterations = (int)iters;

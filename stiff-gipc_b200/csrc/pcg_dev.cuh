@@ -1,0 +1,63 @@
+// pcg_dev.cuh -- the by-value parameter block of the PCG phases (pcg.cu).
+#pragma once
+#include "reduce.cuh"
+
+namespace stg
+{
+constexpr int kMaxLevelsDev = 6;
+
+// Everything a phase needs, passed by value.
+struct PcgDev
+{
+    // SpMV structure (padded blocks: FP32 48 B = 3 x float4, FP64 80 B = 5 x double2)
+    const int* row_ptr;
+    const int* cols;
+    const int* t_ptr;
+    const int2* t_ent;
+    const int* fcol;          // full symmetric row-sliced SoA copy (phase A)
+    const void* fval;         // 9 planes of `fstride` values in the iteration precision
+    size_t fstride;
+    const double2* blk64;     // FP64 padded upper blocks (residual replacement)
+    int nrows, n;
+    // vectors in the iteration precision T, one 4-wide (16 B FP32 / 32 B FP64) slot per block
+    // row so that a neighbour gather is one (FP32) or two (FP64) 16-byte loads:
+    //   zp[2]: per block row {z0 z1 z2 -, p0 p1 p2 -} (8 T); double-buffered across iterations
+    //   q    : per block row {q0 q1 q2 -} (4 T)
+    // x, r, b stay FP64 in the caller's [3n] layout
+    void* zp0;
+    void* zp1;
+    void* q;
+    double* x;
+    double* r;
+    const double* b;
+    // MAS
+    const int* part_map;
+    const unsigned* fine_mask;
+    const int* going_next;
+    const unsigned* closed;
+    float* R;
+    float* Z;
+    const float* inv;
+    const int* real_map;
+    const int* coarse_table;
+    int M, V, L, nbanks, fem_dof;
+    int identity;                     // part_map[s] == s for s < V, -1 after
+    int ls[2 * (kMaxLevelsDev + 1)];  // level (count, begin) pairs; constant indices only
+    const int* ls_dev;                // the same pairs in device memory (runtime indices)
+    // non-MAS preconditioners
+    const double* diag_inv;   // null: identity
+    int abd_bodies;
+    const double* abd_inv;
+    // reductions / control
+    double* partials;         // [6][slots]
+    unsigned* counters;       // [8]
+    double* scal;
+    int* flags;
+    int slots;
+    PcgParams prm;
+    cudaGraphConditionalHandle h_while, h_if;
+    int use_cond;
+    unsigned* bar;            // persistent barrier: [0] count, [1] generation
+};
+
+}  // namespace stg

@@ -5,6 +5,7 @@
 // (MASPreconditioner.cuh) and the converted BCOO, all on one CUDA stream.
 #pragma once
 #include "common.cuh"
+#include "pcg_dev.cuh"
 #include "../../include/stgipc.h"
 
 #include <algorithm>
@@ -33,7 +34,12 @@ struct Bcoo
     DBuf<int> t_ptr;             // [nrows+1]
     DBuf<int> t_cnt;             // [nrows+1]
     DBuf<int2> t_ent;            // [offdiag]
-    DBuf<float> blocks32;        // FP32 copy (FP32 mode)
+    DBuf<double> blk64p;         // FP64 blocks padded to 80 B (5 x double2), residual replacement
+    // full symmetric row-sliced SoA copy for the PCG SpMV (see k_build_full in pcg.cu)
+    DBuf<int> fcol;
+    DBuf<float> fval32;
+    DBuf<double> fval64;
+    size_t fstride = 0;
     DBuf<double> diag_inv;       // 3x3 block-Jacobi inverses [nrows*9]
     int offdiag = 0;
 
@@ -50,6 +56,7 @@ struct ConvertScratch
 struct MasState
 {
     bool inited = false, built = false, assembled = false;
+    bool identity = false;        // part_map[s] == s for s < V (Morton order): no slot indirection
     int bank = 16, V = 0, M = 0, L = 0, node_offset = 0, nlist_size = 0;
     int total_clusters = 0, nbanks = 0, nb0 = 0;
     int level_size[2 * (kMaxLevels + 1)] = {};
@@ -67,7 +74,7 @@ struct MasState
     DBuf<int> scratch;
     DBuf<double> mat;             // [nbanks * NS * 9]
     DBuf<float> inv;              // [nbanks * NS * 9]
-    DBuf<float> R, Z;             // [total_clusters * 3]
+    DBuf<float> R, Z;             // [total_clusters * 4], float4 per node
     // Galerkin assembly: coarse triplets and the current / next level operator (upper BCOO)
     ConvertScratch gcv;
     DBuf<int> tr_rows, tr_cols, ga_rows, ga_cols, gb_rows, gb_cols, g_rowptr;
@@ -76,15 +83,15 @@ struct MasState
 
 struct PcgState
 {
-    DBuf<double> r, z, p, q, x64;  // FP64 vectors
-    DBuf<float> p32, q32, z32;     // FP32 vectors (FP32 mode)
-    DBuf<double> partials;         // per-block partial sums
+    DBuf<double> r;                // FP64 residual
+    DBuf<double> vbuf;             // zp0, zp1, q slots in the iteration precision
+    DBuf<double> q;                // scratch for the true residual
+    DBuf<double> partials;         // per-block partial sums, 6 sites
     DBuf<double> scal;             // device scalars, see enum below
     DBuf<unsigned> counters;       // last-block counters
-    DBuf<int> flags;               // [0] done, [1] status
-    int partial_slots = 0;
+    DBuf<int> flags;               // [0] done, [1] status, [2] replacements
+    DBuf<unsigned> bar;            // persistent grid barrier
     cudaGraphExec_t graph = nullptr;
-    long long graph_key[8] = {};
 };
 
 // device scalar slots
@@ -116,9 +123,12 @@ struct Solver
     cudaEvent_t ev[6] = {};
     bool events = false;
     int mas_fem_offset = 0;       // FEM block offset of the last MAS assembly
-    long long generation = 0;     // bumped by every (re)assembly; keys the captured graph
+    long long generation = 0;     // bumped by every (re)assembly
     bool graph_dirty = true;
-    int launches_per_batch = 0;
+    int launches_per_batch = 0;   // kernels in one captured iteration
+    cudaGraph_t pending_if_body = nullptr;
+    PcgDev pcg_dev{};             // parameters of the last solve (measurement hook)
+    bool pcg_ready = false;
 
     ~Solver();
 

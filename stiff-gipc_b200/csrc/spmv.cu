@@ -184,14 +184,6 @@ int Solver::prepare_spmv()
     k_t_sort<<<std::max(1, std::min(div_up(nrows, 256), kSMs * 16)), 256, 0, s>>>(bcoo.t_ptr.data(), bcoo.t_ent.data(), nrows);
     STG_LAUNCH_CHECK();
     launches += 4;
-    if(cfg.precision == STG_PREC_FP32)
-    {
-        STG_TRY(bcoo.blocks32.resize((size_t)nnzb * 9));
-        k_to_f32<<<std::max(1, std::min(div_up((long)nnzb * 9, 256), kSMs * 16)), 256, 0, s>>>(bcoo.B(), bcoo.blocks32.data(),
-                                                                                           (size_t)nnzb * 9);
-        STG_LAUNCH_CHECK();
-        launches++;
-    }
     if(cfg.preconditioner == STG_PRECOND_DIAG)
     {
         STG_TRY(bcoo.diag_inv.resize((size_t)nrows * 9));
