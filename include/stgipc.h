@@ -198,6 +198,27 @@ int stg_mas_export_matrices(stg_handle h, double* mat, float* inv, int* nbanks);
  * vec = 8 or 4 (each array counted once). */
 int stg_profile_spmv(stg_handle h, int reps, float* avg_ms, double* bytes);
 
+/* ---- allocation-free SpMV ---------------------------------------------------------- */
+/* No counterpart in the reference.  The same y = a * A * x + b * y as stg_spmv (same
+ * kernel, same result bit for bit), for callers that cannot allocate device memory: a host
+ * simulator that has reserved the GPU's memory for its own pool and forbids allocations
+ * outside it, or a step loop that cannot take cudaMalloc's implicit device synchronisation.
+ * It takes no handle and allocates nothing: its row pointers and transpose lists live in
+ * one fixed device array of STG_NOALLOC_SCRATCH_BYTES (about 9.5 MiB) inside the library,
+ * held by every GPU that loads the library until the process exits.  Systems larger than
+ * STG_NOALLOC_MAX_ROWS block rows (n / 3) or STG_NOALLOC_MAX_BLOCKS upper blocks are
+ * rejected with STG_ERR_INVALID.  All calls share that array: calls that overlap on the
+ * GPU (two host threads, or two streams) race and give wrong results.  The first call on
+ * each device resolves the array's address on that device; make it before any stream
+ * capture.  `stream` is a cudaStream_t (NULL: the legacy default stream); the call returns
+ * after the stream has finished the product. */
+#define STG_NOALLOC_MAX_ROWS 131072
+#define STG_NOALLOC_MAX_BLOCKS 1048576
+#define STG_NOALLOC_SCRATCH_BYTES (256 + 3 * 4 * 131136 + 8 * 1048576)
+int stg_spmv_noalloc(double a, const double* blocks, const int32_t* rows,
+                     const int32_t* cols, int nnzb, const double* x, double b, double* y,
+                     int n, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

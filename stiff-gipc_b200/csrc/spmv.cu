@@ -16,6 +16,8 @@
 #include "solver.hpp"
 #include "spmv_core.cuh"
 
+#include <mutex>
+
 namespace stg
 {
 
@@ -238,3 +240,139 @@ int Solver::spmv(double a, const double* x, double b, double* y)
 }
 
 }  // namespace stg
+
+// ---------------------------------------------------------------------------------------
+// stg_spmv_noalloc: the same SpMV without a handle and without any device allocation.
+//
+// For callers that cannot allocate device memory: a host simulator that has reserved the
+// GPU's memory for its own pool and forbids allocations outside it, or a step loop that
+// cannot take cudaMalloc's implicit device-wide synchronisation.  The row pointers and
+// transpose lists that stg_spmv keeps in a handle's buffers live here in one file-scope
+// device array of fixed size instead (STG_NOALLOC_SCRATCH_BYTES, about 9.5 MiB), which
+// every GPU that loads this library holds until the process exits.
+//
+// The array is shared by every call: each call rewrites all of it that it reads and clears
+// what must start at zero (the counters and the per-row transpose counts), so nothing
+// carries over from the previous call's contents.  Two calls that overlap on the GPU (two
+// host threads, or two streams) race on the array and give wrong results.
+//
+// Set-up: the first call on each device resolves the array's device address with
+// cudaGetSymbolAddress (with that device current) and caches it; make that first call
+// before any stream capture.
+// ---------------------------------------------------------------------------------------
+namespace
+{
+constexpr size_t kNaCounters = 0;                                                 // 64 ints: [0] bad, [1] scan total
+constexpr size_t kNaRowInts = ((size_t)STG_NOALLOC_MAX_ROWS + 1 + 63) / 64 * 64;  // per-row array, 256 B multiple
+constexpr size_t kNaRowPtr = 64 * sizeof(int);
+constexpr size_t kNaTPtr = kNaRowPtr + kNaRowInts * sizeof(int);
+constexpr size_t kNaTCnt = kNaTPtr + kNaRowInts * sizeof(int);
+constexpr size_t kNaTEnt = kNaTCnt + kNaRowInts * sizeof(int);
+constexpr size_t kNaBytes = kNaTEnt + (size_t)STG_NOALLOC_MAX_BLOCKS * sizeof(int2);
+static_assert(kNaBytes == STG_NOALLOC_SCRATCH_BYTES, "header and library disagree on the scratch size");
+static_assert(kNaTEnt % 256 == 0, "transpose list must stay 256-byte aligned");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+constexpr int kNaMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_addr[kNaMaxDevices] = {};
+
+// device address of g_noalloc_scratch on the current device (resolved once per device)
+int noalloc_scratch(unsigned char** out)
+{
+    int dev = -1;
+    STG_CUDA_TRY(cudaGetDevice(&dev));
+    if(dev < 0 || dev >= kNaMaxDevices)
+    {
+        stg::set_error("stg_spmv_noalloc: device ordinal " + std::to_string(dev) + " beyond the supported " +
+                       std::to_string(kNaMaxDevices));
+        return STG_ERR_INVALID;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if(!g_noalloc_addr[dev])
+    {
+        void* p = nullptr;
+        STG_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return 0;
+}
+
+int spmv_noalloc(double a, const double* blocks, const int* rows, const int* cols, int nnzb, const double* x, double b,
+                 double* y, int n, cudaStream_t s)
+{
+    using namespace stg;
+    if(nnzb < 0 || n < 0 || n % 3 != 0 || (nnzb > 0 && (!blocks || !rows || !cols)) || (n > 0 && (!x || !y)))
+    {
+        set_error("stg_spmv_noalloc: invalid arguments");
+        return STG_ERR_INVALID;
+    }
+    const int nrows = n / 3;
+    if(nrows > STG_NOALLOC_MAX_ROWS || nnzb > STG_NOALLOC_MAX_BLOCKS)
+    {
+        set_error("stg_spmv_noalloc: " + std::to_string(nrows) + " block rows / " + std::to_string(nnzb) +
+                  " blocks exceed the fixed scratch maximum of " + std::to_string(STG_NOALLOC_MAX_ROWS) + " / " +
+                  std::to_string(STG_NOALLOC_MAX_BLOCKS) + "; use stg_spmv");
+        return STG_ERR_INVALID;
+    }
+    if(nrows == 0) return STG_OK;
+    unsigned char* base = nullptr;
+    STG_TRY(noalloc_scratch(&base));
+    int* counters = reinterpret_cast<int*>(base + kNaCounters);
+    int* row_ptr = reinterpret_cast<int*>(base + kNaRowPtr);
+    int* t_ptr = reinterpret_cast<int*>(base + kNaTPtr);
+    int* t_cnt = reinterpret_cast<int*>(base + kNaTCnt);
+    int2* t_ent = reinterpret_cast<int2*>(base + kNaTEnt);
+
+    STG_CUDA_TRY(cudaMemsetAsync(counters, 0, 64 * sizeof(int), s));
+    if(nnzb > 0)
+    {
+        k_bcoo_validate<<<std::max(1, std::min(div_up(nnzb, 256), kSMs * 8)), 256, 0, s>>>(rows, cols, nnzb, nrows,
+                                                                                          counters);
+        STG_LAUNCH_CHECK();
+        int bad = 0;
+        STG_CUDA_TRY(cudaMemcpyAsync(&bad, counters, sizeof(int), cudaMemcpyDeviceToHost, s));
+        STG_CUDA_TRY(cudaStreamSynchronize(s));
+        if(bad)
+        {
+            set_error("stg_spmv_noalloc: BCOO input: " + std::to_string(bad) +
+                      " entries are out of range, lower-triangular, unsorted or duplicated (run stg_convert first)");
+            return STG_ERR_INVALID;
+        }
+    }
+    const int g = std::max(1, std::min(div_up(nnzb + 1, 256), kSMs * 16));
+    k_row_ptr<<<g, 256, 0, s>>>(rows, nnzb, nrows, row_ptr);
+    STG_LAUNCH_CHECK();
+    STG_CUDA_TRY(cudaMemsetAsync(t_cnt, 0, sizeof(int) * (nrows + 1), s));
+    k_t_count<<<g, 256, 0, s>>>(rows, cols, nnzb, t_cnt);
+    STG_LAUNCH_CHECK();
+    k_scan_exclusive<<<1, 1024, 0, s>>>(t_cnt, t_ptr, nullptr, nrows + 1, counters + 1);
+    STG_LAUNCH_CHECK();
+    STG_CUDA_TRY(cudaMemsetAsync(t_cnt, 0, sizeof(int) * (nrows + 1), s));
+    k_t_fill<<<g, 256, 0, s>>>(rows, cols, nnzb, t_ptr, t_cnt, t_ent);
+    STG_LAUNCH_CHECK();
+    k_t_sort<<<std::max(1, std::min(div_up(nrows, 256), kSMs * 16)), 256, 0, s>>>(t_ptr, t_ent, nrows);
+    STG_LAUNCH_CHECK();
+    const int grid = std::max(1, std::min(div_up(nrows, 256 / 16), kSMs * 8));
+    k_spmv_sym<double, 16><<<grid, 256, 0, s>>>(row_ptr, cols, blocks, t_ptr, t_ent, x, y, a, b, nrows);
+    STG_LAUNCH_CHECK();
+    STG_CUDA_TRY(cudaStreamSynchronize(s));
+    return STG_OK;
+}
+}  // namespace
+
+extern "C" int stg_spmv_noalloc(double a, const double* blocks, const int32_t* rows, const int32_t* cols, int nnzb,
+                                const double* x, double b, double* y, int n, void* stream)
+{
+    try
+    {
+        return spmv_noalloc(a, blocks, rows, cols, nnzb, x, b, y, n, static_cast<cudaStream_t>(stream));
+    }
+    catch(const std::exception& e)
+    {
+        stg::set_error(std::string("stg_spmv_noalloc: ") + e.what());
+        return STG_ERR_INVALID;
+    }
+}

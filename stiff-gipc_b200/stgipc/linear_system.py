@@ -70,6 +70,19 @@ def _require_cuda(*ts):
             raise ValueError("device arrays must be CUDA tensors")
 
 
+def spmv_noalloc(a, blocks, rows, cols, nnzb, x, b, y, stream=None):
+    """y = a A x + b y without a handle and without device allocation (stg_spmv_noalloc).
+
+    For callers that cannot allocate device memory; sizes up to STG_NOALLOC_MAX_ROWS block
+    rows and STG_NOALLOC_MAX_BLOCKS blocks.  Calls share one fixed device scratch array, so
+    calls that overlap on the GPU race.  `stream` is a torch.cuda.Stream or None (legacy
+    default stream)."""
+    _require_cuda(blocks, rows, cols, x, y)
+    s = None if stream is None else stream.cuda_stream
+    check(_L.lib().stg_spmv_noalloc(float(a), _ptr(blocks), _ptr(rows), _ptr(cols), int(nnzb), _ptr(x), float(b),
+                                    _ptr(y), int(y.numel()), s), "stg_spmv_noalloc")
+
+
 class Solver:
     """One handle: GlobalLinearSystem + PCGSolver + MAS preconditioner on one stream."""
 
