@@ -33,6 +33,7 @@
 //               bounded grid barrier that also finishes the reductions.
 #include "solver.hpp"
 #include "reduce.cuh"
+#include "spmv_core.cuh"
 
 namespace stg
 {
@@ -65,13 +66,14 @@ __device__ __forceinline__ void set_conditionals(const PcgDev& c, int op)
     }
 }
 
+template <int BLOCK = PB>
 __device__ __forceinline__ void finish_reduction(const PcgDev& c, double v, int site, int op, int slot = 0)
 {
-    __shared__ double red[PB / 32];
+    __shared__ double red[BLOCK / 32];
     __shared__ bool last;
     double* partials = c.partials + (size_t)site * c.slots;
     unsigned* counter = c.counters + site;
-    const double bs = block_sum<PB>(v, red);
+    const double bs = block_sum<BLOCK>(v, red);
     if(threadIdx.x == 0)
     {
         partials[blockIdx.x] = bs;
@@ -82,8 +84,8 @@ __device__ __forceinline__ void finish_reduction(const PcgDev& c, double v, int 
     if(!last) return;
     __threadfence();
     double acc = 0;
-    for(int i = threadIdx.x; i < (int)gridDim.x; i += PB) acc += __ldcg(partials + i);
-    const double tot = block_sum<PB>(acc, red);
+    for(int i = threadIdx.x; i < (int)gridDim.x; i += BLOCK) acc += __ldcg(partials + i);
+    const double tot = block_sum<BLOCK>(acc, red);
     if(threadIdx.x == 0)
     {
         post_op(op, slot, tot, c.scal, c.flags, c.prm);
@@ -185,30 +187,24 @@ __device__ __forceinline__ void row_spmv_zp(const PcgDev& c, const T* blk, int i
     }
 }
 
-// Row i of A * (z + beta p) on the full symmetric SoA copy (phase A).  LPR lanes per row,
-// warp-wide shuffles: every lane of the warp must call it.
+// Row i of A * (z + beta p) on the full symmetric plane copy (untiled phase A).  LPR lanes
+// per row, warp-wide shuffles: every lane of the warp must call it.
 template <typename T, int LPR>
 __device__ __forceinline__ void row_spmv_full(const PcgDev& c, int i, bool valid, int sub, const T* zp, T beta, T& a0,
                                               T& a1, T& a2)
 {
     a0 = a1 = a2 = T(0);
-    size_t f0 = 0;
-    int deg = 0;
+    int f0 = 0, deg = 0;
     if(valid)
     {
-        const int r0 = __ldg(c.row_ptr + i), r1 = __ldg(c.row_ptr + i + 1);
-        const int t0 = __ldg(c.t_ptr + i), t1 = __ldg(c.t_ptr + i + 1);
-        f0 = (size_t)r0 + t0;
-        deg = (r1 - r0) + (t1 - t0);
+        f0 = __ldg(c.frow + i);
+        deg = __ldg(c.frow + i + 1) - f0;
     }
-    const T* v = reinterpret_cast<const T*>(c.fval);
     for(int e = sub; e < deg; e += LPR)
     {
-        const size_t f = f0 + e;
-        const int j = __ldg(c.fcol + f);
+        int j;
         T h[9];
-#pragma unroll
-        for(int t = 0; t < 9; t++) h[t] = __ldg(v + t * c.fstride + f);
+        ldg_entry(c.fent, c.fstride, f0 + e, h, j);
         T x0, x1, x2, p0, p1, p2;
         ld4(zp + 8 * (size_t)j, x0, x1, x2);
         ld4(zp + 8 * (size_t)j + 4, p0, p1, p2);
@@ -693,6 +689,334 @@ __global__ void __launch_bounds__(D_WARPS * 32) k_phase_d16(PcgDev c)
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// A, tiled: the SpMV phase with its matrix stream staged in shared memory by the Tensor
+// Memory Accelerator.  Each CTA owns a contiguous, balanced range of rows, cut into tiles of
+// RT rows (64 FP32, 32 FP64).  A tile's entries are one contiguous range [frow[r0], frow[r1])
+// of every plane of the full copy (FullPlanes), so one producer lane moves a whole tile with
+// one bulk copy per plane, plus one for the tile's row bounds, into a ring of stages that
+// complete on per-stage mbarriers.  Eight consumer warps compute the tile from shared memory
+// (16-byte loads, no bank conflicts) with LPR lanes per row (4 FP32, 8 FP64): lane `sub`
+// sums the entries sub, sub + LPR, ... of its row in order, four at a time with their
+// neighbour gathers of z / p issued before the block values are read, and an xor tree over
+// the LPR lanes finishes the row.  A tile with more entries than a stage holds is computed
+// from global memory (only its row bounds are copied).  Every wait is bounded; a wait that
+// gives up sets STG_ERR_TIMEOUT and the kernel drains its copies in flight before returning.
+// ---------------------------------------------------------------------------------------
+constexpr int A_CW = 8;            // consumer warps
+constexpr int A_THREADS = (A_CW + 1) * 32;
+
+template <typename T>
+struct ATile
+{
+    using FP = FullPlanes<T>;
+    static constexpr int RT = sizeof(T) == 4 ? 64 : 32;         // rows per tile
+    static constexpr int LPR = 32 * A_CW / RT;                   // consumer lanes per row
+    static constexpr int CAP = 20 * RT;                          // entries per stage (even)
+    static constexpr int STAGES = 2;
+    static constexpr int FROW = 4 * (RT + 4);                    // frow[r0 .. r0 + RT + 4)
+    static constexpr int STAGE = CAP * FP::ES + FROW;            // planes + row bounds
+    static constexpr int META = 16 * STAGES;                     // per stage: {F0a, overflow}
+    static constexpr int BARS = 16 * STAGES;                     // full[s], empty[s]
+    static constexpr int SMEM = STAGES * STAGE + META + BARS;
+    static constexpr int MIN_CTAS = 2;                           // resident CTAs per SM
+};
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// shared-memory loads by 32-bit shared address
+__device__ __forceinline__ int lds_s32(unsigned a)
+{
+    int v;
+    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(a));
+    return v;
+}
+
+// entry f of a stage's planes (CAP entries per plane) at shared address sb: the tail
+// {h8, col} and the eight other values, loaded separately so that the neighbour gather can
+// be issued before the bulk of the block is read
+template <int CAP>
+__device__ __forceinline__ void lds_tail(unsigned sb, int f, float& h8, int& col)
+{
+    unsigned tc;
+    asm volatile("ld.shared.v2.b32 {%0, %1}, [%2];" : "=f"(h8), "=r"(tc) : "r"(sb + 32u * CAP + 8u * f));
+    col = (int)tc;
+}
+template <int CAP>
+__device__ __forceinline__ void lds_tail(unsigned sb, int f, double& h8, int& col)
+{
+    unsigned long long tc;
+    asm volatile("ld.shared.v2.b64 {%0, %1}, [%2];" : "=d"(h8), "=l"(tc) : "r"(sb + 64u * CAP + 16u * f));
+    col = (int)tc;
+}
+template <int CAP>
+__device__ __forceinline__ void lds_main(unsigned sb, int f, float h[9])
+{
+    const unsigned a0 = sb + 16u * f, a1 = sb + 16u * CAP + 16u * f;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(h[0]), "=f"(h[1]), "=f"(h[2]), "=f"(h[3]) : "r"(a0));
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(h[4]), "=f"(h[5]), "=f"(h[6]), "=f"(h[7]) : "r"(a1));
+}
+template <int CAP>
+__device__ __forceinline__ void lds_main(unsigned sb, int f, double h[9])
+{
+#pragma unroll
+    for(int p = 0; p < 4; p++)
+        asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];"
+                     : "=d"(h[2 * p]), "=d"(h[2 * p + 1])
+                     : "r"(sb + 16u * p * CAP + 16u * f));
+}
+
+// v_j = z_j + beta p_j gathered from the zp slots
+template <typename T>
+__device__ __forceinline__ void a_gather(int j, const T* zp, T beta, T& x0, T& x1, T& x2)
+{
+    T p0, p1, p2;
+    ld4(zp + 8 * (size_t)j, x0, x1, x2);
+    ld4(zp + 8 * (size_t)j + 4, p0, p1, p2);
+    x0 += beta * p0;
+    x1 += beta * p1;
+    x2 += beta * p2;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(A_THREADS, ATile<T>::MIN_CTAS) k_phase_a_tiled(PcgDev c)
+{
+    using G = ATile<T>;
+    using FP = FullPlanes<T>;
+    constexpr int RT = G::RT, LPR = G::LPR, CAP = G::CAP;
+    extern __shared__ __align__(128) unsigned char asm_[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // this CTA's rows: a contiguous range [rb, re) of about nrows / gridDim.x rows (starts
+    // are multiples of 4, so that every tile's row-bound copy is 16-byte aligned), cut into
+    // tiles of RT rows: tile k is [rb + k RT, min(rb + (k + 1) RT, re))
+    auto range_start = [&](long long b) -> int {
+        return b == 0 ? 0 : (b >= gridDim.x ? c.nrows : (int)((b * c.nrows / gridDim.x) & ~3LL));
+    };
+    const int rb = range_start(blockIdx.x), re = range_start(blockIdx.x + 1LL);
+    const int mine = re > rb ? (re - rb + RT - 1) / RT : 0;
+    // the loads the start depends on are independent: issue them together
+    const int done = __ldcg(c.flags + F_DONE);
+    const double s_iter = __ldcg(c.scal + SS_ITER), s_beta = __ldcg(c.scal + SS_BETA);
+    int lo = 0, hi = 0;  // producer: entry bounds of the next 32 tiles, one per lane
+    if(warp == A_CW && lane < mine)
+    {
+        const int r0 = rb + lane * RT;
+        lo = __ldg(c.frow + r0);
+        hi = __ldg(c.frow + min(r0 + RT, re));
+    }
+    if(done) return;
+    int* meta = reinterpret_cast<int*>(asm_ + G::STAGES * G::STAGE);
+    const unsigned sbase = smem_u32(asm_);
+    const unsigned bar_full = smem_u32(asm_ + G::STAGES * G::STAGE + G::META);
+    const unsigned bar_empty = bar_full + 8 * G::STAGES;
+    if(threadIdx.x == 0)
+    {
+        for(int s = 0; s < G::STAGES; s++)
+        {
+            mbar_init(bar_full + 8 * s, 1);
+            mbar_init(bar_empty + 8 * s, A_CW);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    const int par = ((long)s_iter) & 1;
+    const T* zp = zpbuf<T>(c, par);
+    T* zpn = zpbuf<T>(c, par ^ 1);
+    T* q = reinterpret_cast<T*>(c.q);
+    const T beta = (T)s_beta;
+    double acc = 0;
+    bool failed = false;
+
+    if(warp == A_CW)
+    {
+        // ---- producer warp: lane 0 issues, all lanes fetch the tile bounds ----
+        int issued = 0;
+        for(int k0 = 0; k0 < mine && !failed; k0 += 32)
+        {
+            if(k0 > 0)
+            {
+                lo = hi = 0;
+                if(k0 + lane < mine)
+                {
+                    const int r0 = rb + (k0 + lane) * RT;
+                    lo = __ldg(c.frow + r0);
+                    hi = __ldg(c.frow + min(r0 + RT, re));
+                }
+            }
+            const int cnt = min(32, mine - k0);
+            for(int u = 0; u < cnt; u++)
+            {
+                const int F0 = __shfl_sync(0xffffffffu, lo, u), F1 = __shfl_sync(0xffffffffu, hi, u);
+                const int k = k0 + u, s = k % G::STAGES;
+                if(lane == 0)
+                {
+                    if(k >= G::STAGES && !mbar_wait(bar_empty + 8 * s, ((k / G::STAGES) - 1) & 1)) failed = true;
+                    if(!failed)
+                    {
+                        const int F0a = F0 & ~1, n2 = ((F1 + 1) & ~1) - F0a;
+                        const bool ovf = n2 > CAP;
+                        const int nc = ovf ? 0 : n2;
+                        meta[4 * s] = F0a;
+                        meta[4 * s + 1] = ovf ? 1 : 0;
+                        unsigned char* st = asm_ + (size_t)s * G::STAGE;
+                        const unsigned bf = bar_full + 8 * s;
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        mbar_expect_tx(bf, (unsigned)(G::FROW + nc * FP::ES));
+                        tma_load_1d(st + CAP * FP::ES, c.frow + rb + (size_t)k * RT, G::FROW, bf);
+                        if(nc)
+                        {
+#pragma unroll 1
+                            for(int pl = 0; pl < FP::NP; pl++)
+                                tma_load_1d(st + (size_t)16 * pl * CAP, c.fent + 16 * (pl * c.fstride + F0a),
+                                            (unsigned)(16 * nc), bf);
+                            tma_load_1d(st + (size_t)16 * FP::NP * CAP,
+                                        c.fent + 16 * FP::NP * c.fstride + (size_t)FP::TAIL * F0a,
+                                        (unsigned)(FP::TAIL * nc), bf);
+                        }
+                        issued = k + 1;
+                    }
+                }
+                failed = __shfl_sync(0xffffffffu, failed ? 1 : 0, 0) != 0;
+                if(failed) break;
+            }
+        }
+        if(lane == 0)
+        {
+            if(failed)
+            {
+                atomicExch(c.flags + F_STATUS, 6);  // STG_ERR_TIMEOUT
+                atomicExch(c.flags + F_DONE, 1);
+            }
+            // drain: every issued stage's copies must have landed before the CTA exits
+            for(int k = max(0, issued - G::STAGES); k < issued; k++)
+                mbar_wait(bar_full + 8 * (k % G::STAGES), (k / G::STAGES) & 1);
+        }
+    }
+    else
+    {
+        // ---- consumer warps: LPR lanes per row; lane `sub` of row r (tile-local) sums the
+        //      entries e = sub, sub + LPR, ... of that row in order, up to four at a time ----
+        // The lane whose entry is the row's diagonal block gathers v_i = z_i + beta p_i, which
+        // is p_new of the row; it is shuffled to the row's first lane (a row without a
+        // diagonal block gathers it there).
+        const int sub = lane & (LPR - 1);
+        const int rloc = warp * (32 / LPR) + lane / LPR;
+        const unsigned grp = (LPR == 32 ? 0xffffffffu : ((1u << LPR) - 1u)) << (lane & ~(LPR - 1));
+        for(int k = 0; k < mine; k++)
+        {
+            const int s = k % G::STAGES;
+            const int r0 = rb + k * RT, r1 = min(r0 + RT, re);
+            const int i = r0 + rloc;
+            if(!mbar_wait(bar_full + 8 * s, (k / G::STAGES) & 1))
+            {
+                failed = true;
+                break;
+            }
+            const unsigned sb = sbase + (unsigned)(s * G::STAGE);
+            const unsigned sfrow = sb + CAP * FP::ES;
+            const int F0a = meta[4 * s];
+            const bool ovf = meta[4 * s + 1] != 0;
+            int f = 0, d = 0;
+            if(i < r1)
+            {
+                const int x0 = lds_s32(sfrow + 4 * rloc), x1 = lds_s32(sfrow + 4 * rloc + 4);
+                f = x0 - F0a;
+                d = x1 - x0;
+            }
+            T y0 = T(0), y1 = T(0), y2 = T(0), pn0 = T(0), pn1 = T(0), pn2 = T(0);
+            bool hit = false;
+            for(int e0 = sub; e0 < d; e0 += 4 * LPR)
+            {
+                T h8[4], x[4][3];
+                int j[4];
+#pragma unroll
+                for(int u = 0; u < 4; u++)
+                {
+                    const int e = e0 + u * LPR;
+                    h8[u] = T(0);
+                    j[u] = 0;
+                    if(e < d)
+                    {
+                        if(!ovf)
+                            lds_tail<CAP>(sb, f + e, h8[u], j[u]);
+                        else
+                        {
+                            T hh[9];
+                            ldg_entry(c.fent, c.fstride, F0a + f + e, hh, j[u]);
+                            h8[u] = hh[8];
+                        }
+                    }
+                }
+#pragma unroll
+                for(int u = 0; u < 4; u++)
+                    if(e0 + u * LPR < d) a_gather<T>(j[u], zp, beta, x[u][0], x[u][1], x[u][2]);
+#pragma unroll
+                for(int u = 0; u < 4; u++)
+                {
+                    const int e = e0 + u * LPR;
+                    if(e < d)
+                    {
+                        T h[9];
+                        int jj;
+                        if(!ovf)
+                            lds_main<CAP>(sb, f + e, h);
+                        else
+                            ldg_entry(c.fent, c.fstride, F0a + f + e, h, jj);
+                        h[8] = h8[u];
+                        mv3<T>(h, false, x[u][0], x[u][1], x[u][2], y0, y1, y2);
+                        if(j[u] == i)
+                        {
+                            pn0 = x[u][0];
+                            pn1 = x[u][1];
+                            pn2 = x[u][2];
+                            hit = true;
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+            if(lane == 0) mbar_arrive(bar_empty + 8 * s);
+#pragma unroll
+            for(int o = LPR / 2; o > 0; o >>= 1)
+            {
+                y0 += __shfl_xor_sync(0xffffffffu, y0, o);
+                y1 += __shfl_xor_sync(0xffffffffu, y1, o);
+                y2 += __shfl_xor_sync(0xffffffffu, y2, o);
+            }
+            const unsigned hm = __ballot_sync(0xffffffffu, hit) & grp;
+            const int src = hm ? __ffs(hm) - 1 : lane;
+            T p0 = __shfl_sync(0xffffffffu, pn0, src);
+            T p1 = __shfl_sync(0xffffffffu, pn1, src);
+            T p2 = __shfl_sync(0xffffffffu, pn2, src);
+            if(sub == 0 && i < r1)
+            {
+                if(!hm) a_gather<T>(i, zp, beta, p0, p1, p2);
+                st4(zpn + 8 * (size_t)i + 4, p0, p1, p2);
+                st4(q + 4 * (size_t)i, y0, y1, y2);
+                acc += (double)p0 * (double)y0 + (double)p1 * (double)y1 + (double)p2 * (double)y2;
+            }
+        }
+        if(failed && lane == 0)
+        {
+            atomicExch(c.flags + F_STATUS, 6);  // STG_ERR_TIMEOUT
+            atomicExch(c.flags + F_DONE, 1);
+        }
+    }
+    finish_reduction<A_THREADS>(c, acc, SITE_A, POST_ALPHA);
+}
+
 // E (MAS): z = sum over levels (FP32) on the FEM range + ABD block-Jacobi; share of r.z
 // ABD 12x12 block-Jacobi (abd_preconditioner.cu:20-38): one thread per dof of the first
 // 12 * bodies dofs, z written into the zp slots; returns the share of r.z
@@ -1008,39 +1332,52 @@ __global__ void k_pack_blocks(const double* __restrict__ src, int nnzb, float* d
     }
 }
 
-// Full symmetric row-sliced SoA copy used by the PCG SpMV (phase A): row i holds, sorted by
-// column, its lower blocks (transposes of the upper blocks k with col(k) == i, from the
-// transpose list) followed by its upper blocks; entry e of row i sits at
-// f = row_ptr[i] + t_ptr[i] + e, its column in fcol[f] and component t (column-major) in
-// plane t: fval[t * stride + f].  The 16 lanes of a row read consecutive entries of every
-// plane, so each block component is one coalesced 64-byte access and no block is fetched
-// from a random address.
+// Builds the full symmetric plane copy (FullPlanes) used by the PCG SpMV (phase A): row i
+// holds its lower blocks (transposes of the upper blocks k with col(k) == i, in transpose-
+// list order) followed by its upper blocks.  16 lanes per row, one entry per lane.
 template <typename T>
 __global__ void k_build_full(const int* __restrict__ row_ptr, const int* __restrict__ cols,
                              const int* __restrict__ t_ptr, const int2* __restrict__ t_ent,
-                             const double* __restrict__ blocks, int nrows, size_t stride, int* fcol, T* fval)
+                             const double* __restrict__ blocks, int nrows, size_t S, unsigned char* fent)
 {
-    for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrows; i += gridDim.x * blockDim.x)
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, sub = gt & 15;
+    for(int i = gt >> 4; i < nrows; i += (gridDim.x * blockDim.x) >> 4)
     {
-        size_t f = (size_t)row_ptr[i] + t_ptr[i];
-        for(int e = t_ptr[i]; e < t_ptr[i + 1]; e++, f++)
+        const int u0 = row_ptr[i], nu = row_ptr[i + 1] - u0;
+        const int t0 = t_ptr[i], nt = t_ptr[i + 1] - t0;
+        const size_t f0 = (size_t)u0 + t0;
+        for(int e = sub; e < nt + nu; e += 16)
         {
-            const int2 te = t_ent[e];
-            const double* H = blocks + 9 * (size_t)te.x;
-            fcol[f] = te.y;
+            T h[9];
+            int col;
+            if(e < nt)
+            {
+                const int2 te = t_ent[t0 + e];
+                const double* H = blocks + 9 * (size_t)te.x;
 #pragma unroll
-            for(int a = 0; a < 3; a++)
+                for(int a = 0; a < 3; a++)
 #pragma unroll
-                for(int b = 0; b < 3; b++) fval[(size_t)(b * 3 + a) * stride + f] = (T)H[a * 3 + b];  // H^T
-        }
-        for(int k = row_ptr[i]; k < row_ptr[i + 1]; k++, f++)
-        {
-            const double* H = blocks + 9 * (size_t)k;
-            fcol[f] = cols[k];
+                    for(int b = 0; b < 3; b++) h[b * 3 + a] = (T)H[a * 3 + b];  // H^T
+                col = te.y;
+            }
+            else
+            {
+                const int k = u0 + e - nt;
+                const double* H = blocks + 9 * (size_t)k;
 #pragma unroll
-            for(int t = 0; t < 9; t++) fval[(size_t)t * stride + f] = (T)H[t];
+                for(int t = 0; t < 9; t++) h[t] = (T)H[t];
+                col = cols[k];
+            }
+            store_entry(fent, S, f0 + e, h, col);
         }
     }
+}
+
+// first full-copy entry of every row: frow[i] = row_ptr[i] + t_ptr[i], i <= nrows
+__global__ void k_frow(const int* __restrict__ row_ptr, const int* __restrict__ t_ptr, int nrows, int* frow)
+{
+    for(int i = blockIdx.x * blockDim.x + threadIdx.x; i <= nrows; i += gridDim.x * blockDim.x)
+        frow[i] = row_ptr[i] + t_ptr[i];
 }
 
 int pack_blocks(Solver& S)
@@ -1053,21 +1390,26 @@ int pack_blocks(Solver& S)
     k_pack_blocks<<<std::max(1, std::min(div_up(nnzb, 256), kSMs * 16)), 256, 0, S.stream>>>(A.B(), nnzb, nullptr,
                                                                                            A.blk64p.data());
     STG_LAUNCH_CHECK();
-    // full symmetric copy: at most 2 * nnzb entries
-    A.fstride = (size_t)2 * nnzb;
-    STG_TRY(A.fcol.resize(A.fstride));
-    const int g = std::max(1, std::min(div_up(A.nrows, 128), kSMs * 16));
+    // full symmetric copy: at most 2 * nnzb entries per plane, rounded up to an even count
+    // so that every even-aligned entry range of the 8-byte tail plane is a 16-byte multiple
+    A.fstride = ((size_t)2 * nnzb + 2) & ~(size_t)1;
+    STG_TRY(A.frow.resize((size_t)A.nrows + 1 + 72));  // tiles copy frow[r0 .. r0 + RT + 4)
+    k_frow<<<std::max(1, std::min(div_up(A.nrows + 1, 256), kSMs * 8)), 256, 0, S.stream>>>(
+        A.row_ptr.data(), A.t_ptr.data(), A.nrows, A.frow.data());
+    STG_LAUNCH_CHECK();
+    S.launches++;
+    const int g = std::max(1, std::min(div_up(A.nrows, 16), kSMs * 16));
     if(fp32)
     {
-        STG_TRY(A.fval32.resize(9 * A.fstride));
-        k_build_full<float><<<g, 128, 0, S.stream>>>(A.row_ptr.data(), A.C(), A.t_ptr.data(), A.t_ent.data(), A.B(),
-                                                     A.nrows, A.fstride, A.fcol.data(), A.fval32.data());
+        STG_TRY(A.fent.resize(A.fstride * FullPlanes<float>::ES));
+        k_build_full<float><<<g, 256, 0, S.stream>>>(A.row_ptr.data(), A.C(), A.t_ptr.data(), A.t_ent.data(), A.B(),
+                                                     A.nrows, A.fstride, A.fent.data());
     }
     else
     {
-        STG_TRY(A.fval64.resize(9 * A.fstride));
-        k_build_full<double><<<g, 128, 0, S.stream>>>(A.row_ptr.data(), A.C(), A.t_ptr.data(), A.t_ent.data(), A.B(),
-                                                      A.nrows, A.fstride, A.fcol.data(), A.fval64.data());
+        STG_TRY(A.fent.resize(A.fstride * FullPlanes<double>::ES));
+        k_build_full<double><<<g, 256, 0, S.stream>>>(A.row_ptr.data(), A.C(), A.t_ptr.data(), A.t_ent.data(), A.B(),
+                                                      A.nrows, A.fstride, A.fent.data());
     }
     STG_LAUNCH_CHECK();
     S.launches += 2;
@@ -1132,13 +1474,30 @@ static int upload_upper16(cudaStream_t s)
     return 0;
 }
 
+// tiled phase A: the shared-memory opt-in and one resident wave of CTAs
+template <typename T>
+static int launch_phase_a(const PcgDev& c, cudaStream_t s)
+{
+    static thread_local int per_sm = -1;
+    if(per_sm < 0)
+    {
+        STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_a_tiled<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          ATile<T>::SMEM));
+        STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase_a_tiled<T>, A_THREADS,
+                                                                   ATile<T>::SMEM));
+    }
+    const int grid = std::max(1, std::min(div_up(c.nrows, ATile<T>::RT), std::max(per_sm, 1) * kSMs));
+    k_phase_a_tiled<T><<<grid, A_THREADS, ATile<T>::SMEM, s>>>(c);
+    STG_LAUNCH_CHECK();
+    return 0;
+}
+
 template <typename T, int B>
 static int launch_iteration(Solver& S, const PcgDev& c, int grid_vec, int grid_rows, bool in_graph_cond)
 {
     cudaStream_t s = S.stream;
     const bool fp32 = sizeof(T) == 4;
-    k_phase_a<T><<<grid_rows, PB, 0, s>>>(c);
-    STG_LAUNCH_CHECK();
+    STG_TRY(launch_phase_a<T>(c, s));
     k_phase_b<T, B><<<B > 0 ? std::max(1, std::min(div_up(c.M, PB), kSMs * 4)) : grid_vec, PB, 0, s>>>(c);
     STG_LAUNCH_CHECK();
     S.launches += 2;
@@ -1202,9 +1561,34 @@ static int record_if_body(Solver& S, const PcgDev& c, int grid_rows, cudaGraph_t
     return 0;
 }
 
+// Every kernel of the iteration asks for the same shared-memory carveout (the largest), so
+// that consecutive phases do not make the SMs switch their L1 / shared split between
+// launches.
+template <typename T, int B>
+static int set_carveouts()
+{
+    static thread_local bool done = false;
+    if(done) return 0;
+    const int cv = cudaSharedmemCarveoutMaxShared;
+    constexpr int BB = B > 0 ? B : 16;
+    STG_CUDA_TRY(cudaFuncSetAttribute(k_init<T>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
+    STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_a_tiled<T>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
+    STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_b<T, B>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
+    STG_CUDA_TRY(cudaFuncSetAttribute(k_replace, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
+    STG_CUDA_TRY(cudaFuncSetAttribute(k_restrict01<BB>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
+    STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_c1<BB>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
+    STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_c2<BB>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
+    STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_d<BB>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
+    STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_d16, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
+    STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_e<T, B>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
+    done = true;
+    return 0;
+}
+
 template <typename T, int B>
 static int pcg_run(Solver& S, PcgDev& c, int& h_done)
 {
+    STG_TRY((set_carveouts<T, B>()));
     cudaStream_t s = S.stream;
     PcgState& P = S.pcg;
     const int grid_vec = std::max(1, std::min(div_up(c.n, PB), kSMs * 4));
@@ -1353,7 +1737,23 @@ static int pcg_run(Solver& S, PcgDev& c, int& h_done)
     return 0;
 }
 
-// Times `reps` launches of the phase-A SpMV on the last solved system (measurement hook).
+// reads `n` 16-byte words (evicts the L2 without leaving dirty lines to write back)
+__global__ void k_l2_scrub(const uint4* __restrict__ buf, size_t n, unsigned* sink)
+{
+    unsigned acc = 0;
+    for(size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    {
+        const uint4 v = __ldcs(buf + i);
+        acc ^= v.x ^ v.y ^ v.z ^ v.w;
+    }
+    if(acc == 0x9e3779b9u) *sink = acc;  // keeps the loads; the buffer is zero, never taken
+}
+
+// Times `reps` launches of the phase-A SpMV (the tiled kernel the iteration runs) on the
+// last solved system (measurement hook).  Before every launch a 256 MiB buffer (twice the
+// L2) is read, so each launch starts with the matrix out of L2 as in the PCG loop, where
+// the bank inverses and vectors stream through L2 between two SpMVs; each launch is timed
+// alone with CUDA events on the handle's stream and the durations are averaged.
 int profile_spmv(Solver& S, int reps, float* avg_ms, double* bytes)
 {
     if(!S.pcg_ready)
@@ -1364,35 +1764,42 @@ int profile_spmv(Solver& S, int reps, float* avg_ms, double* bytes)
     const bool fp32 = S.cfg.precision == STG_PREC_FP32;
     PcgDev c = S.pcg_dev;
     cudaStream_t s = S.stream;
-    int per_sm_a = 0;
-    if(fp32)
-        STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_a, k_phase_a<float>, PB, 0));
-    else
-        STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_a, k_phase_a<double>, PB, 0));
-    const int grid_rows = std::max(1, std::min(div_up(c.nrows, PB / 16), std::max(per_sm_a, 1) * kSMs));
+    const size_t flush_bytes = (size_t)256 << 20;
+    STG_CUDA_TRY(cudaFuncSetAttribute(k_l2_scrub, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      cudaSharedmemCarveoutMaxShared));
+    const bool fresh = S.pcg.flush.cap < flush_bytes;
+    STG_TRY(S.pcg.flush.resize(flush_bytes));
+    if(fresh) STG_CUDA_TRY(cudaMemsetAsync(S.pcg.flush.data(), 0, flush_bytes, s));
     int saved[4];
     STG_CUDA_TRY(cudaMemcpyAsync(saved, c.flags, sizeof(saved), cudaMemcpyDeviceToHost, s));
     STG_CUDA_TRY(cudaStreamSynchronize(s));
     STG_CUDA_TRY(cudaMemsetAsync(c.flags, 0, sizeof(int) * 4, s));
-    auto launch = [&]() {
+    auto launch = [&]() -> int {
         if(fp32)
-            k_phase_a<float><<<grid_rows, PB, 0, s>>>(c);
+            STG_TRY(launch_phase_a<float>(c, s));
         else
-            k_phase_a<double><<<grid_rows, PB, 0, s>>>(c);
+            STG_TRY(launch_phase_a<double>(c, s));
+        return 0;
     };
-    for(int i = 0; i < 3; i++) launch();
-    STG_LAUNCH_CHECK();
-    STG_CUDA_TRY(cudaEventRecord(S.ev[4], s));
-    for(int i = 0; i < reps; i++) launch();
-    STG_LAUNCH_CHECK();
-    STG_CUDA_TRY(cudaEventRecord(S.ev[5], s));
-    STG_CUDA_TRY(cudaEventSynchronize(S.ev[5]));
-    float ms = 0;
-    STG_CUDA_TRY(cudaEventElapsedTime(&ms, S.ev[4], S.ev[5]));
-    S.launches += reps + 3;
+    for(int i = 0; i < 3; i++) STG_TRY(launch());
+    double total = 0;
+    for(int i = 0; i < reps; i++)
+    {
+        k_l2_scrub<<<kSMs * 8, 256, 0, s>>>(reinterpret_cast<const uint4*>(S.pcg.flush.data()), flush_bytes / 16,
+                                            reinterpret_cast<unsigned*>(c.counters + 7));
+        STG_LAUNCH_CHECK();
+        STG_CUDA_TRY(cudaEventRecord(S.ev[4], s));
+        STG_TRY(launch());
+        STG_CUDA_TRY(cudaEventRecord(S.ev[5], s));
+        STG_CUDA_TRY(cudaEventSynchronize(S.ev[5]));
+        float ms = 0;
+        STG_CUDA_TRY(cudaEventElapsedTime(&ms, S.ev[4], S.ev[5]));
+        total += ms;
+    }
+    S.launches += 2 * reps + 3;
     STG_CUDA_TRY(cudaMemcpyAsync(c.flags, saved, sizeof(saved), cudaMemcpyHostToDevice, s));
     STG_CUDA_TRY(cudaStreamSynchronize(s));
-    if(avg_ms) *avg_ms = ms / std::max(reps, 1);
+    if(avg_ms) *avg_ms = (float)(total / std::max(reps, 1));
     const double blk = fp32 ? 36.0 : 72.0, vec = fp32 ? 4.0 : 8.0;
     if(bytes) *bytes = (double)S.bcoo.nnzb * (blk + 8.0) + 3.0 * c.n * vec;
     return 0;
@@ -1443,8 +1850,8 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
     c.t_ptr = bcoo.t_ptr.data();
     c.t_ent = bcoo.t_ent.data();
     c.blk64 = reinterpret_cast<const double2*>(bcoo.blk64p.data());
-    c.fcol = bcoo.fcol.data();
-    c.fval = fp32 ? (const void*)bcoo.fval32.data() : (const void*)bcoo.fval64.data();
+    c.fent = bcoo.fent.data();
+    c.frow = bcoo.frow.data();
     c.fstride = bcoo.fstride;
     c.nrows = bcoo.nrows;
     c.n = n;

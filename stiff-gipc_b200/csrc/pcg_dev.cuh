@@ -14,9 +14,9 @@ struct PcgDev
     const int* cols;
     const int* t_ptr;
     const int2* t_ent;
-    const int* fcol;          // full symmetric row-sliced SoA copy (phase A)
-    const void* fval;         // 9 planes of `fstride` values in the iteration precision
-    size_t fstride;
+    const unsigned char* fent;  // full symmetric row-sliced copy in 16-byte planes (phase A)
+    const int* frow;          // [nrows+1] first entry of each row in fent
+    size_t fstride;           // entries per plane
     const double2* blk64;     // FP64 padded upper blocks (residual replacement)
     int nrows, n;
     // vectors in the iteration precision T, one 4-wide (16 B FP32 / 32 B FP64) slot per block

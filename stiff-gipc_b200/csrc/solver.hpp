@@ -35,11 +35,11 @@ struct Bcoo
     DBuf<int> t_cnt;             // [nrows+1]
     DBuf<int2> t_ent;            // [offdiag]
     DBuf<double> blk64p;         // FP64 blocks padded to 80 B (5 x double2), residual replacement
-    // full symmetric row-sliced SoA copy for the PCG SpMV (see k_build_full in pcg.cu)
-    DBuf<int> fcol;
-    DBuf<float> fval32;
-    DBuf<double> fval64;
-    size_t fstride = 0;
+    // full symmetric row-sliced copy for the PCG SpMV in 16-byte planes (FullPlanes in
+    // spmv_core.cuh, built by k_build_full in pcg.cu)
+    DBuf<unsigned char> fent;
+    DBuf<int> frow;              // [nrows+1] first entry of each row (row_ptr + t_ptr)
+    size_t fstride = 0;          // entries per plane
     DBuf<double> diag_inv;       // 3x3 block-Jacobi inverses [nrows*9]
     int offdiag = 0;
 
@@ -91,6 +91,7 @@ struct PcgState
     DBuf<unsigned> counters;       // last-block counters
     DBuf<int> flags;               // [0] done, [1] status, [2] replacements
     DBuf<unsigned> bar;            // persistent grid barrier
+    DBuf<unsigned char> flush;     // 256 MiB written between timed SpMV launches (L2 flush)
     cudaGraphExec_t graph = nullptr;
 };
 

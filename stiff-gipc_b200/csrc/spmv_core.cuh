@@ -64,4 +64,91 @@ __device__ __forceinline__ void row_spmv(int i, bool valid, int sub, const int* 
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// Full symmetric row-sliced copy of the matrix for the PCG SpMV, in 16-byte planes.
+// Row i holds, sorted by column, its lower blocks (transposes of the upper blocks k with
+// col(k) == i) followed by its upper blocks; entry e of row i sits at f = frow[i] + e.
+// Entry f of a plane copy with S entries per plane is stored as
+//   FP32: plane 0 {h0 h1 h2 h3} at 16 f, plane 1 {h4 h5 h6 h7} at 16 S + 16 f,
+//         tail {h8, col} at 32 S + 8 f                                     (40 B per entry)
+//   FP64: planes p = 0..3 {h(2p) h(2p+1)} at 16 p S + 16 f,
+//         tail {h8, col, 0} at 64 S + 16 f                                 (80 B per entry)
+// (h column-major).  Lanes that read consecutive entries read consecutive 16-byte (or 8-byte)
+// words of every plane: coalesced in global memory and free of shared-memory bank
+// conflicts, and a row range is one contiguous range of every plane (one bulk copy each).
+// ---------------------------------------------------------------------------------------
+template <typename T>
+struct FullPlanes
+{
+    static constexpr int NP = sizeof(T) == 4 ? 2 : 4;     // 16-byte value planes
+    static constexpr int TAIL = sizeof(T) == 4 ? 8 : 16;  // bytes of the {h8, col} plane
+    static constexpr int ES = 16 * NP + TAIL;             // bytes per entry
+};
+
+__device__ __forceinline__ void load_entry(const unsigned char* base, size_t S, int f, float h[9], int& col)
+{
+    const float4 a = reinterpret_cast<const float4*>(base)[f];
+    const float4 b = reinterpret_cast<const float4*>(base + 16 * S)[f];
+    const float2 t = reinterpret_cast<const float2*>(base + 32 * S)[f];
+    h[0] = a.x; h[1] = a.y; h[2] = a.z; h[3] = a.w;
+    h[4] = b.x; h[5] = b.y; h[6] = b.z; h[7] = b.w;
+    h[8] = t.x;
+    col = __float_as_int(t.y);
+}
+
+__device__ __forceinline__ void load_entry(const unsigned char* base, size_t S, int f, double h[9], int& col)
+{
+#pragma unroll
+    for(int p = 0; p < 4; p++)
+    {
+        const double2 v = reinterpret_cast<const double2*>(base + 16 * p * S)[f];
+        h[2 * p] = v.x;
+        h[2 * p + 1] = v.y;
+    }
+    const double2 t = reinterpret_cast<const double2*>(base + 64 * S)[f];
+    h[8] = t.x;
+    col = (int)__double_as_longlong(t.y);
+}
+
+// the same from global memory through the read-only path
+__device__ __forceinline__ void ldg_entry(const unsigned char* base, size_t S, int f, float h[9], int& col)
+{
+    const float4 a = __ldg(reinterpret_cast<const float4*>(base) + f);
+    const float4 b = __ldg(reinterpret_cast<const float4*>(base + 16 * S) + f);
+    const float2 t = __ldg(reinterpret_cast<const float2*>(base + 32 * S) + f);
+    h[0] = a.x; h[1] = a.y; h[2] = a.z; h[3] = a.w;
+    h[4] = b.x; h[5] = b.y; h[6] = b.z; h[7] = b.w;
+    h[8] = t.x;
+    col = __float_as_int(t.y);
+}
+
+__device__ __forceinline__ void ldg_entry(const unsigned char* base, size_t S, int f, double h[9], int& col)
+{
+#pragma unroll
+    for(int p = 0; p < 4; p++)
+    {
+        const double2 v = __ldg(reinterpret_cast<const double2*>(base + 16 * p * S) + f);
+        h[2 * p] = v.x;
+        h[2 * p + 1] = v.y;
+    }
+    const double2 t = __ldg(reinterpret_cast<const double2*>(base + 64 * S) + f);
+    h[8] = t.x;
+    col = (int)__double_as_longlong(t.y);
+}
+
+// writes entry f (h column-major) into a plane copy with S entries per plane
+__device__ __forceinline__ void store_entry(unsigned char* base, size_t S, size_t f, const float h[9], int col)
+{
+    reinterpret_cast<float4*>(base)[f] = make_float4(h[0], h[1], h[2], h[3]);
+    reinterpret_cast<float4*>(base + 16 * S)[f] = make_float4(h[4], h[5], h[6], h[7]);
+    reinterpret_cast<float2*>(base + 32 * S)[f] = make_float2(h[8], __int_as_float(col));
+}
+
+__device__ __forceinline__ void store_entry(unsigned char* base, size_t S, size_t f, const double h[9], int col)
+{
+#pragma unroll
+    for(int p = 0; p < 4; p++) reinterpret_cast<double2*>(base + 16 * p * S)[f] = make_double2(h[2 * p], h[2 * p + 1]);
+    reinterpret_cast<double2*>(base + 64 * S)[f] = make_double2(h[8], __longlong_as_double((long long)(unsigned)col));
+}
+
 }  // namespace stg
