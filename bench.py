@@ -122,6 +122,23 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+PROFILE_A = "profiles/k_phase_a_tiled_hetcube48.md"
+
+
+def profiled_traffic(workload):
+    """DRAM bytes (read + write) of one SpMV-phase launch from the committed ncu summary of
+    the same kernel on the same workload, or None."""
+    if workload != "hetcube48":
+        return None
+    try:
+        for line in open(os.path.join(ROOT, PROFILE_A)):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def cpu_baseline(sysm, budget_s, bank):
     """The oracle's MAS-PCG (single thread C port) on a bounded sample: convert + MAS build +
     assembly once, then PCG iterations until the relative residual reaches 1e-4 or the time
@@ -296,6 +313,7 @@ def main():
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
+    traffic = profiled_traffic(args.workload)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -331,10 +349,12 @@ def main():
             "fp32_vs_fp64_solution_rel_err": err_fast,
             "phases_ms": {k: round(st_fast[k], 3) for k in ("ms_convert", "ms_mas_build", "ms_mas_assemble", "ms_pcg")},
             "dof_iter_per_s": sysm.n * st_fast["iterations"] / (ms_fast * 1e-3),
-            "roofline": {"bound": "hbm", "kernel": "k_pcg_spmv<float>", "achieved": achieved, "peak": hbm,
-                         "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+            "roofline": {"bound": "hbm", "kernel": "k_phase_a_tiled<float>", "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                         "traffic_source": PROFILE_A if traffic else None,
+                         "timing": "each launch alone after reading a 256 MiB buffer (L2 cold), CUDA events",
                          "bytes_per_launch": spmv_bytes, "ms_per_launch": spmv_ms,
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650"},
+                         "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650"},
             "cpu_baseline": cpu,
             "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(st_fast["kernel_launches"] * args.steps),

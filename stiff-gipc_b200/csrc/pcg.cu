@@ -696,7 +696,7 @@ __global__ void __launch_bounds__(D_WARPS * 32) k_phase_d16(PcgDev c)
 // of every plane of the full copy (FullPlanes), so one producer lane moves a whole tile with
 // one bulk copy per plane, plus one for the tile's row bounds, into a ring of stages that
 // complete on per-stage mbarriers.  Eight consumer warps compute the tile from shared memory
-// (16-byte loads, no bank conflicts) with LPR lanes per row (4 FP32, 8 FP64): lane `sub`
+// (16-byte loads) with LPR lanes per row (4 FP32, 8 FP64): lane `sub`
 // sums the entries sub, sub + LPR, ... of its row in order, four at a time with their
 // neighbour gathers of z / p issued before the block values are read, and an xor tree over
 // the LPR lanes finishes the row.  A tile with more entries than a stage holds is computed
@@ -1927,6 +1927,12 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
     int status = h_flags[F_DONE] ? h_flags[F_STATUS] : STG_MAX_ITER;
     if(status == STG_ERR_TIMEOUT) set_error("persistent PCG: a grid barrier wait gave up");
     const long iters = max_iter <= 1 ? 1 : (long)h_scal[S_ITER];
+    if(cfg.loop_mode == STG_LOOP_GRAPH && max_iter > 1)
+    {
+        // the graph's body ran once per iteration; its IF node (residual replacement plus
+        // the level-0/1 re-restriction) once per replacement
+        launches += (int)iters * launches_per_batch + h_flags[F_REPL] * (use_mas ? 2 : 1);
+    }
     if(st)
     {
         st->iterations = (int)iters;
