@@ -1,0 +1,154 @@
+"""Batches of independent Newton systems of uneven size, and their sharding over ranks.
+
+A batch (e.g. 256 cubes of 375 to 47k DOFs, each with its own Hessian, contacts and MAS
+partition) is solved scene by scene through the same C ABI as a single system
+(``stg_solve_linear_system``).  On one GPU the scenes are spread over ``streams`` CUDA
+streams, one host thread and one handle per scene.  The ctypes calls release the GIL, so
+the solves overlap on the device: every scene runs its own graph-captured PCG, and small
+scenes fill the SMs that a single small solve leaves idle.  Results are bitwise those of
+a solve of the scene alone (the kernels are deterministic and per-handle).
+
+Over several ranks the scenes are the units: ``shard_by_dof`` assigns whole scenes to
+ranks by greedy DOF-balanced bin packing (largest first, onto the least-loaded rank).
+Each rank solves its shard with no exchange during the solves.  The only collective is the
+final gather of the per-scene statistics (``solve_distributed``).
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+from typing import Callable, List, Optional, Sequence
+
+import numpy as np
+
+from .linear_system import PCGSolverConfig, Solver
+
+
+def shard_by_dof(dofs: Sequence[int], world: int) -> List[List[int]]:
+    """Scene indices per rank: largest scene first onto the least-loaded rank (ties go to
+    the lower rank); each shard sorted.  Deterministic, so every rank computes the same
+    assignment without communicating."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(dofs)), key=lambda i: (-int(dofs[i]), i))
+    loads = [0] * world
+    shards: List[List[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (loads[k], k))
+        shards[r].append(i)
+        loads[r] += int(dofs[i])
+    return [sorted(s) for s in shards]
+
+
+class BatchSolver:
+    """Solves a list of ``scenes.NewtonSystem`` on one GPU over ``streams`` CUDA streams."""
+
+    def __init__(self, systems, config: Optional[PCGSolverConfig] = None, device="cuda", streams: int = 8):
+        import torch
+        self.config = config or PCGSolverConfig()
+        self.device = torch.device(device)
+        if self.device.index is None:
+            self.device = torch.device(self.device.type, torch.cuda.current_device())
+        self.systems = list(systems)
+        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(max(1, min(streams, len(self.systems))))]
+        self.items = []
+        for k, s in enumerate(self.systems):
+            st = self.streams[k % len(self.streams)]
+            solver = Solver(self.config, stream=st)
+            if self.config.preconditioner == "mas":
+                pm, rm = s.slot_maps(self.config.bank_size)
+                solver.mas_init(s.num_verts, s.neighbor_start, s.neighbor_num, s.neighbor_list, pm, rm,
+                                collision_node_offset=0)
+            with torch.cuda.stream(st):
+                t = dict(rows=torch.from_numpy(s.rows).to(self.device), cols=torch.from_numpy(s.cols).to(self.device),
+                         blocks=torch.from_numpy(s.blocks.reshape(-1)).to(self.device),
+                         b=torch.from_numpy(s.b).to(self.device),
+                         contacts=(torch.from_numpy(s.contacts).to(self.device) if s.contacts.size else None))
+                t["x"] = torch.zeros_like(t["b"])
+            self.items.append((solver, st, t, s))
+        torch.cuda.synchronize(self.device)
+
+    def _solve_lane(self, lane: int) -> list:
+        import torch
+        torch.cuda.set_device(self.device)
+        out = []
+        for k in range(lane, len(self.items), len(self.streams)):
+            solver, st, t, s = self.items[k]
+            stats = solver.solve_linear_system(t["rows"], t["cols"], t["blocks"], t["b"], t["x"],
+                                               fem_block_offset=s.fem_block_offset, contacts=t["contacts"])
+            out.append((k, stats))
+        return out
+
+    def solve(self) -> List[dict]:
+        """One Newton solve of every scene; per-scene statistics in scene order."""
+        res: List[Optional[dict]] = [None] * len(self.items)
+        with cf.ThreadPoolExecutor(max_workers=len(self.streams)) as ex:
+            for part in ex.map(self._solve_lane, range(len(self.streams))):
+                for k, stats in part:
+                    res[k] = stats
+        return res  # type: ignore[return-value]
+
+    def upload_from_host(self):
+        """Copies every scene's triplets, b (and contacts) again from pinned host memory on
+        the scene's stream (the host-to-device part of an end-to-end step)."""
+        import torch
+        if not hasattr(self, "_host"):
+            self._host = []
+            for _, _, t, _ in self.items:
+                self._host.append({k: v.cpu().pin_memory() for k, v in t.items() if v is not None and k != "x"})
+        for (solver, st, t, s), h in zip(self.items, self._host):
+            with torch.cuda.stream(st):
+                for k, v in h.items():
+                    t[k].copy_(v, non_blocking=True)
+
+    def host_bytes(self):
+        """(host-to-device, device-to-host) bytes of one end-to-end step."""
+        h2d = sum(v.numel() * v.element_size() for _, _, t, _ in self.items for k, v in t.items()
+                  if v is not None and k != "x")
+        d2h = sum(t["x"].numel() * t["x"].element_size() for _, _, t, _ in self.items)
+        return h2d, d2h
+
+    def solution(self, k: int) -> np.ndarray:
+        return self.items[k][2]["x"].cpu().numpy()
+
+    def close(self):
+        for solver, _, _, _ in self.items:
+            solver.close()
+        self.items = []
+
+
+def solve_distributed(systems, rank: int, world: int, solve_shard: Optional[Callable] = None,
+                      config: Optional[PCGSolverConfig] = None, streams: int = 8, group=None) -> List[dict]:
+    """Solves ``systems`` sharded over ``world`` ranks (whole scenes per rank, see
+    shard_by_dof) and returns every scene's statistics, in scene order, on every rank.
+
+    ``solve_shard(list_of_systems) -> list_of_stats`` solves one rank's scenes (default: a
+    BatchSolver on this rank's current GPU).  The statistics are gathered with
+    ``torch.distributed.all_gather_object`` when ``world > 1``.
+    """
+    shards = shard_by_dof([s.n for s in systems], world)
+    mine = shards[rank]
+    if solve_shard is None:
+        def solve_shard(local):
+            bs = BatchSolver(local, config=config, streams=streams)
+            try:
+                return bs.solve()
+            finally:
+                bs.close()
+    local_stats = solve_shard([systems[i] for i in mine]) if mine else []
+    pairs = list(zip(mine, local_stats))
+    if world > 1:
+        import torch.distributed as dist
+        gathered: list = [None] * world
+        dist.all_gather_object(gathered, pairs, group=group)
+    else:
+        gathered = [pairs]
+    out: List[Optional[dict]] = [None] * len(systems)
+    for part in gathered:
+        for i, st in part:
+            if out[i] is not None:
+                raise RuntimeError(f"scene {i} solved on two ranks")
+            out[i] = st
+    missing = [i for i, st in enumerate(out) if st is None]
+    if missing:
+        raise RuntimeError(f"scenes {missing[:8]} were not solved")
+    return out  # type: ignore[return-value]
