@@ -549,18 +549,18 @@ __device__ __forceinline__ void phase_d(const PcgDev& c, int b0, int b1, int bst
 // D (16-vertex banks): one warp per bank, the bank's packed inverse (136 3x3 FP32 blocks,
 // 4,896 B) and its 16 residual slots (256 B) staged in shared memory by the Tensor Memory
 // Accelerator (cp.async.bulk, completion on an mbarrier), double-buffered so that the copy
-// of the warp's next bank overlaps the solve of the current one.
+// of the warp's next bank overlaps the solve of the current one.  Lane (a, h) = (l & 15,
+// l >> 4) forms block row a of z = P r over the column blocks cc = 8h + ((j + a) & 7),
+// j < 8 (upper block (a, cc) as stored, lower ones as the transpose of (cc, a)); the two
+// halves meet in one shuffle.  The rotation by a spreads a warp's block reads over the
+// shared-memory banks (1.9 wavefronts per load on average, at most 2).
 // ---------------------------------------------------------------------------------------
 constexpr int D_WARPS = 4;                        // warps per CTA
 constexpr int D_PBYTES = 136 * 9 * 4;             // packed inverse of one bank
 constexpr int D_RBYTES = 16 * 16;                 // 16 float4 residual slots
 constexpr int D_BUF = D_PBYTES + D_RBYTES;        // one stage (16-byte multiple)
-constexpr int D_PART = 16 * 65;                   // partial products, row stride 65 floats
-constexpr int D_WARP_BYTES = 2 * D_BUF + D_PART * 4 + 16;
+constexpr int D_WARP_BYTES = 2 * D_BUF + 16;      // two stages + two mbarriers
 constexpr unsigned D_WAIT_LIMIT = 1u << 22;       // bounded mbarrier polling
-
-// (row, col) of packed upper block k of a 16-bank
-__constant__ unsigned char c_upper16[136][2];
 
 __device__ __forceinline__ unsigned smem_u32(const void* p)
 {
@@ -606,10 +606,23 @@ __global__ void __launch_bounds__(D_WARPS * 32) k_phase_d16(PcgDev c)
     char* base = dsm + (size_t)warp * D_WARP_BYTES;
     char* const stage0 = base;
     char* const stage1 = base + D_BUF;
-    float* part = reinterpret_cast<float*>(base + 2 * D_BUF);
-    const unsigned bar0 = smem_u32(base + 2 * D_BUF + D_PART * 4), bar1 = bar0 + 8;
+    const unsigned bar0 = smem_u32(base + 2 * D_BUF), bar1 = bar0 + 8;
     const int gw = blockIdx.x * D_WARPS + warp, nw = gridDim.x * D_WARPS;
     if(gw >= c.nbanks) return;
+    // this lane's eight blocks: word offset of block k in the packed upper order and
+    // whether it is used transposed (the stored block is (cc, a) with cc < a)
+    const int a = lane & 15, h = lane >> 4;
+    int koff[8], rcol[8];
+    unsigned tmask = 0u;
+#pragma unroll
+    for(int j = 0; j < 8; j++)
+    {
+        const int cc = 8 * h + ((j + a) & 7);
+        const int lo = min(a, cc), hi = max(a, cc);
+        koff[j] = 9 * (lo * 16 - lo * (lo - 1) / 2 + (hi - lo));
+        rcol[j] = 4 * cc;
+        if(cc < a) tmask |= 1u << j;
+    }
     if(lane == 0)
     {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0) : "memory");
@@ -648,43 +661,31 @@ __global__ void __launch_bounds__(D_WARPS * 32) k_phase_d16(PcgDev c)
             ph0 ^= 1u;
         const float* P = reinterpret_cast<const float*>(cur);
         const float* rs = reinterpret_cast<const float*>(cur + D_PBYTES);
+        float z0 = 0.f, z1 = 0.f, z2 = 0.f;
 #pragma unroll
-        for(int m = 0; m < 5; m++)
+        for(int j = 0; j < 8; j++)
         {
-            const int k = lane + 32 * m;
-            if(k < 136)
+            const float* H = P + koff[j];  // column-major 3x3
+            const float4 r = *reinterpret_cast<const float4*>(rs + rcol[j]);
+            const float h0 = H[0], h1 = H[1], h2 = H[2], h3 = H[3], h4 = H[4], h5 = H[5], h6 = H[6], h7 = H[7],
+                        h8 = H[8];
+            if(tmask & (1u << j))
             {
-                const int a = c_upper16[k][0], cc = c_upper16[k][1];
-                const float* h = P + 9 * k;  // column-major 3x3
-                const float x0 = rs[4 * cc], x1 = rs[4 * cc + 1], x2 = rs[4 * cc + 2];
-                float* pa = part + a * 65 + cc * 4;
-                pa[0] = h[0] * x0 + h[3] * x1 + h[6] * x2;
-                pa[1] = h[1] * x0 + h[4] * x1 + h[7] * x2;
-                pa[2] = h[2] * x0 + h[5] * x1 + h[8] * x2;
-                if(cc != a)
-                {
-                    const float y0 = rs[4 * a], y1 = rs[4 * a + 1], y2 = rs[4 * a + 2];
-                    float* pc = part + cc * 65 + a * 4;  // H^T r_a into row cc
-                    pc[0] = h[0] * y0 + h[1] * y1 + h[2] * y2;
-                    pc[1] = h[3] * y0 + h[4] * y1 + h[5] * y2;
-                    pc[2] = h[6] * y0 + h[7] * y1 + h[8] * y2;
-                }
+                z0 += h0 * r.x + h1 * r.y + h2 * r.z;
+                z1 += h3 * r.x + h4 * r.y + h5 * r.z;
+                z2 += h6 * r.x + h7 * r.y + h8 * r.z;
+            }
+            else
+            {
+                z0 += h0 * r.x + h3 * r.y + h6 * r.z;
+                z1 += h1 * r.x + h4 * r.y + h7 * r.z;
+                z2 += h2 * r.x + h5 * r.y + h8 * r.z;
             }
         }
-        __syncwarp();
-        if(lane < 16)
-        {
-            float z0 = 0.f, z1 = 0.f, z2 = 0.f;
-            const float* pr = part + lane * 65;
-#pragma unroll
-            for(int col = 0; col < 16; col++)
-            {
-                z0 += pr[4 * col];
-                z1 += pr[4 * col + 1];
-                z2 += pr[4 * col + 2];
-            }
-            st4(c.Z + ((size_t)bk * 16 + lane) * 4, z0, z1, z2);
-        }
+        z0 += __shfl_xor_sync(0xffffffffu, z0, 16);
+        z1 += __shfl_xor_sync(0xffffffffu, z1, 16);
+        z2 += __shfl_xor_sync(0xffffffffu, z2, 16);
+        if(h == 0) st4(c.Z + ((size_t)bk * 16 + a) * 4, z0, z1, z2);
         __syncwarp();
     }
 }
@@ -1459,20 +1460,6 @@ static int launch_mas_cd(Solver& S, const PcgDev& c)
     return 0;
 }
 
-// (row, col) of every packed upper block of a 16-bank, for k_phase_d16
-static int upload_upper16(cudaStream_t s)
-{
-    static unsigned char tab[136][2];
-    int k = 0;
-    for(int a = 0; a < 16; a++)
-        for(int col = a; col < 16; col++, k++)
-        {
-            tab[k][0] = (unsigned char)a;
-            tab[k][1] = (unsigned char)col;
-        }
-    STG_CUDA_TRY(cudaMemcpyToSymbolAsync(c_upper16, tab, sizeof(tab), 0, cudaMemcpyHostToDevice, s));
-    return 0;
-}
 
 // tiled phase A: the shared-memory opt-in and one resident wave of CTAs
 template <typename T>
@@ -1833,7 +1820,6 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
     const size_t zp_bytes = (8 * nr * es + 255) / 256 * 256, q_bytes = (4 * nr * es + 255) / 256 * 256;
     STG_TRY(P.vbuf.resize((2 * zp_bytes + q_bytes) / sizeof(double) + 32));
     STG_TRY(pack_blocks(*this));
-    if(use_mas && cfg.bank_size == 16) STG_TRY(upload_upper16(s));
     const int slots = kSMs * 8;
     STG_TRY(P.partials.resize((size_t)slots * 6));
     STG_TRY(P.scal.resize(S_COUNT));
