@@ -479,6 +479,100 @@ __global__ void __launch_bounds__(3 * B) k_mas_invert(const double* __restrict__
     }
 }
 
+// The same Gauss-Jordan for 16-banks with each column in registers: thread i of a bank owns
+// column i (48 doubles); pivot j broadcasts the old column j through shared memory and every
+// column updates itself, all loop indices compile-time (fully unrolled).  The operation
+// order per element is the one of k_mas_invert, so the results are the same; only shared
+// memory traffic is gone (one column per pivot instead of a load and a store per FMA).
+// Two banks per CTA, 64 threads per bank (lanes 48..63 idle).
+constexpr int INV16_BANKS = 2;
+
+__global__ void __launch_bounds__(64 * INV16_BANKS) k_mas_invert16(const double* __restrict__ mat, float* inv, int nbanks)
+{
+    constexpr int B = 16, N = 48;
+    const int NS = nsym(B);
+    __shared__ double colj[INV16_BANKS][N];
+    __shared__ double band[INV16_BANKS][N][5];  // A[i + d][i], d = -2..2, for the final mirror
+    const int g = threadIdx.x / 64, i = threadIdx.x % 64;
+    const int bk = blockIdx.x * INV16_BANKS + g;
+    const bool live = bk < nbanks && i < N;
+    double c[N];
+    const double* Mb = mat + (size_t)(bk < nbanks ? bk : 0) * NS * 9;
+#pragma unroll
+    for(int j = 0; j < N; j++)
+    {
+        double v = 0.0;
+        if(live)
+        {
+            const int rowId = j / 3, colId = i / 3;
+            if(colId >= rowId)
+                v = Mb[upper_index(B, rowId, colId) * 9 + (i % 3) * 3 + (j % 3)];
+            else
+                v = Mb[upper_index(B, colId, rowId) * 9 + (j % 3) * 3 + (i % 3)];
+            if(i == j && v == 0.0) v = 1.0;
+        }
+        c[j] = v;  // A[j][i]
+    }
+#pragma unroll
+    for(int j = 0; j < N; j++)
+    {
+        if(i == j)
+        {
+#pragma unroll
+            for(int k = 0; k < N; k++) colj[g][k] = c[k];
+        }
+        __syncthreads();
+        const double rt = colj[g][j];
+        if(i == j)
+        {
+#pragma unroll
+            for(int k = 0; k < N; k++) c[k] = (k == j) ? 1.0 : 0.0;
+        }
+        c[j] /= rt;
+        const double aji = c[j];
+#pragma unroll
+        for(int k = 0; k < N; k++)
+            if(k != j) c[k] = fma(-colj[g][k], aji, c[k]);
+        __syncthreads();
+    }
+    // lower triangle of the diagonal 3x3 blocks mirrored from the upper one (as k_mas_invert)
+    if(i < N)
+    {
+#pragma unroll
+        for(int d = -2; d <= 2; d++)
+        {
+            double v = 0.0;
+#pragma unroll
+            for(int k = 0; k < N; k++)
+                if(k == i + d) v = c[k];
+            band[g][i][d + 2] = v;
+        }
+    }
+    __syncthreads();
+    if(i < N)
+    {
+        // lower entries (1,0), (2,1), (2,0) of the diagonal 3x3 block from (0,1), (1,2), (0,2);
+        // band[col][d + 2] = A[col + d][col]
+        const double v1 = i % 3 < 2 ? band[g][i + 1][1] : 0.0;   // A[i][i + 1]
+        const double v2 = i % 3 == 0 ? band[g][i + 2][0] : 0.0;  // A[i][i + 2]
+#pragma unroll
+        for(int k = 0; k < N; k++)
+        {
+            if(i % 3 < 2 && k == i + 1) c[k] = v1;
+            if(i % 3 == 0 && k == i + 2) c[k] = v2;
+        }
+    }
+    __syncthreads();
+    if(!live) return;
+    float* P = inv + (size_t)bk * NS * 9;
+#pragma unroll
+    for(int j = 0; j < N; j++)
+    {
+        const int rowId = j / 3, colId = i / 3;
+        if(colId >= rowId) P[upper_index(B, rowId, colId) * 9 + (i % 3) * 3 + (j % 3)] = (float)c[j];
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 // apply
 // ---------------------------------------------------------------------------------------
@@ -888,11 +982,19 @@ static int mas_assemble_t(Solver& S, int offset)
             nnz = nnz2;
         }
     }
-    const size_t smem = sizeof(double) * (3 * B * 3 * B + 3 * B);
-    if(smem > 48 * 1024)
-        STG_CUDA_TRY(cudaFuncSetAttribute(k_mas_invert<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_mas_invert<B><<<m.nbanks, 3 * B, smem, s>>>(m.mat.data(), m.inv.data(), m.nbanks);
-    STG_LAUNCH_CHECK();
+    if(B == 16)
+    {
+        k_mas_invert16<<<div_up(m.nbanks, INV16_BANKS), 64 * INV16_BANKS, 0, s>>>(m.mat.data(), m.inv.data(), m.nbanks);
+        STG_LAUNCH_CHECK();
+    }
+    else
+    {
+        const size_t smem = sizeof(double) * (3 * B * 3 * B + 3 * B);
+        if(smem > 48 * 1024)
+            STG_CUDA_TRY(cudaFuncSetAttribute(k_mas_invert<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_mas_invert<B><<<m.nbanks, 3 * B, smem, s>>>(m.mat.data(), m.inv.data(), m.nbanks);
+        STG_LAUNCH_CHECK();
+    }
     S.launches++;
     m.assembled = true;
     return 0;
