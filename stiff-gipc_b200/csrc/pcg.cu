@@ -67,7 +67,8 @@ __device__ __forceinline__ void set_conditionals(const PcgDev& c, int op)
 }
 
 template <int BLOCK = PB>
-__device__ __forceinline__ void finish_reduction(const PcgDev& c, double v, int site, int op, int slot = 0)
+__device__ __forceinline__ void finish_reduction(const PcgDev& c, double v, int site, int op, int slot = 0,
+                                                 double aux = 0.0)
 {
     __shared__ double red[BLOCK / 32];
     __shared__ bool last;
@@ -88,11 +89,27 @@ __device__ __forceinline__ void finish_reduction(const PcgDev& c, double v, int 
     const double tot = block_sum<BLOCK>(acc, red);
     if(threadIdx.x == 0)
     {
-        post_op(op, slot, tot, c.scal, c.flags, c.prm);
-        set_conditionals(c, op);
+        post_op(op, slot, tot, c.scal, c.flags, c.prm, aux);
+        set_conditionals(c, op == POST_CHECK_PQ ? (int)POST_CHECK : op);
         *counter = 0u;
         __threadfence();
     }
+}
+
+// p.q of the SpMV phase, finished by each CTA of the consumer (phase B) from the SpMV
+// phase's per-CTA partials, in the same fixed order in every CTA (so every CTA gets the
+// same value): the SpMV phase needs no last-CTA step of its own.
+__device__ __forceinline__ double consume_pq(const PcgDev& c)
+{
+    __shared__ double red[PB / 32];
+    __shared__ double tot;
+    const double* part = c.partials + (size_t)SITE_A * c.slots;
+    double a = 0;
+    for(int t = threadIdx.x; t < c.grid_a; t += PB) a += __ldcg(part + t);
+    const double s = block_sum<PB>(a, red);
+    if(threadIdx.x == 0) tot = s;
+    __syncthreads();
+    return tot;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -296,9 +313,8 @@ __device__ __forceinline__ void axpy_row(const PcgDev& c, const T* pn, const T* 
 }
 
 template <typename T, int B>
-__device__ __forceinline__ double phase_b_mas(const PcgDev& c, int gt, int gn)
+__device__ __forceinline__ double phase_b_mas(const PcgDev& c, int gt, int gn, double alpha)
 {
-    const double alpha = __ldcg(c.scal + SS_ALPHA);
     const T* pn = zpbuf<T>(c, iter_parity(c) ^ 1);
     const T* q = reinterpret_cast<const T*>(c.q);
     double acc = 0;
@@ -353,9 +369,8 @@ __device__ __forceinline__ double phase_b_mas(const PcgDev& c, int gt, int gn)
 
 // B (block-Jacobi / identity): plain axpy over all block rows
 template <typename T>
-__device__ __forceinline__ double phase_b_plain(const PcgDev& c, int gt, int gn)
+__device__ __forceinline__ double phase_b_plain(const PcgDev& c, int gt, int gn, double alpha)
 {
-    const double alpha = __ldcg(c.scal + SS_ALPHA);
     const T* pn = zpbuf<T>(c, iter_parity(c) ^ 1);
     const T* q = reinterpret_cast<const T*>(c.q);
     double acc = 0;
@@ -1015,7 +1030,10 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T>::MIN_CTAS) k_phase_a_tiled
             atomicExch(c.flags + F_DONE, 1);
         }
     }
-    finish_reduction<A_THREADS>(c, acc, SITE_A, POST_ALPHA);
+    // p.q: this CTA's partial only; phase B finishes the sum (consume_pq)
+    __shared__ double red[A_THREADS / 32];
+    const double bs = block_sum<A_THREADS>(acc, red);
+    if(threadIdx.x == 0) c.partials[(size_t)SITE_A * c.slots + blockIdx.x] = bs;
 }
 
 // E (MAS): z = sum over levels (FP32) on the FEM range + ABD block-Jacobi; share of r.z
@@ -1128,8 +1146,14 @@ template <typename T, int B>
 __global__ void __launch_bounds__(PB, 8) k_phase_b(PcgDev c)
 {
     if(c.flags[F_DONE]) return;
-    const double v = B > 0 ? phase_b_mas<T, (B > 0 ? B : 16)>(c, GT, GN) : phase_b_plain<T>(c, GT, GN);
-    finish_reduction(c, v, SITE_B, POST_CHECK);
+    const double pq = consume_pq(c);
+    double v = 0;
+    if(pq > 0.0 && isfinite(pq))  // else breakdown: no update; the last CTA reports it
+    {
+        const double alpha = __ldcg(c.scal + SS_RZ) / pq;
+        v = B > 0 ? phase_b_mas<T, (B > 0 ? B : 16)>(c, GT, GN, alpha) : phase_b_plain<T>(c, GT, GN, alpha);
+    }
+    finish_reduction(c, v, SITE_B, POST_CHECK_PQ, 0, pq);
 }
 
 // guarded: runs only when this iteration is a replacement iteration (host / plain graph),
@@ -1268,7 +1292,8 @@ __global__ void __launch_bounds__(PB) k_pcg_persistent(PcgDev c)
         if(is_done(c)) break;
         grid_barrier(c, phase_a<T>(c, gt, gn), SITE_A, POST_ALPHA, gen);
         if(is_done(c)) break;
-        const double vb = B > 0 ? phase_b_mas<T, BB>(c, gt, gn) : phase_b_plain<T>(c, gt, gn);
+        const double alpha = __ldcg(c.scal + SS_ALPHA);
+        const double vb = B > 0 ? phase_b_mas<T, BB>(c, gt, gn, alpha) : phase_b_plain<T>(c, gt, gn, alpha);
         grid_barrier(c, vb, SITE_B, POST_CHECK, gen);
         if(is_done(c)) break;
         const long k = (long)__ldcg(c.scal + SS_ITER);
@@ -1463,7 +1488,7 @@ static int launch_mas_cd(Solver& S, const PcgDev& c)
 
 // tiled phase A: the shared-memory opt-in and one resident wave of CTAs
 template <typename T>
-static int launch_phase_a(const PcgDev& c, cudaStream_t s)
+static int phase_a_grid(int nrows, int* grid)
 {
     static thread_local int per_sm = -1;
     if(per_sm < 0)
@@ -1473,7 +1498,20 @@ static int launch_phase_a(const PcgDev& c, cudaStream_t s)
         STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase_a_tiled<T>, A_THREADS,
                                                                    ATile<T>::SMEM));
     }
-    const int grid = std::max(1, std::min(div_up(c.nrows, ATile<T>::RT), std::max(per_sm, 1) * kSMs));
+    *grid = std::max(1, std::min(div_up(nrows, ATile<T>::RT), std::max(per_sm, 1) * kSMs));
+    return 0;
+}
+
+template <typename T>
+static int launch_phase_a(const PcgDev& c, cudaStream_t s)
+{
+    int grid = 0;
+    STG_TRY(phase_a_grid<T>(c.nrows, &grid));
+    if(grid != c.grid_a)
+    {
+        set_error("SpMV phase grid differs from the one phase B sums over");
+        return STG_ERR_INVALID;
+    }
     k_phase_a_tiled<T><<<grid, A_THREADS, ATile<T>::SMEM, s>>>(c);
     STG_LAUNCH_CHECK();
     return 0;
@@ -1576,6 +1614,12 @@ template <typename T, int B>
 static int pcg_run(Solver& S, PcgDev& c, int& h_done)
 {
     STG_TRY((set_carveouts<T, B>()));
+    STG_TRY(phase_a_grid<T>(c.nrows, &c.grid_a));
+    if(c.grid_a > c.slots)
+    {
+        set_error("SpMV phase grid larger than the reduction slots");
+        return STG_ERR_INVALID;
+    }
     cudaStream_t s = S.stream;
     PcgState& P = S.pcg;
     const int grid_vec = std::max(1, std::min(div_up(c.n, PB), kSMs * 4));

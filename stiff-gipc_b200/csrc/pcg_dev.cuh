@@ -54,6 +54,7 @@ struct PcgDev
     double* scal;
     int* flags;
     int slots;
+    int grid_a;               // CTAs of the SpMV phase: its p.q partials, summed by phase B
     PcgParams prm;
     cudaGraphConditionalHandle h_while, h_if;
     int use_cond;

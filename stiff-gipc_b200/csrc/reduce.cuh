@@ -21,7 +21,9 @@ enum PostOp : int
     POST_ALPHA = 2,    // pq = total; alpha = rz / pq (breakdown check)
     POST_CHECK = 3,    // rr = total; iteration k completed; stop tests
     POST_BETA = 4,     // beta = total / rz; rz = total
-    POST_RECHECK = 5   // rr = total after residual replacement; stop test only
+    POST_RECHECK = 5,  // rr = total after residual replacement; stop test only
+    POST_CHECK_PQ = 6  // as POST_CHECK, with p.q (aux) finished by the consumer: the
+                       // breakdown test of POST_ALPHA first, alpha and pq recorded
 };
 
 enum : int
@@ -37,8 +39,21 @@ enum : int
     SS_RZ = 0, SS_RZ0 = 1, SS_PQ = 2, SS_ALPHA = 3, SS_BETA = 4, SS_RZNEW = 5, SS_RR = 6, SS_BB = 7, SS_ITER = 9
 };
 
-__device__ __forceinline__ void post_op(int op, int slot, double total, double* scal, int* flags, const PcgParams& p)
+__device__ __forceinline__ void post_op(int op, int slot, double total, double* scal, int* flags, const PcgParams& p,
+                                        double aux = 0.0)
 {
+    if(op == POST_CHECK_PQ)
+    {
+        scal[SS_PQ] = aux;
+        if(!(aux > 0.0) || !isfinite(aux))
+        {
+            flags[F_DONE] = 1;
+            flags[F_STATUS] = 5;  // STG_BREAKDOWN: no update was applied
+            return;
+        }
+        scal[SS_ALPHA] = scal[SS_RZ] / aux;
+        op = POST_CHECK;
+    }
     switch(op)
     {
         case POST_STORE: scal[slot] = total; break;
