@@ -68,7 +68,7 @@ __device__ __forceinline__ void set_conditionals(const PcgDev& c, int op)
 
 template <int BLOCK = PB>
 __device__ __forceinline__ void finish_reduction(const PcgDev& c, double v, int site, int op, int slot = 0,
-                                                 double aux = 0.0)
+                                                 double aux = 0.0, double aux2 = 0.0)
 {
     __shared__ double red[BLOCK / 32];
     __shared__ bool last;
@@ -89,24 +89,26 @@ __device__ __forceinline__ void finish_reduction(const PcgDev& c, double v, int 
     const double tot = block_sum<BLOCK>(acc, red);
     if(threadIdx.x == 0)
     {
-        post_op(op, slot, tot, c.scal, c.flags, c.prm, aux);
+        post_op(op, slot, tot, c.scal, c.flags, c.prm, aux, aux2);
         set_conditionals(c, op == POST_CHECK_PQ ? (int)POST_CHECK : op);
         *counter = 0u;
         __threadfence();
     }
 }
 
-// p.q of the SpMV phase, finished by each CTA of the consumer (phase B) from the SpMV
-// phase's per-CTA partials, in the same fixed order in every CTA (so every CTA gets the
-// same value): the SpMV phase needs no last-CTA step of its own.
-__device__ __forceinline__ double consume_pq(const PcgDev& c)
+// A reduction finished by each CTA of its consumer from the producer's per-CTA partials,
+// in the same fixed order in every CTA (so every CTA gets the same value): p.q of the SpMV
+// phase (consumed by phase B) and r.z of phase E (consumed by the next SpMV phase for beta
+// and by phase B for alpha).  The producers need no last-CTA step of their own.
+template <int BLOCK>
+__device__ __forceinline__ double consume_sum(const PcgDev& c, int site, int count)
 {
-    __shared__ double red[PB / 32];
+    __shared__ double red[BLOCK / 32];
     __shared__ double tot;
-    const double* part = c.partials + (size_t)SITE_A * c.slots;
+    const double* part = c.partials + (size_t)site * c.slots;
     double a = 0;
-    for(int t = threadIdx.x; t < c.grid_a; t += PB) a += __ldcg(part + t);
-    const double s = block_sum<PB>(a, red);
+    for(int t = threadIdx.x; t < count; t += BLOCK) a += __ldcg(part + t);
+    const double s = block_sum<BLOCK>(a, red);
     if(threadIdx.x == 0) tot = s;
     __syncthreads();
     return tot;
@@ -823,7 +825,7 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T>::MIN_CTAS) k_phase_a_tiled
     const int mine = re > rb ? (re - rb + RT - 1) / RT : 0;
     // the loads the start depends on are independent: issue them together
     const int done = __ldcg(c.flags + F_DONE);
-    const double s_iter = __ldcg(c.scal + SS_ITER), s_beta = __ldcg(c.scal + SS_BETA);
+    const double s_iter = __ldcg(c.scal + SS_ITER), rz_old = __ldcg(c.scal + SS_RZ);
     int lo = 0, hi = 0;  // producer: entry bounds of the next 32 tiles, one per lane
     if(warp == A_CW && lane < mine)
     {
@@ -832,6 +834,10 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T>::MIN_CTAS) k_phase_a_tiled
         hi = __ldg(c.frow + min(r0 + RT, re));
     }
     if(done) return;
+    // beta = rz_k / rz_(k-1): rz_k from phase E's partials, rz_(k-1) as phase B recorded it
+    // (the first iteration has p_0 = 0: beta = 0)
+    const double rz_new = consume_sum<A_THREADS>(c, SITE_E, c.grid_e);
+    const double s_beta = (long)s_iter == 0 ? 0.0 : rz_new / rz_old;
     int* meta = reinterpret_cast<int*>(asm_ + G::STAGES * G::STAGE);
     const unsigned sbase = smem_u32(asm_);
     const unsigned bar_full = smem_u32(asm_ + G::STAGES * G::STAGE + G::META);
@@ -1030,7 +1036,7 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T>::MIN_CTAS) k_phase_a_tiled
             atomicExch(c.flags + F_DONE, 1);
         }
     }
-    // p.q: this CTA's partial only; phase B finishes the sum (consume_pq)
+    // p.q: this CTA's partial only; phase B finishes the sum (consume_sum)
     __shared__ double red[A_THREADS / 32];
     const double bs = block_sum<A_THREADS>(acc, red);
     if(threadIdx.x == 0) c.partials[(size_t)SITE_A * c.slots + blockIdx.x] = bs;
@@ -1146,14 +1152,15 @@ template <typename T, int B>
 __global__ void __launch_bounds__(PB, 8) k_phase_b(PcgDev c)
 {
     if(c.flags[F_DONE]) return;
-    const double pq = consume_pq(c);
+    const double pq = consume_sum<PB>(c, SITE_A, c.grid_a);
+    const double rz = consume_sum<PB>(c, SITE_E, c.grid_e);
     double v = 0;
     if(pq > 0.0 && isfinite(pq))  // else breakdown: no update; the last CTA reports it
     {
-        const double alpha = __ldcg(c.scal + SS_RZ) / pq;
+        const double alpha = rz / pq;
         v = B > 0 ? phase_b_mas<T, (B > 0 ? B : 16)>(c, GT, GN, alpha) : phase_b_plain<T>(c, GT, GN, alpha);
     }
-    finish_reduction(c, v, SITE_B, POST_CHECK_PQ, 0, pq);
+    finish_reduction(c, v, SITE_B, POST_CHECK_PQ, 0, pq, rz);
 }
 
 // guarded: runs only when this iteration is a replacement iteration (host / plain graph),
@@ -1210,7 +1217,15 @@ __global__ void __launch_bounds__(PB, 8) k_phase_e(PcgDev c, int op)
 {
     if(c.flags[F_DONE]) return;
     const double v = B > 0 ? phase_e_mas<T>(c, GT, GN) : phase_e_plain<T>(c, GT, GN);
-    finish_reduction(c, v, op == POST_INIT_RZ ? SITE_INIT_RZ : SITE_E, op);
+    if(op == POST_INIT_RZ)
+    {
+        finish_reduction(c, v, SITE_E, POST_INIT_RZ);
+        return;
+    }
+    // r.z: this CTA's partial only; the next SpMV phase and phase B finish the sum
+    __shared__ double red[PB / 32];
+    const double bs = block_sum<PB>(v, red);
+    if(threadIdx.x == 0) c.partials[(size_t)SITE_E * c.slots + blockIdx.x] = bs;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1615,7 +1630,8 @@ static int pcg_run(Solver& S, PcgDev& c, int& h_done)
 {
     STG_TRY((set_carveouts<T, B>()));
     STG_TRY(phase_a_grid<T>(c.nrows, &c.grid_a));
-    if(c.grid_a > c.slots)
+    c.grid_e = std::max(1, std::min(div_up(c.n, PB), kSMs * 4));  // grid_vec below
+    if(c.grid_a > c.slots || c.grid_e > c.slots)
     {
         set_error("SpMV phase grid larger than the reduction slots");
         return STG_ERR_INVALID;

@@ -55,6 +55,7 @@ struct PcgDev
     int* flags;
     int slots;
     int grid_a;               // CTAs of the SpMV phase: its p.q partials, summed by phase B
+    int grid_e;               // CTAs of phase E: its r.z partials, summed by phases A and B
     PcgParams prm;
     cudaGraphConditionalHandle h_while, h_if;
     int use_cond;

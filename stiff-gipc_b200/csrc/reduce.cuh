@@ -22,8 +22,9 @@ enum PostOp : int
     POST_CHECK = 3,    // rr = total; iteration k completed; stop tests
     POST_BETA = 4,     // beta = total / rz; rz = total
     POST_RECHECK = 5,  // rr = total after residual replacement; stop test only
-    POST_CHECK_PQ = 6  // as POST_CHECK, with p.q (aux) finished by the consumer: the
-                       // breakdown test of POST_ALPHA first, alpha and pq recorded
+    POST_CHECK_PQ = 6  // as POST_CHECK, with p.q (aux) and r.z (aux2) finished by the
+                       // consumer: rz recorded, the breakdown test of POST_ALPHA first,
+                       // alpha and pq recorded
 };
 
 enum : int
@@ -40,10 +41,11 @@ enum : int
 };
 
 __device__ __forceinline__ void post_op(int op, int slot, double total, double* scal, int* flags, const PcgParams& p,
-                                        double aux = 0.0)
+                                        double aux = 0.0, double aux2 = 0.0)
 {
     if(op == POST_CHECK_PQ)
     {
+        scal[SS_RZ] = aux2;
         scal[SS_PQ] = aux;
         if(!(aux > 0.0) || !isfinite(aux))
         {
