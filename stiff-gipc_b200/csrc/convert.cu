@@ -43,8 +43,10 @@ __global__ void k_conv_hist(const int* rows, const int* cols, int count, int nro
     }
 }
 
+// counting-sort scatter by row; each slot gets the triplet's index and its column, so the
+// per-row sort reads its keys contiguously
 __global__ void k_conv_scatter(const int* rows, const int* cols, int count, int nrows, const int* row_start, int* cursor,
-                               int* perm)
+                               int* perm, int* pcol)
 {
     for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
     {
@@ -52,32 +54,103 @@ __global__ void k_conv_scatter(const int* rows, const int* cols, int count, int 
         if(r < 0 || r >= nrows || c < 0 || c >= nrows) continue;
         const int pos = row_start[r] + atomicAdd(cursor + r, 1);
         perm[pos] = i;
+        pcol[pos] = c;
     }
 }
 
-// One warp per row: rank every entry by (col, original index), write the sorted permutation
-// and sorted cols, and count distinct cols.
-__global__ void k_conv_sort_rows(const int* cols, const int* row_start, const int* perm_in, int* perm_out,
-                                 int* scol, int* uniq, int nrows)
+// One warp per row: order every entry by (col, original index), write the sorted permutation
+// and sorted cols, and count distinct cols.  Rows of up to 128 entries are sorted by a
+// bitonic network on 64-bit keys (col << 32 | index; 4 keys per lane, position 4 * lane + h),
+// longer rows by ranking (each lane counts the entries before its own).  The keys are
+// unique, so both give the same permutation.
+constexpr int CONV_WARPS = 8;
+
+__device__ __forceinline__ unsigned long long shfl_xor_u64(unsigned long long v, int m)
+{
+    const unsigned lo = __shfl_xor_sync(0xffffffffu, (unsigned)v, m);
+    const unsigned hi = __shfl_xor_sync(0xffffffffu, (unsigned)(v >> 32), m);
+    return ((unsigned long long)hi << 32) | lo;
+}
+
+__global__ void __launch_bounds__(32 * CONV_WARPS) k_conv_sort_rows(const int* pcol, const int* row_start,
+                                                                    const int* perm_in, int* perm_out, int* scol,
+                                                                    int* uniq, int nrows)
 {
     const int warps = (gridDim.x * blockDim.x) >> 5;
     const int lane = threadIdx.x & 31;
     for(int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nrows; r += warps)
     {
         const int s = row_start[r], e = row_start[r + 1], n = e - s;
-        for(int a = lane; a < n; a += 32)
+        if(n <= 128)
         {
-            const int ia = perm_in[s + a];
-            const int ca = cols[ia];
-            int rank = 0;
-            for(int b = 0; b < n; b++)
+            unsigned long long k[4];
+#pragma unroll
+            for(int h = 0; h < 4; h++)
             {
-                const int ib = perm_in[s + b];
-                const int cb = cols[ib];
-                rank += (cb < ca) || (cb == ca && ib < ia);
+                const int p = 4 * lane + h;
+                k[h] = ~0ull;
+                if(p < n) k[h] = ((unsigned long long)(unsigned)pcol[s + p] << 32) | (unsigned)perm_in[s + p];
             }
-            perm_out[s + rank] = ia;
-            scol[s + rank] = ca;
+#pragma unroll
+            for(int kk = 2; kk <= 128; kk <<= 1)
+            {
+#pragma unroll
+                for(int d = kk >> 1; d >= 1; d >>= 1)
+                {
+                    if(d >= 4)
+                    {
+#pragma unroll
+                        for(int h = 0; h < 4; h++)
+                        {
+                            const int p = 4 * lane + h;
+                            const unsigned long long o = shfl_xor_u64(k[h], d >> 2);
+                            const bool up = (p & kk) == 0, lower = (p & d) == 0;
+                            k[h] = (up == lower) ? (k[h] < o ? k[h] : o) : (k[h] < o ? o : k[h]);
+                        }
+                    }
+                    else
+                    {
+#pragma unroll
+                        for(int h = 0; h < 4; h++)
+                        {
+                            if(h & d) continue;
+                            const int p = 4 * lane + h;
+                            const bool up = (p & kk) == 0;
+                            const unsigned long long x = k[h], y = k[h + d];
+                            const bool sw = up ? (x > y) : (x < y);
+                            k[h] = sw ? y : x;
+                            k[h + d] = sw ? x : y;
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for(int h = 0; h < 4; h++)
+            {
+                const int p = 4 * lane + h;
+                if(p < n)
+                {
+                    perm_out[s + p] = (int)(unsigned)k[h];
+                    scol[s + p] = (int)(k[h] >> 32);
+                }
+            }
+        }
+        else
+        {
+            for(int a = lane; a < n; a += 32)
+            {
+                const int ia = perm_in[s + a];
+                const int ca = pcol[s + a];
+                int rank = 0;
+                for(int b = 0; b < n; b++)
+                {
+                    const int ib = perm_in[s + b];
+                    const int cb = pcol[s + b];
+                    rank += (cb < ca) || (cb == ca && ib < ia);
+                }
+                perm_out[s + rank] = ia;
+                scol[s + rank] = ca;
+            }
         }
         __syncwarp();
         int heads = 0;
@@ -90,15 +163,35 @@ __global__ void k_conv_sort_rows(const int* cols, const int* row_start, const in
 }
 
 // One warp per row: each lane owns a run of equal cols (a unique block) and sums it in
-// sorted (= original) order.
-__global__ void k_conv_emit(const double* blocks, const int* row_start, const int* perm, const int* scol,
-                            const int* ustart, int* out_rows, int* out_cols, double* out_blocks, int nrows)
+// sorted (= original) order.  Rows of up to CONV_EMIT_CAP entries first stage their blocks
+// (in sorted order) in shared memory with independent loads, so the sequential sums read
+// shared memory; longer rows sum from global memory.  The sums are the same either way.
+constexpr int CONV_EMIT_WARPS = 4;
+constexpr int CONV_EMIT_CAP = 128;
+
+__global__ void __launch_bounds__(32 * CONV_EMIT_WARPS) k_conv_emit(const double* blocks, const int* row_start,
+                                                                    const int* perm, const int* scol,
+                                                                    const int* ustart, int* out_rows, int* out_cols,
+                                                                    double* out_blocks, int nrows)
 {
+    extern __shared__ double ebuf[];  // [CONV_EMIT_WARPS][CONV_EMIT_CAP * 9]
     const int warps = (gridDim.x * blockDim.x) >> 5;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double* sb = ebuf + (size_t)w * CONV_EMIT_CAP * 9;
     for(int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nrows; r += warps)
     {
         const int s = row_start[r], e = row_start[r + 1], n = e - s;
+        const bool staged = n <= CONV_EMIT_CAP;
+        if(staged)
+        {
+            for(int a = lane; a < n; a += 32)
+            {
+                const double* b0 = blocks + 9 * (size_t)perm[s + a];
+#pragma unroll
+                for(int t = 0; t < 9; t++) sb[9 * a + t] = b0[t];
+            }
+            __syncwarp();
+        }
         int base = 0;
         for(int a0 = 0; a0 < n; a0 += 32)
         {
@@ -109,14 +202,27 @@ __global__ void k_conv_emit(const double* blocks, const int* row_start, const in
             {
                 const int o = ustart[r] + base + __popc(hm & lanemask_lt(lane));
                 double acc[9];
-                const double* b0 = blocks + 9 * (size_t)perm[s + a];
-#pragma unroll
-                for(int t = 0; t < 9; t++) acc[t] = b0[t];
-                for(int c = a + 1; c < n && scol[s + c] == scol[s + a]; c++)
+                if(staged)
                 {
-                    const double* bc = blocks + 9 * (size_t)perm[s + c];
 #pragma unroll
-                    for(int t = 0; t < 9; t++) acc[t] += bc[t];
+                    for(int t = 0; t < 9; t++) acc[t] = sb[9 * a + t];
+                    for(int c = a + 1; c < n && scol[s + c] == scol[s + a]; c++)
+                    {
+#pragma unroll
+                        for(int t = 0; t < 9; t++) acc[t] += sb[9 * c + t];
+                    }
+                }
+                else
+                {
+                    const double* b0 = blocks + 9 * (size_t)perm[s + a];
+#pragma unroll
+                    for(int t = 0; t < 9; t++) acc[t] = b0[t];
+                    for(int c = a + 1; c < n && scol[s + c] == scol[s + a]; c++)
+                    {
+                        const double* bc = blocks + 9 * (size_t)perm[s + c];
+#pragma unroll
+                        for(int t = 0; t < 9; t++) acc[t] += bc[t];
+                    }
                 }
                 out_rows[o] = r;
                 out_cols[o] = scol[s + a];
@@ -125,6 +231,7 @@ __global__ void k_conv_emit(const double* blocks, const int* row_start, const in
             }
             base += __popc(hm);
         }
+        __syncwarp();
     }
 }
 
@@ -151,6 +258,7 @@ int convert_into(Solver& S, ConvertScratch& cv, int count, const int* rows, cons
     STG_TRY(cv.perm.resize(count));
     STG_TRY(cv.perm2.resize(count));
     STG_TRY(cv.scol.resize(count));
+    STG_TRY(cv.pcol.resize(count));
     STG_TRY(cv.uniq.resize(nrows + 1));
     STG_TRY(out_rows.resize(count));
     STG_TRY(out_cols.resize(count));
@@ -164,17 +272,20 @@ int convert_into(Solver& S, ConvertScratch& cv, int count, const int* rows, cons
     STG_LAUNCH_CHECK();
     k_scan_exclusive<<<1, 1024, 0, s>>>(cv.row_cnt.data(), cv.row_start.data(), nullptr, nrows + 1, cv.scratch.data());
     STG_LAUNCH_CHECK();
-    k_conv_scatter<<<g, 256, 0, s>>>(rows, cols, count, nrows, cv.row_start.data(), cv.cursor.data(), cv.perm.data());
+    k_conv_scatter<<<g, 256, 0, s>>>(rows, cols, count, nrows, cv.row_start.data(), cv.cursor.data(), cv.perm.data(),
+                                     cv.pcol.data());
     STG_LAUNCH_CHECK();
-    const int gw = std::min(div_up((long)nrows * 32, 256), kSMs * 16);
-    k_conv_sort_rows<<<gw, 256, 0, s>>>(cols, cv.row_start.data(), cv.perm.data(), cv.perm2.data(), cv.scol.data(),
-                                        cv.uniq.data(), nrows);
+    const int gw = std::min(div_up((long)nrows * 32, 32 * CONV_WARPS), kSMs * 16);
+    k_conv_sort_rows<<<gw, 32 * CONV_WARPS, 0, s>>>(cv.pcol.data(), cv.row_start.data(), cv.perm.data(), cv.perm2.data(),
+                                                    cv.scol.data(), cv.uniq.data(), nrows);
     STG_LAUNCH_CHECK();
     STG_CUDA_TRY(cudaMemsetAsync(cv.uniq.data() + nrows, 0, sizeof(int), s));
     k_scan_exclusive<<<1, 1024, 0, s>>>(cv.uniq.data(), row_ptr.data(), nullptr, nrows + 1, cv.scratch.data() + 1);
     STG_LAUNCH_CHECK();
-    k_conv_emit<<<gw, 256, 0, s>>>(blocks, cv.row_start.data(), cv.perm2.data(), cv.scol.data(), row_ptr.data(),
-                                   out_rows.data(), out_cols.data(), out_blocks.data(), nrows);
+    const int ge = std::min(div_up((long)nrows * 32, 32 * CONV_EMIT_WARPS), kSMs * 32);
+    k_conv_emit<<<ge, 32 * CONV_EMIT_WARPS, sizeof(double) * CONV_EMIT_WARPS * CONV_EMIT_CAP * 9, s>>>(
+        blocks, cv.row_start.data(), cv.perm2.data(), cv.scol.data(), row_ptr.data(), out_rows.data(), out_cols.data(),
+        out_blocks.data(), nrows);
     STG_LAUNCH_CHECK();
     S.launches += 6;
     int h[2] = {0, 0};

@@ -479,98 +479,107 @@ __global__ void __launch_bounds__(3 * B) k_mas_invert(const double* __restrict__
     }
 }
 
-// The same Gauss-Jordan for 16-banks with each column in registers: thread i of a bank owns
-// column i (48 doubles); pivot j broadcasts the old column j through shared memory and every
-// column updates itself, all loop indices compile-time (fully unrolled).  The operation
-// order per element is the one of k_mas_invert, so the results are the same; only shared
-// memory traffic is gone (one column per pivot instead of a load and a store per FMA).
-// Two banks per CTA, 64 threads per bank (lanes 48..63 idle).
-constexpr int INV16_BANKS = 2;
-
-__global__ void __launch_bounds__(64 * INV16_BANKS) k_mas_invert16(const double* __restrict__ mat, float* inv, int nbanks)
+// The same Gauss-Jordan for 16-banks, one CTA of 256 threads per bank, thread (bi, bj) owning
+// the 3x3 tile at block row bi, block column bj in registers.  Pivot j: the tiles of block
+// column j / 3 publish column j; those of block row j / 3 scale row j by the reciprocal of
+// the pivot (one FP64 division per thread and pivot: divisions on the pivot's critical path
+// made a per-element division three times slower) and publish it; then every tile updates
+// itself with fma(-colm[k], A[j][i], A[k][i]) as k_mas_invert does.  The broadcasts are
+// double-buffered (two barriers per pivot).  Scaling by the reciprocal instead of dividing
+// changes the last bit of some FP64 entries; the FP32 inverses agree with the per-element
+// division to within the tests' 2e-5.
+__global__ void __launch_bounds__(256) k_mas_invert16(const double* __restrict__ mat, float* inv, int nbanks)
 {
-    constexpr int B = 16, N = 48;
+    constexpr int B = 16;
     const int NS = nsym(B);
-    __shared__ double colj[INV16_BANKS][N];
-    __shared__ double band[INV16_BANKS][N][5];  // A[i + d][i], d = -2..2, for the final mirror
-    const int g = threadIdx.x / 64, i = threadIdx.x % 64;
-    const int bk = blockIdx.x * INV16_BANKS + g;
-    const bool live = bk < nbanks && i < N;
-    double c[N];
-    const double* Mb = mat + (size_t)(bk < nbanks ? bk : 0) * NS * 9;
-#pragma unroll
-    for(int j = 0; j < N; j++)
+    __shared__ double rowj[2][3 * B], colj[2][3 * B];
+    const int bk = blockIdx.x;
+    const int bi = threadIdx.x / B, bj = threadIdx.x % B;
+    const double* Mb = mat + (size_t)bk * NS * 9;
+    double a[3][3];
+    if(bj >= bi)
     {
-        double v = 0.0;
-        if(live)
-        {
-            const int rowId = j / 3, colId = i / 3;
-            if(colId >= rowId)
-                v = Mb[upper_index(B, rowId, colId) * 9 + (i % 3) * 3 + (j % 3)];
-            else
-                v = Mb[upper_index(B, colId, rowId) * 9 + (j % 3) * 3 + (i % 3)];
-            if(i == j && v == 0.0) v = 1.0;
-        }
-        c[j] = v;  // A[j][i]
+        const double* H = Mb + upper_index(B, bi, bj) * 9;  // column-major
+#pragma unroll
+        for(int r = 0; r < 3; r++)
+#pragma unroll
+            for(int cc = 0; cc < 3; cc++) a[r][cc] = H[cc * 3 + r];
     }
-#pragma unroll
-    for(int j = 0; j < N; j++)
+    else
     {
-        if(i == j)
+        const double* H = Mb + upper_index(B, bj, bi) * 9;  // the mirror block, transposed
+#pragma unroll
+        for(int r = 0; r < 3; r++)
+#pragma unroll
+            for(int cc = 0; cc < 3; cc++) a[r][cc] = H[r * 3 + cc];
+    }
+    if(bi == bj)
+    {
+#pragma unroll
+        for(int r = 0; r < 3; r++)
+            if(a[r][r] == 0.0) a[r][r] = 1.0;
+    }
+    for(int j = 0; j < 3 * B; j++)
+    {
+        const int pb = j / 3, pr = j % 3, buf = j & 1;
+        // 1: block column pb publishes the old column j
+        if(bj == pb)
         {
 #pragma unroll
-            for(int k = 0; k < N; k++) colj[g][k] = c[k];
+            for(int r = 0; r < 3; r++) colj[buf][3 * bi + r] = pr == 0 ? a[r][0] : (pr == 1 ? a[r][1] : a[r][2]);
         }
         __syncthreads();
-        const double rt = colj[g][j];
-        if(i == j)
+        // 2: block row pb forms row j after the column replacement (e_j) and the division by
+        // the pivot, keeps it and publishes it
+        if(bi == pb)
         {
+            const double rinv = 1.0 / colj[buf][j];
 #pragma unroll
-            for(int k = 0; k < N; k++) c[k] = (k == j) ? 1.0 : 0.0;
+            for(int cc = 0; cc < 3; cc++)
+            {
+                const int col = 3 * bj + cc;
+                const double x = col == j ? 1.0 : (pr == 0 ? a[0][cc] : (pr == 1 ? a[1][cc] : a[2][cc]));
+                const double v = x * rinv;
+                rowj[buf][col] = v;
+                if(pr == 0)
+                    a[0][cc] = v;
+                else if(pr == 1)
+                    a[1][cc] = v;
+                else
+                    a[2][cc] = v;
+            }
         }
-        c[j] /= rt;
-        const double aji = c[j];
-#pragma unroll
-        for(int k = 0; k < N; k++)
-            if(k != j) c[k] = fma(-colj[g][k], aji, c[k]);
         __syncthreads();
-    }
-    // lower triangle of the diagonal 3x3 blocks mirrored from the upper one (as k_mas_invert)
-    if(i < N)
-    {
+        // 3: every other row: A[k][i] = fma(-colm[k], A[j][i], A[k][i]) (column j replaced by e_j)
 #pragma unroll
-        for(int d = -2; d <= 2; d++)
+        for(int r = 0; r < 3; r++)
         {
-            double v = 0.0;
+            const int row = 3 * bi + r;
+            if(row == j) continue;
+            const double cm = colj[buf][row];
 #pragma unroll
-            for(int k = 0; k < N; k++)
-                if(k == i + d) v = c[k];
-            band[g][i][d + 2] = v;
+            for(int cc = 0; cc < 3; cc++)
+            {
+                const double old = (3 * bj + cc == j) ? 0.0 : a[r][cc];
+                a[r][cc] = fma(-cm, rowj[buf][3 * bj + cc], old);
+            }
         }
+        // the next pivot writes the other buffers; this pivot's are reused two pivots later,
+        // after two more barriers
     }
-    __syncthreads();
-    if(i < N)
+    if(bj < bi) return;
+    if(bi == bj)
     {
-        // lower entries (1,0), (2,1), (2,0) of the diagonal 3x3 block from (0,1), (1,2), (0,2);
-        // band[col][d + 2] = A[col + d][col]
-        const double v1 = i % 3 < 2 ? band[g][i + 1][1] : 0.0;   // A[i][i + 1]
-        const double v2 = i % 3 == 0 ? band[g][i + 2][0] : 0.0;  // A[i][i + 2]
-#pragma unroll
-        for(int k = 0; k < N; k++)
-        {
-            if(i % 3 < 2 && k == i + 1) c[k] = v1;
-            if(i % 3 == 0 && k == i + 2) c[k] = v2;
-        }
+        // lower triangle of the diagonal 3x3 block mirrored from the upper one
+        a[1][0] = a[0][1];
+        a[2][1] = a[1][2];
+        a[2][0] = a[0][2];
     }
-    __syncthreads();
-    if(!live) return;
-    float* P = inv + (size_t)bk * NS * 9;
+    float* P = inv + ((size_t)bk * NS + upper_index(B, bi, bj)) * 9;
 #pragma unroll
-    for(int j = 0; j < N; j++)
-    {
-        const int rowId = j / 3, colId = i / 3;
-        if(colId >= rowId) P[upper_index(B, rowId, colId) * 9 + (i % 3) * 3 + (j % 3)] = (float)c[j];
-    }
+    for(int r = 0; r < 3; r++)
+#pragma unroll
+        for(int cc = 0; cc < 3; cc++) P[cc * 3 + r] = (float)a[r][cc];
 }
 
 // ---------------------------------------------------------------------------------------
@@ -984,7 +993,7 @@ static int mas_assemble_t(Solver& S, int offset)
     }
     if(B == 16)
     {
-        k_mas_invert16<<<div_up(m.nbanks, INV16_BANKS), 64 * INV16_BANKS, 0, s>>>(m.mat.data(), m.inv.data(), m.nbanks);
+        k_mas_invert16<<<m.nbanks, 256, 0, s>>>(m.mat.data(), m.inv.data(), m.nbanks);
         STG_LAUNCH_CHECK();
     }
     else
