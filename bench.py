@@ -19,8 +19,8 @@ FP64 true residual reported).
            x copied back, every step.
 
 ``--impl reference`` times the CPU oracle port (the reference's MAS-PCG restated in C,
-oracle/) on the host cores: the reference itself is GPU-only and cannot be built here
-(it needs Eigen 3.4).
+oracle/) on all host cores (OpenMP): the reference itself is GPU-only and cannot be built
+here (it needs Eigen 3.4).
 """
 from __future__ import annotations
 
@@ -139,55 +139,49 @@ def profiled_traffic(workload):
     return None
 
 
-def cpu_baseline(sysm, budget_s, bank):
-    """The oracle's MAS-PCG (single thread C port) on a bounded sample: convert + MAS build +
-    assembly once, then PCG iterations until the relative residual reaches 1e-4 or the time
-    budget ends; the per-solve time is set-up + per-iteration time x the iterations the full
-    solve needs (measured if it finished, else the GPU FP64 path's count)."""
+def cpu_solve_ms(sysm, bank, budget_s, fallback_iters=None):
+    """One MAS-PCG Newton solve of the oracle (the reference's algorithm restated in C) on all
+    host threads: convert + MAS build + assembly (serial C), then the PCG loop with OpenMP
+    (full-symmetric CSR SpMV, bank solves and vector updates in parallel) for up to
+    `budget_s` seconds.  Returns (ms per solve, iterations used, threads, sample text)."""
     from oracle import oracle as orc
+    orc.build()
     t0 = time.perf_counter()
     r, c, b = orc.convert(sysm.rows, sysm.cols, sysm.blocks)
-    m = orc.Mas(bank, sysm.num_verts, sysm.neighbor_start, sysm.neighbor_num, sysm.neighbor_list, *sysm.slot_maps(bank))
+    m = orc.Mas(bank, sysm.num_verts, sysm.neighbor_start, sysm.neighbor_num, sysm.neighbor_list,
+                *sysm.slot_maps(bank))
     m.build()
     m.assemble(r, c, b)
     t_setup = time.perf_counter() - t0
-    return orc, (r, c, b), m, t_setup
+    _, k, t_csr, t_iter, done, threads, rel = orc.pcg_timed_mt(r, c, b, sysm.b, m, tol=1e-4, budget_s=budget_s)
+    n_it = k if done else (fallback_iters or orc.extrapolated_iterations({"iterations": k, "rel_residual": rel}))
+    ms = (t_setup + t_csr + t_iter * n_it) * 1e3
+    sample = (f"oracle MAS-PCG (bank {bank}): convert + MAS build/assembly ({t_setup:.1f} s, serial) + "
+              f"{k} PCG iterations on {threads} threads ({'converged' if done else 'time-bounded'}), "
+              f"per-iteration time x {n_it} iterations")
+    return ms, n_it, threads, sample
 
 
 def run_reference(args):
-    """--impl reference: the CPU oracle port of the reference's MAS-PCG on the host cores."""
+    """--impl reference: the CPU oracle port of the reference's MAS-PCG on all host cores."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     sysm, desc = load_system(args.workload)
-    from oracle import oracle as orc
-    orc.build()
-    cores = 1
-    times, iters_seen = [], []
     budget = max(2.0, 150.0 / max(1, args.steps + args.warmup))
+    times, threads, sample = [], 1, ""
     for step in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        r, c, b = orc.convert(sysm.rows, sysm.cols, sysm.blocks)
-        m = orc.Mas(args.bank, sysm.num_verts, sysm.neighbor_start, sysm.neighbor_num, sysm.neighbor_list,
-                    *sysm.slot_maps(args.bank))
-        m.build()
-        m.assemble(r, c, b)
-        t_setup = time.perf_counter() - t0
-        x, st, t_iter, done = orc.pcg_timed(r, c, b, sysm.b, mas=m, tol=1e-4, stop_rule="relative_residual",
-                                            budget_s=budget)
-        per_solve = t_setup + t_iter * (st["iterations"] if done else orc.extrapolated_iterations(st))
+        ms, n_it, threads, sample = cpu_solve_ms(sysm, args.bank, budget)
         if step >= args.warmup:
-            times.append(per_solve * 1e3)
-            iters_seen.append(st["iterations"])
+            times.append(ms)
     ms = statistics.mean(times)
     line = {"metric": METRIC, "value": ms, "unit": "ms", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": {"workload": args.workload, "desc": desc, "dof": sysm.n, "bank": args.bank,
                        "stop": "||b-Ax||/||b|| <= 1e-4"},
-            "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores, "kind": "port",
-                             "sample": f"per step: convert + MAS build/assembly + up to {budget:.0f} s of PCG "
-                                       f"iterations, scaled to a full solve ({iters_seen[-1]} iterations seen)"},
+            "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "port",
+                             "sample": "per step: " + sample},
             "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -411,21 +405,9 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        from oracle import oracle as orc
-        orc.build()
-        t0 = time.perf_counter()
-        r, c, bb = orc.convert(sysm.rows, sysm.cols, sysm.blocks)
-        m = orc.Mas(args.bank, sysm.num_verts, sysm.neighbor_start, sysm.neighbor_num, sysm.neighbor_list, pm, rm)
-        m.build()
-        m.assemble(r, c, bb)
-        t_setup = time.perf_counter() - t0
-        _, st_c, t_iter, done = orc.pcg_timed(r, c, bb, sysm.b, mas=m, tol=1e-4, stop_rule="relative_residual",
-                                             budget_s=args.cpu_budget_s)
-        n_it = st_c["iterations"] if done else st_plain["iterations"]
-        cpu = {"value": (t_setup + t_iter * n_it) * 1e3, "unit": "ms", "cores": 1, "kind": "port",
-               "sample": f"oracle MAS-PCG (bank {args.bank}): convert + MAS build/assembly ({t_setup:.1f} s) + "
-                         f"{st_c['iterations']} PCG iterations ({'converged' if done else 'time-bounded'}), "
-                         f"per-iteration time x {n_it} iterations"}
+        ms_cpu, _, threads, sample = cpu_solve_ms(sysm, args.bank, args.cpu_budget_s,
+                                                  fallback_iters=st_plain["iterations"])
+        cpu = {"value": ms_cpu, "unit": "ms", "cores": threads, "kind": "port", "sample": sample}
 
     if rank == 0:
         line = {

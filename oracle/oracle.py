@@ -71,6 +71,10 @@ def lib():
                                  C.c_int, C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_double,
                                  C.POINTER(PcgStats), C.POINTER(C.c_double), C.POINTER(C.c_int)]
         L.orc_pcg_ex.restype = C.c_int
+        L.orc_pcg_mt.argtypes = [_i32p, _i32p, _f64p, C.c_int, C.c_int, _f64p, _f64p, C.c_void_p, C.c_double,
+                                 C.c_double, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                 C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.orc_pcg_mt.restype = C.c_int
         _lib = L
     return _lib
 
@@ -190,6 +194,21 @@ def pcg_timed(rows, cols, blocks, b, mas: Mas | None = None, fem_offset=0, use_d
                  0 if stop_rule == "reference" else 1, float(budget_s), C.byref(st), C.byref(t_iter), C.byref(done))
     stats = dict(iterations=st.iterations, rz0=st.rz0, rz_final=st.rz_final, rel_residual=st.rel_residual)
     return x, stats, t_iter.value, bool(done.value)
+
+
+def pcg_timed_mt(rows, cols, blocks, b, mas: Mas, tol=1e-4, max_iter_ratio=0.3, budget_s=0.0):
+    """The MAS-PCG recurrence on all host threads (OpenMP; stop rule ||r|| <= tol ||b||),
+    for timing only.  Returns (x, iterations, seconds of set-up, seconds per iteration,
+    finished, threads, last relative residual)."""
+    n = b.size
+    x = np.zeros(n)
+    t_setup, t_iter, rel = C.c_double(), C.c_double(), C.c_double()
+    done, threads = C.c_int(), C.c_int()
+    k = lib().orc_pcg_mt(np.ascontiguousarray(rows, np.int32), np.ascontiguousarray(cols, np.int32),
+                         np.ascontiguousarray(blocks, np.float64).reshape(-1), rows.size, n,
+                         np.ascontiguousarray(b, np.float64), x, mas.h, tol, max_iter_ratio, float(budget_s),
+                         C.byref(t_setup), C.byref(t_iter), C.byref(done), C.byref(threads), C.byref(rel))
+    return x, int(k), t_setup.value, t_iter.value, bool(done.value), threads.value, rel.value
 
 
 def extrapolated_iterations(stats, target=1e-4):

@@ -903,3 +903,206 @@ int orc_pcg_ex(const int* rows, const int* cols, const double* blocks, int nnzb,
     free(r); free(z); free(p); free(Ap); free(s.diag_inv);
     return (int)k;
 }
+
+/* ------------------------------------------------------------------------------------ */
+/* Multithreaded timing variant (CPU baseline only)                                      */
+/* ------------------------------------------------------------------------------------ */
+/* The same MAS-PCG recurrence as orc_pcg_ex (stop rule 1: ||r|| <= tol ||b||), spread over
+ * the host's threads with OpenMP: the SpMV on a full symmetric CSR copy built once (rows in
+ * parallel), the bank solves of the MAS apply in parallel over banks, the prolongation over
+ * vertices, and the vector updates and dot products over entries.  The restriction to the
+ * coarse levels stays serial (it accumulates into shared coarse nodes).  Used to time the
+ * reference algorithm on all host cores; the serial functions above are the checker. */
+#include <omp.h>
+
+typedef struct
+{
+    int n3;          /* block rows */
+    int* ptr;        /* [n3 + 1] */
+    int* col;
+    double* val;     /* 9 per entry, column-major */
+} orc_csr;
+
+static void csr_build(orc_csr* A, int nnzb, const int* rows, const int* cols, const double* blocks, int n3)
+{
+    A->n3 = n3;
+    A->ptr = (int*)calloc((size_t)n3 + 1, sizeof(int));
+    for(int k = 0; k < nnzb; k++)
+    {
+        A->ptr[rows[k] + 1]++;
+        if(rows[k] != cols[k]) A->ptr[cols[k] + 1]++;
+    }
+    for(int i = 0; i < n3; i++) A->ptr[i + 1] += A->ptr[i];
+    const int nnz = A->ptr[n3];
+    A->col = (int*)malloc(sizeof(int) * (size_t)(nnz > 0 ? nnz : 1));
+    A->val = (double*)malloc(sizeof(double) * 9 * (size_t)(nnz > 0 ? nnz : 1));
+    int* cur = (int*)malloc(sizeof(int) * (size_t)n3);
+    memcpy(cur, A->ptr, sizeof(int) * (size_t)n3);
+    for(int k = 0; k < nnzb; k++)
+    {
+        const int i = rows[k], j = cols[k];
+        const double* H = blocks + 9 * (size_t)k;
+        int e = cur[i]++;
+        A->col[e] = j;
+        memcpy(A->val + 9 * (size_t)e, H, 9 * sizeof(double));
+        if(i != j)
+        {
+            e = cur[j]++;
+            A->col[e] = i;
+            for(int r = 0; r < 3; r++)
+                for(int c = 0; c < 3; c++) A->val[9 * (size_t)e + c * 3 + r] = bget(H, c, r);  /* H^T */
+        }
+    }
+    free(cur);
+}
+
+static void csr_spmv(const orc_csr* A, const double* x, double* y)
+{
+#pragma omp parallel for schedule(static)
+    for(int i = 0; i < A->n3; i++)
+    {
+        double s0 = 0, s1 = 0, s2 = 0;
+        for(int e = A->ptr[i]; e < A->ptr[i + 1]; e++)
+        {
+            const double* H = A->val + 9 * (size_t)e;
+            const double* xj = x + 3 * (size_t)A->col[e];
+            s0 += H[0] * xj[0] + H[3] * xj[1] + H[6] * xj[2];
+            s1 += H[1] * xj[0] + H[4] * xj[1] + H[7] * xj[2];
+            s2 += H[2] * xj[0] + H[5] * xj[1] + H[8] * xj[2];
+        }
+        y[3 * i] = s0;
+        y[3 * i + 1] = s1;
+        y[3 * i + 2] = s2;
+    }
+}
+
+static void mas_apply_mt(const orc_mas* m, const double* r, double* z, float* R, float* Zc)
+{
+    const int B = m->bank, V = m->V, M = m->M, L = m->L, T = m->total_clusters;
+    memset(R, 0, sizeof(float) * 3 * (size_t)T);
+    for(int s = 0; s < M; s++)
+    {
+        int v = m->part_map[s];
+        if(v < 0) continue;
+        float rv[3] = {(float)r[3 * v], (float)r[3 * v + 1], (float)r[3 * v + 2]};
+        for(int c = 0; c < 3; c++) R[3 * s + c] = rv[c];
+        int id = v;
+        for(int level = 1; level < L; level++)
+        {
+            id = m->going_next[id];
+            for(int c = 0; c < 3; c++) R[3 * (size_t)id + c] += rv[c];
+        }
+    }
+    const int NS = nsym(B);
+#pragma omp parallel for schedule(static)
+    for(int bk = 0; bk < T / B; bk++)
+    {
+        const float* P = m->inv + (size_t)bk * NS * 9;
+        for(int a = 0; a < B; a++)
+        {
+            float acc[3] = {0, 0, 0};
+            for(int c = 0; c < B; c++)
+            {
+                const float* rc = R + 3 * ((size_t)bk * B + c);
+                if(c >= a)
+                {
+                    const float* Pb = P + (size_t)upper_index(B, a, c) * 9;
+                    for(int i = 0; i < 3; i++) acc[i] += Pb[i] * rc[0] + Pb[3 + i] * rc[1] + Pb[6 + i] * rc[2];
+                }
+                else
+                {
+                    const float* Pb = P + (size_t)upper_index(B, c, a) * 9;
+                    for(int i = 0; i < 3; i++) acc[i] += Pb[i * 3] * rc[0] + Pb[i * 3 + 1] * rc[1] + Pb[i * 3 + 2] * rc[2];
+                }
+            }
+            for(int i = 0; i < 3; i++) Zc[3 * ((size_t)bk * B + a) + i] = acc[i];
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for(int v = 0; v < V; v++)
+    {
+        int s = m->real_map[v];
+        float cz[3] = {Zc[3 * (size_t)s], Zc[3 * (size_t)s + 1], Zc[3 * (size_t)s + 2]};
+        for(int l = 1; l < L; l++)
+        {
+            int now = m->coarse_table[(size_t)v * (L - 1) + l - 1];
+            for(int c = 0; c < 3; c++) cz[c] += Zc[3 * (size_t)now + c];
+        }
+        for(int c = 0; c < 3; c++) z[3 * v + c] = (double)cz[c];
+    }
+}
+
+static double dot_mt(const double* a, const double* b, int n)
+{
+    double s = 0;
+#pragma omp parallel for schedule(static) reduction(+ : s)
+    for(int i = 0; i < n; i++) s += a[i] * b[i];
+    return s;
+}
+
+/* MAS-PCG (FEM-only system, MAS over the whole range) with all host threads; returns the
+ * iterations, *t_setup the seconds of the CSR build, *t_iter the seconds per iteration,
+ * *threads the OpenMP thread count, *rel the last ||r|| / ||b||.  The loop stops at ||r|| <= tol ||b||, max_iter or
+ * after budget_s seconds (*done = 0). */
+int orc_pcg_mt(const int* rows, const int* cols, const double* blocks, int nnzb, int n, const double* b, double* x,
+               const orc_mas* mas, double tol, double max_iter_ratio, double budget_s, double* t_setup,
+               double* t_iter, int* done, int* threads, double* rel)
+{
+    const double ts = now_s();
+    orc_csr A;
+    csr_build(&A, nnzb, rows, cols, blocks, n / 3);
+    *t_setup = now_s() - ts;
+    *threads = omp_get_max_threads();
+    double* r = (double*)malloc(sizeof(double) * n);
+    double* z = (double*)malloc(sizeof(double) * n);
+    double* p = (double*)malloc(sizeof(double) * n);
+    double* Ap = (double*)malloc(sizeof(double) * n);
+    float* R = (float*)malloc(sizeof(float) * 3 * (size_t)mas->total_clusters);
+    float* Zc = (float*)malloc(sizeof(float) * 3 * (size_t)mas->total_clusters);
+    const long max_iter = (long)(max_iter_ratio * (double)n);
+#pragma omp parallel for schedule(static)
+    for(int i = 0; i < n; i++)
+    {
+        x[i] = 0;
+        r[i] = b[i];
+    }
+    mas_apply_mt(mas, r, z, R, Zc);
+    double rz = dot_mt(r, z, n);
+    memcpy(p, z, sizeof(double) * n);
+    const double bb = dot_mt(b, b, n);
+    const double t0 = now_s();
+    long k, counted = 0;
+    int finished = 0;
+    for(k = 1; k < max_iter; ++k)
+    {
+        csr_spmv(&A, p, Ap);
+        const double alpha = rz / dot_mt(p, Ap, n);
+#pragma omp parallel for schedule(static)
+        for(int i = 0; i < n; i++)
+        {
+            x[i] += alpha * p[i];
+            r[i] -= alpha * Ap[i];
+        }
+        counted = k;
+        const double rr = dot_mt(r, r, n);
+        *rel = bb > 0 ? sqrt(rr / bb) : 0.0;
+        if(rr <= tol * tol * bb)
+        {
+            finished = 1;
+            break;
+        }
+        if(budget_s > 0 && now_s() - t0 > budget_s) break;
+        mas_apply_mt(mas, r, z, R, Zc);
+        const double rz_new = dot_mt(r, z, n);
+        const double beta = rz_new / rz;
+#pragma omp parallel for schedule(static)
+        for(int i = 0; i < n; i++) p[i] = z[i] + beta * p[i];
+        rz = rz_new;
+    }
+    if(k >= max_iter) finished = 1;
+    *t_iter = counted > 0 ? (now_s() - t0) / (double)counted : 0.0;
+    *done = finished;
+    free(r); free(z); free(p); free(Ap); free(R); free(Zc);
+    free(A.ptr); free(A.col); free(A.val);
+    return (int)k;
+}

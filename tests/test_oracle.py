@@ -187,3 +187,20 @@ def test_pcg_reference_stop_rule_and_max_iter():
     # a tiny max_iter_ratio stops at max_iter = (long)(ratio * n)
     x, st = orc.pcg(r, c, b, s.b, use_diag=True, max_iter_ratio=3.0 / s.n)
     assert st["iterations"] == 3
+
+
+def test_threaded_timing_pcg_matches_serial():
+    """The OpenMP timing variant (CPU baseline) follows the same recurrence: same iteration
+    count and the same solution up to summation order."""
+    from oracle import oracle as orc
+    s = cube_system(8)
+    r, c, b = orc.convert(s.rows, s.cols, s.blocks)
+    m = orc.Mas(16, s.num_verts, s.neighbor_start, s.neighbor_num, s.neighbor_list, *s.slot_maps(16))
+    m.build()
+    m.assemble(r, c, b)
+    x1, st1, _, done1 = orc.pcg_timed(r, c, b, s.b, mas=m, tol=1e-6, stop_rule="relative_residual")
+    x2, k2, _, _, done2, threads, rel = orc.pcg_timed_mt(r, c, b, s.b, m, tol=1e-6)
+    assert done1 and done2 and threads >= 1
+    assert abs(k2 - st1["iterations"]) <= 1
+    assert np.linalg.norm(x2 - x1) <= 1e-6 * np.linalg.norm(x1)
+    assert rel <= 1e-6
