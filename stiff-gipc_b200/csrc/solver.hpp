@@ -93,6 +93,9 @@ struct PcgState
     DBuf<unsigned> bar;            // persistent grid barrier
     DBuf<unsigned char> flush;     // 256 MiB written between timed SpMV launches (L2 flush)
     cudaGraphExec_t graph = nullptr;
+    PcgDev graph_key{};            // parameter block of the captured graph (handles zeroed)
+    PcgDev graph_dev{};            // the same with the graph's conditional handles
+    int graph_variant = 0;         // element size * 1000 + bank size of the captured kernels
 };
 
 // device scalar slots

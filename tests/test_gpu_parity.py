@@ -278,6 +278,38 @@ def test_solve_linear_system_end_to_end(dev, bank):
     assert np.linalg.norm(gls.x.cpu().numpy() - xe) <= 1e-4 * np.linalg.norm(xe)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_solve_with_contacts_end_to_end(dev, precision):
+    """The whole solve with sign-encoded contact pairs of all seven encodings: they join the
+    MAS in-bank connectivity (collision_connection) and so change the preconditioner; the
+    GPU hierarchy and solve follow the oracle's."""
+    from oracle import oracle as orc
+    from stgipc import PCGSolverConfig, Solver
+    s = cube_system(16)
+    cp = random_contacts(s.num_verts, 400, seed=17)
+    r, c, bl = _converted(s)
+    om = orc.Mas(16, s.num_verts, s.neighbor_start, s.neighbor_num, s.neighbor_list, *s.slot_maps(16))
+    om.build(cp)
+    om.assemble(r, c, bl)
+    xe, st_e = orc.pcg(r, c, bl, s.b, mas=om)
+    om0 = orc.Mas(16, s.num_verts, s.neighbor_start, s.neighbor_num, s.neighbor_list, *s.slot_maps(16))
+    om0.build()
+    assert om.total != om0.total  # the contacts do change the hierarchy
+    solver = Solver(PCGSolverConfig(precision=precision))
+    solver.mas_init(s.num_verts, s.neighbor_start, s.neighbor_num, s.neighbor_list, *s.slot_maps(16))
+    X = _t(np.zeros(s.n), dev)
+    st = solver.solve_linear_system(_t(s.rows, dev), _t(s.cols, dev), _t(s.blocks.reshape(-1), dev), _t(s.b, dev), X,
+                                    contacts=_t(cp, dev))
+    assert st["total_clusters"] == om.total
+    xg = X.cpu().numpy()
+    if precision == "fp64":
+        assert abs(st["iterations"] - st_e["iterations"]) <= 2
+        assert np.linalg.norm(xg - xe) <= 1e-4 * np.linalg.norm(xe)
+    else:
+        assert abs(st["iterations"] - st_e["iterations"]) <= 4
+        assert np.linalg.norm(xg - xe) <= 1e-3 * np.linalg.norm(xe)
+
+
 def test_fp32_mode_relative_residual(dev):
     """FP32 SpMV/MAS storage, FP64 dots + residual replacement: FP64 residual <= 1e-4."""
     from oracle import oracle as orc
