@@ -65,7 +65,8 @@ typedef struct stg_config
     int refine_interval;    /* FP32 mode: recompute r = b - A x in FP64 every k iters    */
     int loop_mode;          /* STG_LOOP_HOST / STG_LOOP_GRAPH / STG_LOOP_PERSISTENT      */
     int graph_batch;        /* iterations per captured graph launch (STG_LOOP_GRAPH)     */
-    int learned;            /* 1: learned coarse correction inside flexible PCG          */
+    int learned;            /* reserved for a learned coarse correction inside a flexible
+                               PCG; not available in this build: must be 0               */
     void* stream;           /* cudaStream_t (NULL = legacy default stream)               */
 } stg_config;
 
@@ -85,8 +86,8 @@ typedef struct stg_stats
     int levels;             /* MAS levelnum                                          */
     int total_clusters;     /* MAS totalNumberClusters                               */
     int replacements;       /* FP64 residual replacements (FP32 mode)                */
-    int learned_accepted;   /* learned corrections kept                              */
-    int learned_rejected;   /* learned corrections rejected (plain MAS used)         */
+    int learned_accepted;   /* reserved (learned coarse correction): 0               */
+    int learned_rejected;   /* reserved (learned coarse correction): 0               */
     float ms_convert;       /* device time per phase (CUDA events; 0 if not timed)   */
     float ms_mas_build;
     float ms_mas_assemble;
@@ -197,6 +198,13 @@ int stg_mas_export_matrices(stg_handle h, double* mat, float* inv, int* nbanks);
  * bytes per launch, nnzb*(block + 8) + 3*n*vec with block = 72 (FP64) or 36 (FP32) and
  * vec = 8 or 4 (each array counted once). */
 int stg_profile_spmv(stg_handle h, int reps, float* avg_ms, double* bytes);
+
+/* Diagnostic (no counterpart in the reference) for the bounded waits of the bulk-copy
+ * pipelines: one thread waits, with the same bounded poll, on an mbarrier that nothing
+ * completes.  *status receives what the kernel recorded (STG_ERR_TIMEOUT when the wait
+ * gave up, as it must) and *seconds how long the wait took.  Nothing is left in flight;
+ * the device stays usable.  Returns STG_OK when the diagnostic ran. */
+int stg_selftest_wait_timeout(int* status, double* seconds);
 
 /* ---- allocation-free SpMV ---------------------------------------------------------- */
 /* No counterpart in the reference.  The same y = a * A * x + b * y as stg_spmv (same

@@ -137,6 +137,11 @@ int stg_create(const stg_config* cfg, stg_handle* out)
             stg::set_error("stg_create: invalid configuration value");
             return STG_ERR_INVALID;
         }
+        if(c.learned != 0)
+        {
+            stg::set_error("stg_create: the learned coarse correction is not available in this build (learned must be 0)");
+            return STG_ERR_INVALID;
+        }
         int ndev = 0;
         if(cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
         {
@@ -431,6 +436,25 @@ int stg_mas_export_matrices(stg_handle h, double* mat, float* inv, int* nbanks)
 namespace stg
 {
 int profile_spmv(Solver& S, int reps, float* avg_ms, double* bytes);
+}
+
+namespace stg
+{
+int selftest_wait(int* status, double* seconds);
+}
+
+extern "C" int stg_selftest_wait_timeout(int* status, double* seconds)
+{
+    GUARD({
+        int dev = 0;
+        if(cudaGetDeviceCount(&dev) != cudaSuccess || dev < 1)
+        {
+            cudaGetLastError();
+            stg::set_error("no CUDA device");
+            return STG_ERR_NO_DEVICE;
+        }
+        return stg::selftest_wait(status, seconds);
+    })
 }
 
 extern "C" int stg_profile_spmv(stg_handle h, int reps, float* avg_ms, double* bytes)

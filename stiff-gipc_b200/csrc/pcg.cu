@@ -1457,6 +1457,44 @@ int pack_blocks(Solver& S)
     return 0;
 }
 
+// Diagnostic for the bounded waits: one thread arms an mbarrier that no arrival or copy will
+// ever complete and waits on it with the same bounded poll as the bulk-copy pipelines
+// (mbar_wait).  The wait gives up, the kernel records STG_ERR_TIMEOUT and the elapsed
+// nanoseconds, and returns; nothing is in flight, so the context stays usable.
+__global__ void k_selftest_wait(int* status, unsigned long long* ns)
+{
+    __shared__ __align__(8) unsigned long long bar;
+    if(threadIdx.x != 0) return;
+    const unsigned b = smem_u32(&bar);
+    mbar_init(b, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    unsigned long long t0, t1;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    const bool ok = mbar_wait(b, 0);
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+    *status = ok ? 0 : 6;  // STG_ERR_TIMEOUT
+    *ns = t1 - t0;
+}
+
+int selftest_wait(int* status, double* seconds)
+{
+    int* d_status = nullptr;
+    unsigned long long* d_ns = nullptr;
+    STG_CUDA_TRY(cudaMalloc(&d_status, sizeof(int) + sizeof(unsigned long long) * 2));
+    d_ns = reinterpret_cast<unsigned long long*>(d_status + 2);
+    k_selftest_wait<<<1, 32>>>(d_status, d_ns);
+    cudaError_t e = cudaGetLastError();
+    int h_status = -1;
+    unsigned long long h_ns = 0;
+    if(e == cudaSuccess) e = cudaMemcpy(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if(e == cudaSuccess) e = cudaMemcpy(&h_ns, d_ns, sizeof(h_ns), cudaMemcpyDeviceToHost);
+    cudaFree(d_status);
+    STG_CUDA_TRY(e);
+    if(status) *status = h_status;
+    if(seconds) *seconds = 1e-9 * (double)h_ns;
+    return 0;
+}
+
 // ---------------------------------------------------------------------------------------
 // host driver
 // ---------------------------------------------------------------------------------------

@@ -90,6 +90,7 @@ def lib():
     L.stg_mas_export_matrices.argtypes = [vp, vp, vp, C.POINTER(ci)]
     L.stg_profile_spmv.argtypes = [vp, ci, C.POINTER(C.c_float), C.POINTER(cd)]
     L.stg_spmv_noalloc.argtypes = [cd, vp, vp, vp, ci, vp, cd, vp, ci, vp]
+    L.stg_selftest_wait_timeout.argtypes = [C.POINTER(ci), C.POINTER(cd)]
     for name in header_symbols():
         if name not in ("stg_last_error", "stg_config_default"):
             getattr(L, name).restype = ci

@@ -68,3 +68,15 @@ def test_missing_library_fails_loudly(tmp_path, monkeypatch):
     monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "libstgipc.so"))
     with pytest.raises(ImportError):
         _lib.lib()
+
+
+def test_learned_flag_rejected_before_device(L):
+    """The learned coarse correction is not built: asking for it is an error, not a silent
+    plain solve."""
+    from stgipc import _lib
+    h = C.c_void_p()
+    c = _lib.Config()
+    L.stg_config_default(C.byref(c))
+    c.learned = 1
+    assert L.stg_create(C.byref(c), C.byref(h)) == _lib.STG_ERR_INVALID
+    assert b"learned" in L.stg_last_error()
