@@ -1197,12 +1197,75 @@ __global__ void __launch_bounds__(PB) k_phase_c1(PcgDev c)
     phase_c<B>(c, 1, 2, GT, GN, false);
 }
 
-// C2: levels 2 -> 3 -> ... (small) by one CTA
+// C2: levels 2 -> 3 -> ... (small) by one CTA.  All nodes of the levels >= 2 (contiguous
+// from the first level-2 node) fit in shared memory: their residuals, closed masks and
+// parents are loaded in one round, each level is restricted inside shared memory (the
+// component leader sums its members in lane order, as restrict_level does), and the levels
+// >= 3 are stored once at the end.  More nodes than C2_SMEM_NODES: level by level through
+// global memory.
+constexpr int C2_SMEM_NODES = 4096;
+constexpr int C2_SMEM_BYTES = C2_SMEM_NODES * (16 + 4 + 4);
+
 template <int B>
 __global__ void __launch_bounds__(1024) k_phase_c2(PcgDev c)
 {
     if(c.flags[F_DONE]) return;
-    phase_c<B>(c, 2, c.L - 1, threadIdx.x, blockDim.x, true);
+    const int b2 = __ldg(c.ls_dev + 5);                   // first level-2 node
+    const int total = __ldg(c.ls_dev + 2 * (c.L - 1) + 1) + __ldg(c.ls_dev + 2 * (c.L - 1)) - b2;
+    if(total > C2_SMEM_NODES)
+    {
+        phase_c<B>(c, 2, c.L - 1, threadIdx.x, blockDim.x, true);
+        return;
+    }
+    extern __shared__ float4 c2_smem[];
+    float4* rv = c2_smem;
+    unsigned* cm = reinterpret_cast<unsigned*>(rv + C2_SMEM_NODES);
+    int* par = reinterpret_cast<int*>(cm + C2_SMEM_NODES);
+    const int n2 = __ldg(c.ls_dev + 4);
+    for(int i = threadIdx.x; i < total; i += 1024)
+    {
+        rv[i] = i < n2 ? *reinterpret_cast<const float4*>(c.R + 4 * (size_t)(b2 + i)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        cm[i] = c.closed[b2 + i];
+        par[i] = c.going_next[b2 + i] - b2;
+    }
+    __syncthreads();
+    for(int level = 2; level < c.L - 1; level++)
+    {
+        const int number = __ldg(c.ls_dev + 2 * level), begin = __ldg(c.ls_dev + 2 * level + 1) - b2;
+        const int span = (number + 31) / 32 * 32;
+        for(int i = threadIdx.x; i < span; i += 1024)
+        {
+            const bool valid = i < number;
+            float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+            unsigned msk = 0;
+            if(valid)
+            {
+                const float4 v = rv[begin + i];
+                r0 = v.x;
+                r1 = v.y;
+                r2 = v.z;
+                msk = cm[begin + i];
+            }
+            float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll 4
+            for(int bb = 0; bb < B; bb++)
+            {
+                const float x0 = group_shfl<B>(r0, bb);
+                const float x1 = group_shfl<B>(r1, bb);
+                const float x2 = group_shfl<B>(r2, bb);
+                if(msk & (1u << bb))
+                {
+                    a0 += x0;
+                    a1 += x1;
+                    a2 += x2;
+                }
+            }
+            if(valid && __popc(msk & lanemask_lt(i % B)) == 0) rv[par[begin + i]] = make_float4(a0, a1, a2, 0.f);
+        }
+        __syncthreads();
+    }
+    for(int i = n2 + threadIdx.x; i < total; i += 1024)
+        *reinterpret_cast<float4*>(c.R + 4 * (size_t)(b2 + i)) = rv[i];
 }
 
 template <int B>
@@ -1512,7 +1575,7 @@ static int launch_mas_cd(Solver& S, const PcgDev& c)
     }
     if(c.L > 3)
     {
-        k_phase_c2<B><<<1, 1024, 0, s>>>(c);
+        k_phase_c2<B><<<1, 1024, C2_SMEM_BYTES, s>>>(c);
         STG_LAUNCH_CHECK();
         S.launches++;
     }
@@ -1656,6 +1719,7 @@ static int set_carveouts()
     STG_CUDA_TRY(cudaFuncSetAttribute(k_restrict01<BB>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
     STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_c1<BB>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
     STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_c2<BB>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
+    STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_c2<BB>, cudaFuncAttributeMaxDynamicSharedMemorySize, C2_SMEM_BYTES));
     STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_d<BB>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
     STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_d16, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
     STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_e<T, B>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
