@@ -65,8 +65,8 @@ typedef struct stg_config
     int refine_interval;    /* FP32 mode: recompute r = b - A x in FP64 every k iters    */
     int loop_mode;          /* STG_LOOP_HOST / STG_LOOP_GRAPH / STG_LOOP_PERSISTENT      */
     int graph_batch;        /* iterations per captured graph launch (STG_LOOP_GRAPH)     */
-    int learned;            /* reserved for a learned coarse correction inside a flexible
-                               PCG; not available in this build: must be 0               */
+    int learned;            /* 1: apply the learned coarse correction (stg_net_*) inside a
+                               flexible PCG, MAS only, host or graph loop; 0: off        */
     void* stream;           /* cudaStream_t (NULL = legacy default stream)               */
 } stg_config;
 
@@ -86,8 +86,9 @@ typedef struct stg_stats
     int levels;             /* MAS levelnum                                          */
     int total_clusters;     /* MAS totalNumberClusters                               */
     int replacements;       /* FP64 residual replacements (FP32 mode)                */
-    int learned_accepted;   /* reserved (learned coarse correction): 0               */
-    int learned_rejected;   /* reserved (learned coarse correction): 0               */
+    int learned_accepted;   /* residual replacements at which the FP64 residual had
+                               fallen since the previous one with the learned correction on */
+    int learned_rejected;   /* ... had not: the correction was switched off (0 or 1)   */
     float ms_convert;       /* device time per phase (CUDA events; 0 if not timed)   */
     float ms_mas_build;
     float ms_mas_assemble;
@@ -226,6 +227,60 @@ int stg_selftest_wait_timeout(int* status, double* seconds);
 int stg_spmv_noalloc(double a, const double* blocks, const int32_t* rows,
                      const int32_t* cols, int nnzb, const double* x, double b, double* y,
                      int n, void* stream);
+
+/* ---- learned coarse correction ------------------------------------------------------ */
+/* No counterpart in the reference (its MAS is the fallback).  A 3-layer message-passing
+ * network (hidden width 64, BF16 weights, FP32 accumulation) over the nodes of one coarse
+ * MAS level predicts a correction of that level's bank solve: z_l = D_l^-1 r_l + s d(r_l),
+ * inside a flexible PCG (beta = r_k.(z_k - z_(k-1)) / r_(k-1).z_(k-1)).  At every FP64
+ * residual replacement the correction must have lowered the true residual since the
+ * previous one, else the solve continues with plain MAS (stg_stats.learned_*).
+ * Parameters are one FP32 vector of STG_NET_PARAMS floats, every weight matrix stored
+ * [out][in]: W0 [64][16] at 0, b0 [64] at 1024, W1..W3 [64][128] at 1088 + 8192 k, b1..b3
+ * [64] at 25664 + 64 k, Wo [8][64] at 25856, bo [8] at 26368 (outputs 3..7 unused). */
+#define STG_NET_PARAMS 26376
+
+/* The coarse level the network works on (1 .. levels-1; 0 = none).  Takes effect at the
+ * next MAS assembly, which then builds the level's graph from its Galerkin operator. */
+int stg_net_configure(stg_handle h, int level);
+/* Nodes and directed neighbour entries of the level's graph (after an assembly). */
+int stg_net_graph_info(stg_handle h, int* nodes, int* entries);
+/* Copies the graph to caller device buffers: row [nodes+1], col [entries] (both directions,
+ * sorted by column), w [entries] = |A_ij|_F / sqrt(|A_ii|_F |A_jj|_F), oblk [9 entries]
+ * (A_(i,col) row-major), dblk [9 nodes], feat [nodes] (centred log trace of A_ii); FP32. */
+int stg_net_export_graph(stg_handle h, int32_t* row, int32_t* col, float* w, float* oblk, float* dblk,
+                         float* feat);
+/* Arms the sample recorder for the following solves (capacity 0 disarms): at iterations
+ * 0, every, 2 every, ... the level's restricted residual and bank solve (float4 per node,
+ * before any correction) go to rc / zc [capacity][nodes][4]. */
+int stg_net_record(stg_handle h, float* rc, float* zc, int capacity, int every);
+int stg_net_recorded(stg_handle h, int* count);
+/* Parameters for the in-loop network (device pointer, STG_NET_PARAMS floats, copied). */
+int stg_net_set_params(stg_handle h, const float* params);
+
+/* Training, handle-free, on `stream`, through the project's own kernels. */
+typedef struct stg_net_graph
+{
+    int nodes, entries;
+    const int32_t* row;
+    const int32_t* col;
+    const float* w;
+    const float* oblk;
+    const float* dblk;
+    const float* feat;
+} stg_net_graph;
+/* Bytes of the 256-byte aligned device scratch a forward / training step over `samples`
+ * samples of a `nodes`-node graph needs. */
+size_t stg_net_scratch_bytes(int nodes, int samples);
+/* delta [samples][nodes][4] = the network's output d for samples rc / zc. */
+int stg_net_forward(const stg_net_graph* g, const float* rc, const float* zc, int samples, const float* params,
+                    float* delta, void* scratch, size_t scratch_bytes, void* stream);
+/* One step: loss[s] = J(z + s_z d) / |J(z)| per sample (J(v) = v.A v / 2 - v.r), grad =
+ * gradient of the mean loss; with lr > 0 an Adam step (beta 0.9 / 0.999, eps 1e-8, bias
+ * corrections of step `step` >= 1) on params with moments m, v.  All device pointers. */
+int stg_net_train_step(const stg_net_graph* g, const float* rc, const float* zc, int samples, float* params,
+                       float* grad, float* adam_m, float* adam_v, int step, float lr, float* loss, void* scratch,
+                       size_t scratch_bytes, void* stream);
 
 #ifdef __cplusplus
 }

@@ -137,9 +137,19 @@ int stg_create(const stg_config* cfg, stg_handle* out)
             stg::set_error("stg_create: invalid configuration value");
             return STG_ERR_INVALID;
         }
-        if(c.learned != 0)
+        if(c.learned != 0 && c.learned != 1)
         {
-            stg::set_error("stg_create: the learned coarse correction is not available in this build (learned must be 0)");
+            stg::set_error("stg_create: learned must be 0 or 1");
+            return STG_ERR_INVALID;
+        }
+        if(c.learned && c.preconditioner != STG_PRECOND_MAS)
+        {
+            stg::set_error("stg_create: the learned coarse correction needs the MAS preconditioner");
+            return STG_ERR_INVALID;
+        }
+        if(c.learned && c.loop_mode == STG_LOOP_PERSISTENT)
+        {
+            stg::set_error("stg_create: the learned coarse correction runs in the host and graph loops only");
             return STG_ERR_INVALID;
         }
         int ndev = 0;
@@ -467,5 +477,195 @@ extern "C" int stg_profile_spmv(stg_handle h, int reps, float* avg_ms, double* b
             return STG_ERR_INVALID;
         }
         return stg::profile_spmv(*h, reps, avg_ms, bytes);
+    })
+}
+
+// ---- learned coarse correction ------------------------------------------------------------
+namespace
+{
+int net_graph_of(const stg_net_graph* g, stg::NetGraph& out)
+{
+    if(!g || g->nodes < 1 || g->entries < 0 || !g->row || (g->entries > 0 && (!g->col || !g->w || !g->oblk)) ||
+       !g->dblk || !g->feat)
+    {
+        stg::set_error("stg_net: invalid graph");
+        return STG_ERR_INVALID;
+    }
+    out.n = g->nodes;
+    out.nnz = g->entries;
+    out.row = g->row;
+    out.col = g->col;
+    out.w = g->w;
+    out.oblk = g->oblk;
+    out.dblk = g->dblk;
+    out.feat = g->feat;
+    return STG_OK;
+}
+}  // namespace
+
+int stg_net_configure(stg_handle h, int level)
+{
+    CHECK_HANDLE(h);
+    GUARD({
+        if(level < 0 || level >= stg::kMaxLevels)
+        {
+            stg::set_error("stg_net_configure: level out of range");
+            return STG_ERR_INVALID;
+        }
+        h->learned.level = level;
+        h->learned.graph_ready = false;
+        h->graph_dirty = true;
+        return STG_OK;
+    })
+}
+
+int stg_net_graph_info(stg_handle h, int* nodes, int* entries)
+{
+    CHECK_HANDLE(h);
+    if(!h->learned.graph_ready)
+    {
+        stg::set_error("stg_net_graph_info: no graph: configure a level and assemble MAS first");
+        return STG_ERR_NOT_READY;
+    }
+    if(nodes) *nodes = h->learned.graph.n;
+    if(entries) *entries = h->learned.graph.nnz;
+    return STG_OK;
+}
+
+int stg_net_export_graph(stg_handle h, int32_t* row, int32_t* col, float* w, float* oblk, float* dblk, float* feat)
+{
+    CHECK_HANDLE(h);
+    GUARD({
+        const stg::NetGraphStore& G = h->learned.graph;
+        if(!h->learned.graph_ready)
+        {
+            stg::set_error("stg_net_export_graph: no graph: configure a level and assemble MAS first");
+            return STG_ERR_NOT_READY;
+        }
+        if(!row || !dblk || !feat || (G.nnz > 0 && (!col || !w || !oblk)))
+        {
+            stg::set_error("stg_net_export_graph: null buffer");
+            return STG_ERR_INVALID;
+        }
+        cudaStream_t s = h->stream;
+        STG_CUDA_TRY(cudaMemcpyAsync(row, G.row.data(), sizeof(int) * (G.n + 1), cudaMemcpyDeviceToDevice, s));
+        STG_CUDA_TRY(cudaMemcpyAsync(dblk, G.dblk.data(), sizeof(float) * 9 * G.n, cudaMemcpyDeviceToDevice, s));
+        STG_CUDA_TRY(cudaMemcpyAsync(feat, G.feat.data(), sizeof(float) * G.n, cudaMemcpyDeviceToDevice, s));
+        if(G.nnz > 0)
+        {
+            STG_CUDA_TRY(cudaMemcpyAsync(col, G.col.data(), sizeof(int) * G.nnz, cudaMemcpyDeviceToDevice, s));
+            STG_CUDA_TRY(cudaMemcpyAsync(w, G.w.data(), sizeof(float) * G.nnz, cudaMemcpyDeviceToDevice, s));
+            STG_CUDA_TRY(cudaMemcpyAsync(oblk, G.oblk.data(), sizeof(float) * 9 * G.nnz, cudaMemcpyDeviceToDevice, s));
+        }
+        return STG_OK;
+    })
+}
+
+int stg_net_record(stg_handle h, float* rc, float* zc, int capacity, int every)
+{
+    CHECK_HANDLE(h);
+    GUARD({
+        if(capacity < 0 || (capacity > 0 && (!rc || !zc || every < 1)))
+        {
+            stg::set_error("stg_net_record: invalid buffers, capacity or interval");
+            return STG_ERR_INVALID;
+        }
+        stg::LearnedState& L = h->learned;
+        STG_TRY(L.rec_count.resize(1));
+        STG_CUDA_TRY(cudaMemsetAsync(L.rec_count.data(), 0, sizeof(int), h->stream));
+        L.rec_rc = capacity > 0 ? rc : nullptr;
+        L.rec_zc = capacity > 0 ? zc : nullptr;
+        L.rec_cap = capacity;
+        L.rec_every = capacity > 0 ? every : 0;
+        return STG_OK;
+    })
+}
+
+int stg_net_recorded(stg_handle h, int* count)
+{
+    CHECK_HANDLE(h);
+    GUARD({
+        if(!count)
+        {
+            stg::set_error("stg_net_recorded: count is null");
+            return STG_ERR_INVALID;
+        }
+        *count = 0;
+        if(h->learned.rec_count.data())
+        {
+            STG_CUDA_TRY(cudaMemcpyAsync(count, h->learned.rec_count.data(), sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+            STG_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        }
+        return STG_OK;
+    })
+}
+
+int stg_net_set_params(stg_handle h, const float* params)
+{
+    CHECK_HANDLE(h);
+    GUARD({
+        if(!params)
+        {
+            stg::set_error("stg_net_set_params: params is null");
+            return STG_ERR_INVALID;
+        }
+        stg::LearnedState& L = h->learned;
+        STG_TRY(L.params.resize(stg::P_COUNT));
+        STG_TRY(L.wbf.resize(2 * stg::P_COUNT));
+        STG_CUDA_TRY(cudaMemcpyAsync(L.params.data(), params, sizeof(float) * stg::P_COUNT, cudaMemcpyDeviceToDevice,
+                                     h->stream));
+        STG_TRY(stg::net_to_bf16(h->stream, L.params.data(), L.wbf.data()));
+        L.has_params = true;
+        return STG_OK;
+    })
+}
+
+size_t stg_net_scratch_bytes(int nodes, int samples)
+{
+    if(nodes < 1 || samples < 1) return 0;
+    return stg::net_scratch_bytes(nodes, samples);
+}
+
+int stg_net_forward(const stg_net_graph* g, const float* rc, const float* zc, int samples, const float* params,
+                    float* delta, void* scratch, size_t scratch_bytes, void* stream)
+{
+    GUARD({
+        stg::NetGraph G;
+        STG_TRY(net_graph_of(g, G));
+        if(!rc || !zc || !params || !delta || samples < 1)
+        {
+            stg::set_error("stg_net_forward: invalid arguments");
+            return STG_ERR_INVALID;
+        }
+        stg::NetBuffers b;
+        STG_TRY(stg::net_carve(scratch, scratch_bytes, G.n, samples, b));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        int l = 0;
+        STG_TRY(stg::net_to_bf16(s, params, b.wbf));
+        STG_TRY(stg::net_forward(s, G, rc, zc, samples, b, b.wbf, params, nullptr, nullptr, &l));
+        STG_CUDA_TRY(cudaMemcpyAsync(delta, b.delta, sizeof(float) * 4 * (size_t)G.n * samples, cudaMemcpyDeviceToDevice, s));
+        return STG_OK;
+    })
+}
+
+int stg_net_train_step(const stg_net_graph* g, const float* rc, const float* zc, int samples, float* params,
+                       float* grad, float* adam_m, float* adam_v, int step, float lr, float* loss, void* scratch,
+                       size_t scratch_bytes, void* stream)
+{
+    GUARD({
+        stg::NetGraph G;
+        STG_TRY(net_graph_of(g, G));
+        if(!rc || !zc || !params || !grad || samples < 1 || !(lr >= 0.f) || (lr > 0.f && (!adam_m || !adam_v || step < 1)))
+        {
+            stg::set_error("stg_net_train_step: invalid arguments");
+            return STG_ERR_INVALID;
+        }
+        stg::NetBuffers b;
+        STG_TRY(stg::net_carve(scratch, scratch_bytes, G.n, samples, b));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        int l = 0;
+        STG_TRY(stg::net_train_step(s, G, rc, zc, samples, b, params, grad, adam_m, adam_v, step, lr, &l));
+        if(loss) STG_CUDA_TRY(cudaMemcpyAsync(loss, b.loss, sizeof(float) * samples, cudaMemcpyDeviceToDevice, s));
+        return STG_OK;
     })
 }

@@ -945,6 +945,8 @@ static int mas_assemble_t(Solver& S, int offset)
         STG_LAUNCH_CHECK();
         S.launches++;
     }
+    bool learned_captured = false;
+    S.learned.graph_ready = false;
     if(m.L > 1 && nnzb > 0)
     {
         // level 1 from the fine matrix
@@ -961,6 +963,20 @@ static int mas_assemble_t(Solver& S, int offset)
         for(int level = 1;; level++)
         {
             const int begin = m.level_size[2 * level + 1];
+            if(level == S.learned.level && nnz > 0)
+            {
+                // the learned level's Galerkin operator, kept for its graph (built below)
+                LearnedState& Ls = S.learned;
+                STG_TRY(Ls.urow.resize(nnz));
+                STG_TRY(Ls.ucol.resize(nnz));
+                STG_TRY(Ls.ublk.resize(9 * (size_t)nnz));
+                STG_CUDA_TRY(cudaMemcpyAsync(Ls.urow.data(), m.ga_rows.data(), sizeof(int) * nnz, cudaMemcpyDeviceToDevice, s));
+                STG_CUDA_TRY(cudaMemcpyAsync(Ls.ucol.data(), m.ga_cols.data(), sizeof(int) * nnz, cudaMemcpyDeviceToDevice, s));
+                STG_CUDA_TRY(cudaMemcpyAsync(Ls.ublk.data(), m.ga_blocks.data(), sizeof(double) * 9 * nnz,
+                                             cudaMemcpyDeviceToDevice, s));
+                Ls.unnz = nnz;
+                learned_captured = true;
+            }
             if(nnz > 0)
             {
                 k_mas_extract<B><<<std::max(1, std::min(div_up(nnz, 256), kSMs * 16)), 256, 0, s>>>(
@@ -1005,6 +1021,18 @@ static int mas_assemble_t(Solver& S, int offset)
         STG_LAUNCH_CHECK();
     }
     S.launches++;
+    if(learned_captured)
+    {
+        LearnedState& Ls = S.learned;
+        const int n = m.level_size[2 * Ls.level];
+        Ls.begin = m.level_size[2 * Ls.level + 1];
+        STG_TRY(net_build_graph(s, Ls.graph, n, Ls.unnz, Ls.urow.data(), Ls.ucol.data(), Ls.ublk.data(), &S.launches));
+        Ls.graph.level = Ls.level;
+        const size_t bytes = net_scratch_bytes(n, 1);
+        STG_TRY(Ls.scratch.resize(bytes));
+        STG_TRY(net_carve(Ls.scratch.data(), bytes, n, 1, Ls.buf));
+        Ls.graph_ready = true;
+    }
     m.assembled = true;
     return 0;
 }

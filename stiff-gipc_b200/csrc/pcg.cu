@@ -47,7 +47,8 @@ enum Site : int
     SITE_R = 2,
     SITE_E = 3,
     SITE_INIT = 4,
-    SITE_INIT_RZ = 5
+    SITE_INIT_RZ = 5,
+    SITE_F = 6  // r_(k+1).z_k of phase E (flexible PCG)
 };
 
 // ---------------------------------------------------------------------------------------
@@ -837,7 +838,9 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T>::MIN_CTAS) k_phase_a_tiled
     // beta = rz_k / rz_(k-1): rz_k from phase E's partials, rz_(k-1) as phase B recorded it
     // (the first iteration has p_0 = 0: beta = 0)
     const double rz_new = consume_sum<A_THREADS>(c, SITE_E, c.grid_e);
-    const double s_beta = (long)s_iter == 0 ? 0.0 : rz_new / rz_old;
+    // flexible PCG (learned correction): beta = r_k.(z_k - z_(k-1)) / r_(k-1).z_(k-1)
+    const double rz_mix = c.flex && (long)s_iter > 0 ? consume_sum<A_THREADS>(c, SITE_F, c.grid_e) : 0.0;
+    const double s_beta = (long)s_iter == 0 ? 0.0 : (rz_new - rz_mix) / rz_old;
     int* meta = reinterpret_cast<int*>(asm_ + G::STAGES * G::STAGE);
     const unsigned sbase = smem_u32(asm_);
     const unsigned bar_full = smem_u32(asm_ + G::STAGES * G::STAGE + G::META);
@@ -1289,6 +1292,20 @@ __global__ void __launch_bounds__(PB, 8) k_phase_e(PcgDev c, int op)
     __shared__ double red[PB / 32];
     const double bs = block_sum<PB>(v, red);
     if(threadIdx.x == 0) c.partials[(size_t)SITE_E * c.slots + blockIdx.x] = bs;
+    if(c.flex && (long)__ldcg(c.scal + SS_ITER) > 0)
+    {
+        // flexible PCG: r_(k+1).z_k with z_k still in the other zp buffer
+        const T* zo = zpbuf<T>(c, iter_parity(c) ^ 1);
+        double vo = 0;
+        for(int bi = GT; bi < c.nrows; bi += GN)
+        {
+            T z0, z1, z2;
+            ld4(zo + 8 * (size_t)bi, z0, z1, z2);
+            vo += c.r[3 * bi] * (double)z0 + c.r[3 * bi + 1] * (double)z1 + c.r[3 * bi + 2] * (double)z2;
+        }
+        const double bo = block_sum<PB>(vo, red);
+        if(threadIdx.x == 0) c.partials[(size_t)SITE_F * c.slots + blockIdx.x] = bo;
+    }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1633,6 +1650,25 @@ static int launch_phase_a(const PcgDev& c, cudaStream_t s)
     return 0;
 }
 
+// learned coarse correction after the bank solves: the sample recorder (the level's r and
+// z before any correction), then the network's forward pass and apply on the level's Z
+static int launch_learned(Solver& S, const PcgDev& c)
+{
+    LearnedState& Ls = S.learned;
+    const float* R = c.R + 4 * (size_t)Ls.begin;
+    float* Z = c.Z + 4 * (size_t)Ls.begin;
+    if(c.net_mode & 2)
+    {
+        STG_TRY(net_record(S.stream, R, Z, Ls.graph.n, c.scal, c.flags, Ls.rec_rc, Ls.rec_zc, Ls.rec_count.data(),
+                           Ls.rec_cap, Ls.rec_every));
+        S.launches++;
+    }
+    if(c.net_mode & 1)
+        STG_TRY(net_forward(S.stream, Ls.graph.view(), R, Z, 1, Ls.buf, Ls.wbf.data(), Ls.params.data(), Z, c.flags,
+                            &S.launches));
+    return 0;
+}
+
 template <typename T, int B>
 static int launch_iteration(Solver& S, const PcgDev& c, int grid_vec, int grid_rows, bool in_graph_cond)
 {
@@ -1677,6 +1713,7 @@ static int launch_iteration(Solver& S, const PcgDev& c, int grid_vec, int grid_r
         }
     }
     if(B > 0) STG_TRY(launch_mas_cd<(B > 0 ? B : 16)>(S, c));
+    if(c.net_mode) STG_TRY(launch_learned(S, c));
     k_phase_e<T, B><<<grid_vec, PB, 0, s>>>(c, POST_BETA);
     STG_LAUNCH_CHECK();
     S.launches++;
@@ -1757,6 +1794,7 @@ static int pcg_run(Solver& S, PcgDev& c, int& h_done)
         STG_LAUNCH_CHECK();
         S.launches++;
         STG_TRY(launch_mas_cd<BB>(S, c));
+        if(c.net_mode) STG_TRY(launch_learned(S, c));
     }
     k_phase_e<T, B><<<grid_vec, PB, 0, s>>>(c, POST_INIT_RZ);
     STG_LAUNCH_CHECK();
@@ -2006,13 +2044,13 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
     STG_TRY(P.vbuf.resize((2 * zp_bytes + q_bytes) / sizeof(double) + 32));
     STG_TRY(pack_blocks(*this));
     const int slots = kSMs * 8;
-    STG_TRY(P.partials.resize((size_t)slots * 6));
+    STG_TRY(P.partials.resize((size_t)slots * 8));
     STG_TRY(P.scal.resize(S_COUNT));
     STG_TRY(P.counters.resize(8));
-    STG_TRY(P.flags.resize(4));
+    STG_TRY(P.flags.resize(8));
     STG_TRY(P.bar.resize(2));
     STG_CUDA_TRY(cudaMemsetAsync(P.counters.data(), 0, sizeof(unsigned) * 8, s));
-    STG_CUDA_TRY(cudaMemsetAsync(P.flags.data(), 0, sizeof(int) * 4, s));
+    STG_CUDA_TRY(cudaMemsetAsync(P.flags.data(), 0, sizeof(int) * 8, s));
     STG_CUDA_TRY(cudaMemsetAsync(P.scal.data(), 0, sizeof(double) * S_COUNT, s));
 
     // zeroed bytewise (padding included): the graph loop compares parameter blocks with memcmp
@@ -2068,6 +2106,49 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
     c.prm.stop_rule = cfg.stop_rule;
     c.prm.refine = fp32 ? cfg.refine_interval : 0;
     c.bar = P.bar.data();
+    const bool net_apply = cfg.learned != 0, net_rec = learned.rec_cap > 0;
+    if(net_apply || net_rec)
+    {
+        if(!use_mas)
+        {
+            set_error("stg_pcg_solve: the learned coarse correction and its recorder need the MAS preconditioner");
+            return STG_ERR_INVALID;
+        }
+        if(!learned.graph_ready)
+        {
+            set_error("stg_pcg_solve: no graph of the learned level: configure the level (stg_net_configure) before "
+                      "the MAS assembly, with a level below the hierarchy's level count");
+            return STG_ERR_NOT_READY;
+        }
+        if(cfg.loop_mode == STG_LOOP_PERSISTENT)
+        {
+            set_error("stg_pcg_solve: the learned coarse correction runs in the host and graph loops only");
+            return STG_ERR_INVALID;
+        }
+        if(net_apply && !learned.has_params)
+        {
+            set_error("stg_pcg_solve: learned is on but no parameters were set (stg_net_set_params)");
+            return STG_ERR_NOT_READY;
+        }
+        STG_TRY(net_prepare());
+        c.flex = net_apply ? 1 : 0;
+        c.net_mode = (net_apply ? 1 : 0) | (net_rec ? 2 : 0);
+        c.net_n = learned.graph.n;
+        c.net_rec_cap = learned.rec_cap;
+        c.net_rec_every = learned.rec_every;
+        c.net_ptrs[0] = learned.graph.row.data();
+        c.net_ptrs[1] = learned.scratch.data();
+        c.net_ptrs[2] = learned.params.data();
+        c.net_ptrs[3] = learned.rec_rc;
+        c.net_ptrs[4] = learned.rec_zc;
+        c.net_ptrs[5] = learned.rec_count.data();
+        if(net_apply)
+        {
+            const int on = 1;
+            STG_CUDA_TRY(cudaMemcpyAsync(P.flags.data() + F_LEARN, &on, sizeof(int), cudaMemcpyHostToDevice, s));
+        }
+        if(net_rec) STG_CUDA_TRY(cudaMemsetAsync(learned.rec_count.data(), 0, sizeof(int), s));
+    }
 
     int done = 0;
     if(fp32)
@@ -2092,9 +2173,9 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
     pcg_ready = true;
 
     double h_scal[S_COUNT];
-    int h_flags[4];
+    int h_flags[8];
     STG_CUDA_TRY(cudaMemcpyAsync(h_scal, P.scal.data(), sizeof(double) * S_COUNT, cudaMemcpyDeviceToHost, s));
-    STG_CUDA_TRY(cudaMemcpyAsync(h_flags, P.flags.data(), sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
+    STG_CUDA_TRY(cudaMemcpyAsync(h_flags, P.flags.data(), sizeof(int) * 8, cudaMemcpyDeviceToHost, s));
     STG_CUDA_TRY(cudaStreamSynchronize(s));
     const long max_iter = c.prm.max_iter;
     int status = h_flags[F_DONE] ? h_flags[F_STATUS] : STG_MAX_ITER;
@@ -2113,6 +2194,8 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
         st->rz_final = h_scal[S_RZ];
         st->rel_residual_recursive = h_scal[S_BB] > 0 ? std::sqrt(h_scal[S_RR] / h_scal[S_BB]) : 0.0;
         st->replacements = h_flags[F_REPL];
+        st->learned_accepted = h_flags[F_LACC];
+        st->learned_rejected = h_flags[F_LREJ];
     }
     return status;
 }

@@ -49,7 +49,7 @@ struct PcgDev
     int abd_bodies;
     const double* abd_inv;
     // reductions / control
-    double* partials;         // [6][slots]
+    double* partials;         // [8][slots]
     unsigned* counters;       // [8]
     double* scal;
     int* flags;
@@ -60,6 +60,12 @@ struct PcgDev
     cudaGraphConditionalHandle h_while, h_if;
     int use_cond;
     unsigned* bar;            // persistent barrier: [0] count, [1] generation
+    // learned coarse correction: flexible PCG (beta from r_(k+1).(z_(k+1) - z_k), phase E's
+    // r.z_old partials at SITE_F); the rest only keys the captured graph
+    int flex;
+    int net_mode;             // bit 0: network applied, bit 1: samples recorded
+    int net_n, net_rec_cap, net_rec_every;
+    const void* net_ptrs[6];
 };
 
 }  // namespace stg

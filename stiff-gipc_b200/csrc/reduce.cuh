@@ -31,13 +31,17 @@ enum : int
 {
     F_DONE = 0,        // nonzero: loop finished
     F_STATUS = 1,      // STG_OK / STG_MAX_ITER / STG_BREAKDOWN
-    F_REPL = 2         // residual replacements performed
+    F_REPL = 2,        // residual replacements performed
+    F_LEARN = 3,       // nonzero: the learned coarse correction is applied
+    F_LACC = 4,        // replacement checkpoints the learned correction passed
+    F_LREJ = 5         // checkpoints it failed (the correction is then switched off)
 };
 
 // scalar slots (mirror solver.hpp)
 enum : int
 {
-    SS_RZ = 0, SS_RZ0 = 1, SS_PQ = 2, SS_ALPHA = 3, SS_BETA = 4, SS_RZNEW = 5, SS_RR = 6, SS_BB = 7, SS_ITER = 9
+    SS_RZ = 0, SS_RZ0 = 1, SS_PQ = 2, SS_ALPHA = 3, SS_BETA = 4, SS_RZNEW = 5, SS_RR = 6, SS_BB = 7, SS_ITER = 9,
+    SS_LRR = 10
 };
 
 __device__ __forceinline__ void post_op(int op, int slot, double total, double* scal, int* flags, const PcgParams& p,
@@ -64,6 +68,7 @@ __device__ __forceinline__ void post_op(int op, int slot, double total, double* 
             scal[SS_RZ0] = total;
             scal[SS_BETA] = 0.0;
             scal[SS_ITER] = 0.0;
+            scal[SS_LRR] = scal[SS_BB];
             break;
         case POST_ALPHA:
         {
@@ -81,6 +86,19 @@ __device__ __forceinline__ void post_op(int op, int slot, double total, double* 
         case POST_RECHECK:
         {
             scal[SS_RR] = total;
+            if(op == POST_RECHECK && flags[F_LEARN])
+            {
+                // the FP64 residual judges the learned correction: it must have fallen since
+                // the previous replacement (or since r0 = b); else plain MAS from here on
+                if(total < scal[SS_LRR])
+                    flags[F_LACC] += 1;
+                else
+                {
+                    flags[F_LREJ] += 1;
+                    flags[F_LEARN] = 0;
+                }
+            }
+            if(op == POST_RECHECK) scal[SS_LRR] = total;
             long k = (long)scal[SS_ITER];
             if(op == POST_CHECK)
             {

@@ -6,6 +6,7 @@
 #pragma once
 #include "common.cuh"
 #include "pcg_dev.cuh"
+#include "learned.cuh"
 #include "../../include/stgipc.h"
 
 #include <algorithm>
@@ -111,7 +112,30 @@ enum : int
     S_BB = 7,      // b.b
     S_TOL = 8,     // stop threshold
     S_ITER = 9,    // completed iterations (as double)
+    S_LRR = 10,    // true r.r at the last residual replacement (learned correction judge)
     S_COUNT = 16
+};
+
+// The learned coarse correction of one handle: its level, parameters, the level's graph
+// (rebuilt by every MAS assembly), the in-loop forward buffers, and the sample recorder.
+struct LearnedState
+{
+    int level = 0;                 // coarse level of the network; 0: not configured
+    bool has_params = false;
+    bool graph_ready = false;      // graph built from the current assembly
+    int begin = 0;                 // first node of the level in R / Z
+    DBuf<float> params;            // [P_COUNT] FP32
+    DBuf<unsigned char> wbf;       // [P_COUNT] BF16 copy
+    DBuf<unsigned char> scratch;   // forward buffers of one sample
+    NetBuffers buf;
+    NetGraphStore graph;
+    DBuf<int> urow, ucol;          // the level's upper Galerkin BCOO, captured at assembly
+    DBuf<double> ublk;
+    int unnz = 0;
+    float* rec_rc = nullptr;       // recorder (caller buffers): samples r_c, z_c
+    float* rec_zc = nullptr;
+    int rec_cap = 0, rec_every = 0;
+    DBuf<int> rec_count;
 };
 
 struct Solver
@@ -124,6 +148,7 @@ struct Solver
     ConvertScratch cv;
     MasState mas;
     PcgState pcg;
+    LearnedState learned;
     cudaEvent_t ev[6] = {};
     bool events = false;
     int mas_fem_offset = 0;       // FEM block offset of the last MAS assembly

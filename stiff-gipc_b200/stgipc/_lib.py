@@ -49,6 +49,14 @@ class System(C.Structure):
                 ("ncp", C.c_int), ("abd_bodies", C.c_int), ("abd_inv", C.c_void_p)]
 
 
+class NetGraphC(C.Structure):
+    _fields_ = [("nodes", C.c_int), ("entries", C.c_int), ("row", C.c_void_p), ("col", C.c_void_p), ("w", C.c_void_p),
+                ("oblk", C.c_void_p), ("dblk", C.c_void_p), ("feat", C.c_void_p)]
+
+
+NET_PARAMS = 26376
+
+
 class StgError(RuntimeError):
     def __init__(self, status: int, where: str, msg: str):
         super().__init__(f"{where}: {STATUS_NAMES.get(status, status)}: {msg}")
@@ -91,9 +99,20 @@ def lib():
     L.stg_profile_spmv.argtypes = [vp, ci, C.POINTER(C.c_float), C.POINTER(cd)]
     L.stg_spmv_noalloc.argtypes = [cd, vp, vp, vp, ci, vp, cd, vp, ci, vp]
     L.stg_selftest_wait_timeout.argtypes = [C.POINTER(ci), C.POINTER(cd)]
+    L.stg_net_configure.argtypes = [vp, ci]
+    L.stg_net_graph_info.argtypes = [vp, C.POINTER(ci), C.POINTER(ci)]
+    L.stg_net_export_graph.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+    L.stg_net_record.argtypes = [vp, vp, vp, ci, ci]
+    L.stg_net_recorded.argtypes = [vp, C.POINTER(ci)]
+    L.stg_net_set_params.argtypes = [vp, vp]
+    L.stg_net_scratch_bytes.argtypes = [ci, ci]
+    L.stg_net_forward.argtypes = [C.POINTER(NetGraphC), vp, vp, ci, vp, vp, vp, C.c_size_t, vp]
+    L.stg_net_train_step.argtypes = [C.POINTER(NetGraphC), vp, vp, ci, vp, vp, vp, vp, ci, C.c_float, vp, vp,
+                                     C.c_size_t, vp]
     for name in header_symbols():
-        if name not in ("stg_last_error", "stg_config_default"):
+        if name not in ("stg_last_error", "stg_config_default", "stg_net_scratch_bytes"):
             getattr(L, name).restype = ci
+    L.stg_net_scratch_bytes.restype = C.c_size_t
     _lib = L
     return L
 

@@ -1,0 +1,167 @@
+"""The learned coarse correction: data, training and inference helpers over the C ABI.
+
+The network (stgipc.h, ``stg_net_*``) reads one coarse MAS level: its restricted residual
+r_c and bank solve z_c = D^-1 r_c, and predicts g = z_c + s_z d(r_c, z_c) in place of z_c.
+Training minimises the energy loss J(g) / |J(z_c)| with J(g) = g.A_c g / 2 - g.r_c over
+(residual, error) samples that the plain FP64 solver records (``record_samples``); all
+forward, backward and Adam work runs in the library's kernels on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import List, Optional
+
+import numpy as np
+
+from . import _lib as _L
+from ._lib import check
+
+NET_PARAMS = _L.NET_PARAMS
+IN, H, OUT, LAYERS = 16, 64, 8, 3
+OFF = dict(W0=0, b0=1024, W1=1088, b1=25664, Wo=25856, bo=26368)
+
+
+def _ptr(t):
+    return None if t is None else t.data_ptr()
+
+
+@dataclasses.dataclass
+class NetGraph:
+    """One coarse level as a graph (device tensors, layout of stg_net_export_graph)."""
+    nodes: int
+    entries: int
+    row: object
+    col: object
+    w: object
+    oblk: object
+    dblk: object
+    feat: object
+
+    def c(self) -> _L.NetGraphC:
+        g = _L.NetGraphC()
+        g.nodes, g.entries = self.nodes, self.entries
+        g.row, g.col, g.w = _ptr(self.row), _ptr(self.col), _ptr(self.w)
+        g.oblk, g.dblk, g.feat = _ptr(self.oblk), _ptr(self.dblk), _ptr(self.feat)
+        return g
+
+    def numpy(self) -> dict:
+        e = max(self.entries, 1)
+        return dict(n=self.nodes, row=self.row.cpu().numpy(), col=self.col.cpu().numpy()[:self.entries],
+                    w=self.w.cpu().numpy()[:self.entries], oblk=self.oblk.cpu().numpy()[:9 * e].reshape(e, 3, 3)[:self.entries],
+                    dblk=self.dblk.cpu().numpy().reshape(-1, 3, 3), feat=self.feat.cpu().numpy())
+
+
+def init_params(seed: int = 0, head_scale: float = 1e-3) -> np.ndarray:
+    """He-initialised weights, zero biases, a small head (the untrained network is close to
+    plain MAS: d ~ 0)."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(NET_PARAMS, np.float32)
+    p[OFF["W0"]:OFF["b0"]] = rng.standard_normal(H * IN) * np.sqrt(2.0 / 8)  # 8 live inputs
+    for k in range(LAYERS):
+        a = OFF["W1"] + k * H * 2 * H
+        p[a:a + H * 2 * H] = rng.standard_normal(H * 2 * H) * np.sqrt(2.0 / (2 * H))
+    p[OFF["Wo"]:OFF["Wo"] + 3 * H] = rng.standard_normal(3 * H) * head_scale
+    return p
+
+
+def scratch(nodes: int, samples: int, device="cuda"):
+    import torch
+    nb = int(_L.lib().stg_net_scratch_bytes(int(nodes), int(samples)))
+    return torch.empty(nb, dtype=torch.uint8, device=device)
+
+
+def forward(graph: NetGraph, rc, zc, params, samples: int, stream=None, buf=None):
+    """d [samples][nodes][4] for samples rc / zc ([samples][nodes][4] FP32)."""
+    import torch
+    buf = buf if buf is not None else scratch(graph.nodes, samples, rc.device)
+    delta = torch.empty(samples * graph.nodes * 4, dtype=torch.float32, device=rc.device)
+    s = None if stream is None else stream.cuda_stream
+    g = graph.c()
+    check(_L.lib().stg_net_forward(C.byref(g), _ptr(rc), _ptr(zc), int(samples), _ptr(params), _ptr(delta), _ptr(buf),
+                                   buf.numel(), s), "stg_net_forward")
+    return delta.view(samples, graph.nodes, 4)
+
+
+class Trainer:
+    """Adam on the library's kernels; params / moments / gradient are FP32 device tensors."""
+
+    def __init__(self, params: np.ndarray, device="cuda"):
+        import torch
+        self.device = torch.device(device)
+        self.params = torch.from_numpy(np.ascontiguousarray(params, np.float32)).to(self.device)
+        self.m = torch.zeros_like(self.params)
+        self.v = torch.zeros_like(self.params)
+        self.grad = torch.zeros_like(self.params)
+        self.t = 0
+        self._buf = {}
+
+    def _scratch(self, nodes, samples):
+        key = (nodes, samples)
+        if key not in self._buf:
+            self._buf[key] = scratch(nodes, samples, self.device)
+        return self._buf[key]
+
+    def step(self, graph: NetGraph, rc, zc, samples: int, lr: float):
+        """One Adam step on `samples` samples (lr 0: gradient only).  Returns the per-sample
+        losses (device tensor)."""
+        import torch
+        buf = self._scratch(graph.nodes, samples)
+        loss = torch.empty(samples, dtype=torch.float32, device=self.device)
+        if lr > 0:
+            self.t += 1
+        g = graph.c()
+        check(_L.lib().stg_net_train_step(C.byref(g), _ptr(rc), _ptr(zc), int(samples), _ptr(self.params),
+                                          _ptr(self.grad), _ptr(self.m), _ptr(self.v), max(self.t, 1), float(lr),
+                                          _ptr(loss), _ptr(buf), buf.numel(), None), "stg_net_train_step")
+        return loss
+
+    def evaluate(self, graph: NetGraph, rc, zc, samples: int) -> float:
+        """Mean loss without an update."""
+        return float(self.step(graph, rc, zc, samples, 0.0).mean())
+
+
+@dataclasses.dataclass
+class Dataset:
+    graph: NetGraph
+    rc: object       # [samples][nodes][4]
+    zc: object
+    samples: int
+
+
+def record_samples(solver, sysm, capacity: int = 256, every: int = 1, device="cuda") -> Dataset:
+    """Run the plain solver of `solver` (MAS, learned off, level configured) on the scene
+    `sysm` (stgipc.scenes system) with the recorder armed; returns the level's graph and
+    the recorded (r_c, z_c) samples."""
+    import torch
+    dev = torch.device(device)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    rows, cols, blocks, b = t(sysm.rows), t(sysm.cols), t(sysm.blocks.reshape(-1)), t(sysm.b)
+    x = torch.zeros_like(b)
+    # the first assembly (inside the solve) builds the graph; its size sizes the buffers
+    solver.solve_linear_system(rows, cols, blocks, b, x)
+    g = solver.net_graph(device)
+    rc = torch.zeros(capacity * g.nodes * 4, dtype=torch.float32, device=dev)
+    zc = torch.zeros_like(rc)
+    solver.net_record(rc, zc, capacity, every)
+    x.zero_()
+    st = solver.solve_linear_system(rows, cols, blocks, b, x)
+    n = solver.net_recorded()
+    solver.net_record(rc, zc, 0, 1)
+    return Dataset(g, rc.view(capacity, g.nodes, 4)[:n].contiguous(), zc.view(capacity, g.nodes, 4)[:n].contiguous(), n), st
+
+
+def train(trainer: Trainer, data: List[Dataset], steps: int, batch: int = 16, lr: float = 1e-3, seed: int = 0,
+          log_every: int = 0) -> list:
+    """Minibatch Adam over the datasets (one dataset per step, round robin; random samples)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    hist = []
+    for it in range(steps):
+        d = data[it % len(data)]
+        k = min(batch, d.samples)
+        idx = torch.from_numpy(rng.choice(d.samples, size=k, replace=False)).to(d.rc.device)
+        loss = trainer.step(d.graph, d.rc[idx].contiguous(), d.zc[idx].contiguous(), k, lr)
+        if log_every and (it % log_every == 0 or it == steps - 1):
+            hist.append((it, float(loss.mean())))
+    return hist

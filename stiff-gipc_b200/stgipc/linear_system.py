@@ -192,6 +192,45 @@ class Solver:
         return dict(fine_mask=fine, prefix_orig=pref, coarse_tables=ct.reshape(L, V), going_next=gn,
                     coarse_table=tab.reshape(V, max(L - 1, 1)), level_size=ls)
 
+    # -- learned coarse correction (stg_net_*) ---------------------------------------------
+    def net_configure(self, level: int):
+        """Coarse level of the network; the next MAS assembly builds its graph."""
+        check(_L.lib().stg_net_configure(self.h, int(level)), "stg_net_configure")
+
+    def net_graph(self, device="cuda"):
+        """The level's graph (learned.NetGraph) exported to new device tensors."""
+        import torch
+        from .learned import NetGraph
+        n, e = C.c_int(), C.c_int()
+        check(_L.lib().stg_net_graph_info(self.h, C.byref(n), C.byref(e)), "stg_net_graph_info")
+        n, e = n.value, e.value
+        dev = torch.device(device)
+        row = torch.zeros(n + 1, dtype=torch.int32, device=dev)
+        col = torch.zeros(max(e, 1), dtype=torch.int32, device=dev)
+        w = torch.zeros(max(e, 1), dtype=torch.float32, device=dev)
+        oblk = torch.zeros(max(e, 1) * 9, dtype=torch.float32, device=dev)
+        dblk = torch.zeros(n * 9, dtype=torch.float32, device=dev)
+        feat = torch.zeros(n, dtype=torch.float32, device=dev)
+        check(_L.lib().stg_net_export_graph(self.h, _ptr(row), _ptr(col), _ptr(w), _ptr(oblk), _ptr(dblk), _ptr(feat)),
+              "stg_net_export_graph")
+        torch.cuda.synchronize(dev)
+        return NetGraph(n, e, row, col, w, oblk, dblk, feat)
+
+    def net_record(self, rc, zc, capacity: int, every: int):
+        """Record (r_c, z_c) of the level every `every` iterations of the following solves."""
+        _require_cuda(rc, zc)
+        check(_L.lib().stg_net_record(self.h, _ptr(rc), _ptr(zc), int(capacity), int(every)), "stg_net_record")
+        self._rec = (rc, zc)
+
+    def net_recorded(self) -> int:
+        c = C.c_int()
+        check(_L.lib().stg_net_recorded(self.h, C.byref(c)), "stg_net_recorded")
+        return c.value
+
+    def net_set_params(self, params):
+        _require_cuda(params)
+        check(_L.lib().stg_net_set_params(self.h, _ptr(params)), "stg_net_set_params")
+
     def profile_spmv(self, reps: int = 50):
         """(mean ms per PCG SpMV launch, algorithmic bytes per launch) on the last solve."""
         ms, by = C.c_float(), C.c_double()

@@ -70,13 +70,28 @@ def test_missing_library_fails_loudly(tmp_path, monkeypatch):
         _lib.lib()
 
 
-def test_learned_flag_rejected_before_device(L):
-    """The learned coarse correction is not built: asking for it is an error, not a silent
-    plain solve."""
+def test_learned_flag_validated_before_device(L):
+    """The learned coarse correction needs MAS and a host or graph loop; other values and
+    combinations are errors before any device work, not a silent plain solve."""
     from stgipc import _lib
     h = C.c_void_p()
-    c = _lib.Config()
-    L.stg_config_default(C.byref(c))
-    c.learned = 1
-    assert L.stg_create(C.byref(c), C.byref(h)) == _lib.STG_ERR_INVALID
-    assert b"learned" in L.stg_last_error()
+    for learned, pre, loop in ((2, _lib.PRECOND["mas"], _lib.LOOP["graph"]),
+                               (1, _lib.PRECOND["diag"], _lib.LOOP["graph"]),
+                               (1, _lib.PRECOND["mas"], _lib.LOOP["persistent"])):
+        c = _lib.Config()
+        L.stg_config_default(C.byref(c))
+        c.learned, c.preconditioner, c.loop_mode = learned, pre, loop
+        assert L.stg_create(C.byref(c), C.byref(h)) == _lib.STG_ERR_INVALID
+        assert b"learned" in L.stg_last_error()
+
+
+def test_net_training_entry_points_validate(L):
+    """stg_net_* handle-free calls reject bad arguments without touching a device."""
+    from stgipc import _lib
+    assert L.stg_net_scratch_bytes(0, 1) == 0
+    assert L.stg_net_scratch_bytes(100, 2) > 0
+    assert L.stg_net_train_step(None, None, None, 1, None, None, None, None, 1, 0.0, None, None, 0, None) == \
+        _lib.STG_ERR_INVALID
+    g = _lib.NetGraphC()
+    assert L.stg_net_forward(C.byref(g), None, None, 1, None, None, None, 0, None) == _lib.STG_ERR_INVALID
+    assert L.stg_net_configure(None, 1) == _lib.STG_ERR_INVALID
