@@ -275,6 +275,12 @@ size_t stg_net_scratch_bytes(int nodes, int samples);
 /* delta [samples][nodes][4] = the network's output d for samples rc / zc. */
 int stg_net_forward(const stg_net_graph* g, const float* rc, const float* zc, int samples, const float* params,
                     float* delta, void* scratch, size_t scratch_bytes, void* stream);
+/* The in-loop application on one sample, in place: z += theta s_z d(rc, z), theta <= 1 the
+ * largest step that keeps rc.z at least half its value before.  The fused single-launch
+ * kernel (one thread-block cluster) when the graph fits it, else the layered kernels;
+ * *fused (may be NULL) receives the cluster size used, 0 for the layered kernels. */
+int stg_net_apply(const stg_net_graph* g, const float* rc, float* z, const float* params, void* scratch,
+                  size_t scratch_bytes, int* fused, void* stream);
 /* One step: loss[s] = J(z + s_z d) / |J(z)| per sample (J(v) = v.A v / 2 - v.r), grad =
  * gradient of the mean loss; with lr > 0 an Adam step (beta 0.9 / 0.999, eps 1e-8, bias
  * corrections of step `step` >= 1) on params with moments m, v.  All device pointers. */

@@ -669,3 +669,34 @@ int stg_net_train_step(const stg_net_graph* g, const float* rc, const float* zc,
         return STG_OK;
     })
 }
+
+int stg_net_apply(const stg_net_graph* g, const float* rc, float* z, const float* params, void* scratch,
+                  size_t scratch_bytes, int* fused, void* stream)
+{
+    GUARD({
+        stg::NetGraph G;
+        STG_TRY(net_graph_of(g, G));
+        if(!rc || !z || !params)
+        {
+            stg::set_error("stg_net_apply: invalid arguments");
+            return STG_ERR_INVALID;
+        }
+        stg::NetBuffers b;
+        STG_TRY(stg::net_carve(scratch, scratch_bytes, G.n, 1, b));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        std::vector<int> row(G.n + 1);
+        STG_CUDA_TRY(cudaMemcpyAsync(row.data(), G.row, sizeof(int) * (G.n + 1), cudaMemcpyDeviceToHost, s));
+        STG_CUDA_TRY(cudaStreamSynchronize(s));
+        int cl = 0, rpc = 0;
+        STG_TRY(stg::net_fused_plan(row.data(), G.n, &cl, &rpc));
+        STG_TRY(stg::net_prepare());
+        STG_TRY(stg::net_to_bf16(s, params, b.wbf));
+        int l = 0;
+        if(cl > 0)
+            STG_TRY(stg::net_forward_fused(s, G, nullptr, rc, z, b.wbf, params, nullptr, cl, rpc));
+        else
+            STG_TRY(stg::net_forward(s, G, rc, z, 1, b, b.wbf, params, z, nullptr, &l));
+        if(fused) *fused = cl;
+        return STG_OK;
+    })
+}

@@ -9,6 +9,7 @@
 #include "reduce.cuh"
 #include "solver.hpp"
 
+#include <cooperative_groups.h>
 #include <cuda_bf16.h>
 
 namespace stg
@@ -171,6 +172,16 @@ __global__ void k_ng_finish(const double* __restrict__ ublk, int n, const int* _
     }
 }
 
+// neighbour entries packed for the fused kernel: (owner rank << 16 | row in the owner, w)
+__global__ void k_ng_pack(const int* __restrict__ col, const float* __restrict__ w, int nnz, int rpc, int2* out)
+{
+    for(int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += gridDim.x * blockDim.x)
+    {
+        const int j = col[e], o = j / rpc;
+        out[e] = make_int2((o << 16) | (j - o * rpc), __float_as_int(w[e]));
+    }
+}
+
 // f_i = log(trace A_ii) minus its mean over the level (one CTA of 1024 threads)
 __global__ void __launch_bounds__(1024) k_ng_feat(const float* __restrict__ dblk, int n, float* feat)
 {
@@ -235,6 +246,18 @@ int net_build_graph(cudaStream_t s, NetGraphStore& G, int n, int nnzu, const int
     k_ng_feat<<<1, 1024, 0, s>>>(G.dblk.data(), n, G.feat.data());
     STG_LAUNCH_CHECK();
     (*launches) += 2;
+    std::vector<int> hrow(n + 1);
+    STG_CUDA_TRY(cudaMemcpyAsync(hrow.data(), G.row.data(), sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
+    STG_CUDA_TRY(cudaStreamSynchronize(s));
+    STG_TRY(net_fused_plan(hrow.data(), n, &G.fu_cl, &G.fu_rpc));
+    if(G.fu_cl > 0 && nnz > 0)
+    {
+        STG_TRY(G.fu_nb.resize(nnz));
+        k_ng_pack<<<std::max(1, std::min(div_up(nnz, NT), kSMs * 4)), NT, 0, s>>>(G.col.data(), G.w.data(), nnz, G.fu_rpc,
+                                                                                  G.fu_nb.data());
+        STG_LAUNCH_CHECK();
+        (*launches)++;
+    }
     return 0;
 }
 
@@ -696,6 +719,336 @@ int net_record(cudaStream_t s, const float* R, const float* Z, int n, const doub
 }
 
 // ---------------------------------------------------------------------------------------
+// fused in-loop forward: the whole network in one launch of one thread-block cluster
+// ---------------------------------------------------------------------------------------
+namespace cg = cooperative_groups;
+
+constexpr int FU_THREADS = 512;   // 16 warps
+constexpr int FU_RPC = 128;       // max rows (level nodes) per CTA
+constexpr int FU_EPC = 4096;      // max neighbour entries per CTA
+constexpr int FU_HS = 2 * FU_RPC * NET_H * 2;          // own rows' h, double-buffered, bf16
+constexpr int FU_XS = FU_RPC * XS_LD * 2;              // [h, m] tiles, bf16
+constexpr int FU_WS = NET_H * XS_LD * 2;               // staged W_k, bf16
+constexpr int FU_NB = FU_EPC * 8;                      // (owner rank << 16 | local row, w) per entry
+constexpr int FU_DL = FU_RPC * 16;                     // d, float4 per row
+constexpr int FU_RP = (FU_RPC + 4) * 4;                // own rows' entry offsets
+constexpr int FU_RZ = 2 * FU_RPC * 16;                  // own rows' r and z
+constexpr int FU_RED = 512;                             // block sums [32], cluster partials, scales
+constexpr int FU_SMEM = FU_HS + FU_XS + FU_WS + FU_NB + FU_DL + FU_RED + FU_RP + FU_RZ;
+
+namespace
+{
+// two deterministic block sums at once (result valid in thread 0)
+__device__ __forceinline__ void block_sum2_fu(double& x, double& y, double* red)
+{
+    x = warp_sum(x);
+    y = warp_sum(y);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if(lane == 0)
+    {
+        red[warp] = x;
+        red[16 + warp] = y;
+    }
+    __syncthreads();
+    if(threadIdx.x < 32)
+    {
+        x = warp_sum(lane < FU_THREADS / 32 ? red[lane] : 0.0);
+        y = warp_sum(lane < FU_THREADS / 32 ? red[16 + lane] : 0.0);
+    }
+}
+
+// lane q of warp 0 fetches CTA q's pair at red[slot], lane 0 sums them in rank order
+__device__ __forceinline__ void cluster_sum2(cg::cluster_group& cluster, double* red, int slot, int nranks,
+                                             double& a, double& b)
+{
+    const int lane = threadIdx.x & 31;
+    double va = 0, vb = 0;
+    if(lane < nranks)
+    {
+        const double* rq = cluster.map_shared_rank(red, lane);
+        va = rq[slot];
+        vb = rq[slot + 1];
+    }
+    a = 0;
+    b = 0;
+    for(int q = 0; q < nranks; q++)
+    {
+        a += __shfl_sync(0xffffffffu, va, q);
+        b += __shfl_sync(0xffffffffu, vb, q);
+    }
+}
+
+__device__ __forceinline__ unsigned smem_addr(const void* p)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+// 16-byte load from the shared memory of CTA `rank` of the cluster at this CTA's offset `a`
+__device__ __forceinline__ uint4 ld_dsmem16(unsigned a, int rank)
+{
+    unsigned r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    uint4 v;
+    asm volatile("ld.shared::cluster.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "r"(r)
+                 : "memory");
+    return v;
+}
+
+// W_k ([64][128] bf16) into shared memory rows of XS_LD with 16-byte asynchronous copies
+__device__ __forceinline__ void stage_weights_async(const __nv_bfloat16* W, __nv_bfloat16* Ws)
+{
+    for(int i = threadIdx.x; i < NET_H * 2 * NET_H / 8; i += FU_THREADS)
+    {
+        const int o = (8 * i) / (2 * NET_H), k = (8 * i) % (2 * NET_H);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(Ws + o * XS_LD + k)),
+                     "l"(W + 8 * (size_t)i)
+                     : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void fma8(float (&a)[8], float w, uint4 v)
+{
+    const float2 f0 = unpack_bf16(v.x), f1 = unpack_bf16(v.y), f2 = unpack_bf16(v.z), f3 = unpack_bf16(v.w);
+    a[0] = fmaf(w, f0.x, a[0]);
+    a[1] = fmaf(w, f0.y, a[1]);
+    a[2] = fmaf(w, f1.x, a[2]);
+    a[3] = fmaf(w, f1.y, a[3]);
+    a[4] = fmaf(w, f2.x, a[4]);
+    a[5] = fmaf(w, f2.y, a[5]);
+    a[6] = fmaf(w, f3.x, a[6]);
+    a[7] = fmaf(w, f3.y, a[7]);
+}
+
+// The network of learned.cuh for one sample, rows split over the cluster's CTAs in
+// contiguous ranges of rpc rows; a CTA keeps its rows' activations in shared memory and
+// reads its neighbours' from the owning CTA (distributed shared memory).  The order of every
+// sum matches the layered kernels except the RMS scales (CTA partials summed in rank order).
+// nbp: the neighbour entries packed as (owner rank << 16 | row in the owner, w) (graph
+// build), or null (packed here from col / w).
+__global__ void __launch_bounds__(FU_THREADS) k_net_fused(NetGraph g, const int2* __restrict__ nbp,
+                                                         const float* __restrict__ rc, float* Z,
+                                                         const __nv_bfloat16* __restrict__ wbf,
+                                                         const float* __restrict__ params, const int* flags, int rpc)
+{
+    if(net_gated(flags)) return;  // uniform over the cluster: nothing changes the flags meanwhile
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank(), nranks = (int)cluster.num_blocks();
+    extern __shared__ __align__(16) unsigned char fu_smem[];
+    __nv_bfloat16* Hs = reinterpret_cast<__nv_bfloat16*>(fu_smem);
+    __nv_bfloat16* Xs = reinterpret_cast<__nv_bfloat16*>(fu_smem + FU_HS);
+    __nv_bfloat16* Ws = reinterpret_cast<__nv_bfloat16*>(fu_smem + FU_HS + FU_XS);
+    int2* nb = reinterpret_cast<int2*>(fu_smem + FU_HS + FU_XS + FU_WS);
+    float4* dl = reinterpret_cast<float4*>(fu_smem + FU_HS + FU_XS + FU_WS + FU_NB);
+    double* red = reinterpret_cast<double*>(fu_smem + FU_HS + FU_XS + FU_WS + FU_NB + FU_DL);  // [32] block sums
+    int* rp = reinterpret_cast<int*>(fu_smem + FU_HS + FU_XS + FU_WS + FU_NB + FU_DL + FU_RED);
+    float4* rz = reinterpret_cast<float4*>(fu_smem + FU_HS + FU_XS + FU_WS + FU_NB + FU_DL + FU_RED + FU_RP);  // [2][rpc]
+    double* part = red + 32;                         // [4]: cluster partials read by the other CTAs
+    float* sc = reinterpret_cast<float*>(red + 36);  // s_r, s_z, theta
+    const int n = g.n, r0 = min(rank * rpc, n), own = max(0, min(rpc, n - r0));
+    const int tiles = (own + 15) / 16;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = FU_THREADS / 32;
+
+    // ---- P0: layer-0 weights (async), neighbour lists, own r / z, the RMS scales ----
+    stage_weights_async(wbf + P_W1, Ws);
+    const int e_base = g.row[r0], e_end = g.row[r0 + own];
+    for(int i = threadIdx.x; i <= own; i += FU_THREADS) rp[i] = g.row[r0 + i] - e_base;
+    if(nbp)
+    {
+#pragma unroll 4
+        for(int e = e_base + threadIdx.x; e < e_end; e += FU_THREADS) nb[e - e_base] = nbp[e];
+    }
+    else
+        for(int e = e_base + threadIdx.x; e < e_end; e += FU_THREADS)
+        {
+            const int j = g.col[e], o = j / rpc;
+            nb[e - e_base] = make_int2((o << 16) | (j - o * rpc), __float_as_int(g.w[e]));
+        }
+    double rr = 0, zz = 0;
+    for(int i = threadIdx.x; i < own; i += FU_THREADS)
+    {
+        const float4 a = *reinterpret_cast<const float4*>(rc + 4 * (size_t)(r0 + i));
+        const float4 b = *reinterpret_cast<const float4*>(Z + 4 * (size_t)(r0 + i));
+        rz[i] = a;
+        rz[FU_RPC + i] = b;
+        rr += (double)a.x * a.x + (double)a.y * a.y + (double)a.z * a.z;
+        zz += (double)b.x * b.x + (double)b.y * b.y + (double)b.z * b.z;
+    }
+    block_sum2_fu(rr, zz, red);
+    if(threadIdx.x == 0)
+    {
+        part[0] = rr;
+        part[1] = zz;
+    }
+    cluster.sync();
+    if(warp == 0)
+    {
+        double sr, sz;
+        cluster_sum2(cluster, part, 0, nranks, sr, sz);
+        if(lane == 0)
+        {
+            const float fr = n > 0 ? (float)sqrt(sr / n) : 0.f, fz = n > 0 ? (float)sqrt(sz / n) : 0.f;
+            sc[0] = fr > 0.f ? fr : 1.f;
+            sc[1] = fz > 0.f ? fz : 1.f;
+        }
+    }
+    __syncthreads();
+    const float s_r = sc[0], s_z = sc[1];
+
+    // ---- P1: input rows (bf16, in the X tiles' first 16 columns) and the embedding ----
+    {
+        const float ir = 1.f / s_r, iz = 1.f / s_z;
+        for(int i = threadIdx.x; i < tiles * 16; i += FU_THREADS)
+        {
+            uint4 lo = make_uint4(0u, 0u, 0u, 0u);
+            if(i < own)
+            {
+                const float4 a = rz[i], b = rz[FU_RPC + i];
+                lo.x = pack_bf16(a.x * ir, a.y * ir);
+                lo.y = pack_bf16(a.z * ir, b.x * iz);
+                lo.z = pack_bf16(b.y * iz, b.z * iz);
+                lo.w = pack_bf16(g.feat[r0 + i], 1.f);
+            }
+            *reinterpret_cast<uint4*>(Xs + i * XS_LD) = lo;
+            *reinterpret_cast<uint4*>(Xs + i * XS_LD + 8) = make_uint4(0u, 0u, 0u, 0u);
+        }
+        __syncthreads();
+        if(warp < tiles)
+        {
+            float acc[8][4] = {};
+            warp_gemm<NET_IN, 8>(Xs + warp * 16 * XS_LD, XS_LD, wbf + P_W0, NET_IN, acc);
+            store_relu(acc, params + P_B0, Hs, warp * 16);  // buffer 0, row stride 64
+        }
+    }
+    cluster.sync();
+
+    // ---- P2: three message-passing layers ----
+    int cur = 0;
+    for(int k = 0; k < NET_LAYERS; k++)
+    {
+        const __nv_bfloat16* Hc = Hs + cur * FU_RPC * NET_H;
+        const unsigned hbase = smem_addr(Hc);
+        // gather: 4 rows per warp at a time, 8 lanes per row, 8 channels (16 bytes) per lane;
+        // the neighbour rows are fetched 8 at a time, summed in entry order
+        const int sub = lane >> 3, q = lane & 7;
+        for(int base = warp * 4; base < tiles * 16; base += nwarps * 4)
+        {
+            const int i = base + sub;
+            uint4 self = make_uint4(0u, 0u, 0u, 0u), msg = make_uint4(0u, 0u, 0u, 0u);
+            if(i < own)
+            {
+                float a[8] = {};
+                const int eb = rp[i], ee = rp[i + 1];
+                for(int e = eb; e < ee; e += 8)
+                {
+                    uint4 v[8];
+                    float w[8];
+#pragma unroll
+                    for(int u = 0; u < 8; u++)
+                    {
+                        const int2 t = nb[min(e + u, ee - 1)];
+                        w[u] = e + u < ee ? __int_as_float(t.y) : 0.f;
+                        v[u] = ld_dsmem16(hbase + ((t.x & 0xffff) * NET_H + 8 * q) * 2, t.x >> 16);
+                    }
+#pragma unroll
+                    for(int u = 0; u < 8; u++)
+                        if(e + u < ee) fma8(a, w[u], v[u]);
+                }
+                self = *reinterpret_cast<const uint4*>(Hc + i * NET_H + 8 * q);
+                msg = make_uint4(pack_bf16(a[0], a[1]), pack_bf16(a[2], a[3]), pack_bf16(a[4], a[5]), pack_bf16(a[6], a[7]));
+            }
+            *reinterpret_cast<uint4*>(Xs + i * XS_LD + 8 * q) = self;
+            *reinterpret_cast<uint4*>(Xs + i * XS_LD + NET_H + 8 * q) = msg;
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncthreads();
+        if(warp < tiles)
+        {
+            float acc[8][4] = {};
+            warp_gemm<2 * NET_H, 8>(Xs + warp * 16 * XS_LD, XS_LD, Ws, XS_LD, acc);
+            store_relu(acc, params + P_B1 + k * NET_H, Hs + (cur ^ 1) * FU_RPC * NET_H, warp * 16);
+        }
+        cur ^= 1;
+        __syncthreads();  // Ws is free again
+        if(k + 1 < NET_LAYERS) stage_weights_async(wbf + P_W1 + (k + 1) * NET_H * 2 * NET_H, Ws);
+        // the new rows are visible to the cluster, and nobody reads the old buffer any more
+        cluster.sync();
+    }
+
+    // ---- P3: head, the step limit theta over the cluster, apply ----
+    const float* bo = params + P_BO;
+    if(warp < tiles)
+    {
+        float acc[1][4] = {};
+        warp_gemm<NET_H, 1>(Hs + cur * FU_RPC * NET_H + warp * 16 * NET_H, NET_H, wbf + P_WO, NET_H, acc);
+        const int gq = lane >> 2, t = lane & 3;
+        if(t < 2)
+        {
+            float* d0 = reinterpret_cast<float*>(dl + warp * 16 + gq);
+            float* d1 = reinterpret_cast<float*>(dl + warp * 16 + gq + 8);
+            if(t == 0)
+            {
+                d0[0] = acc[0][0] + bo[0];
+                d0[1] = acc[0][1] + bo[1];
+                d1[0] = acc[0][2] + bo[0];
+                d1[1] = acc[0][3] + bo[1];
+            }
+            else
+            {
+                d0[2] = acc[0][0] + bo[2];
+                d0[3] = 0.f;
+                d1[2] = acc[0][2] + bo[2];
+                d1[3] = 0.f;
+            }
+        }
+    }
+    __syncthreads();
+    double pa = 0, pb = 0;
+    for(int i = threadIdx.x; i < own; i += FU_THREADS)
+    {
+        const float4 r = rz[i], z = rz[FU_RPC + i], d = dl[i];
+        pa += (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z;
+        pb += (double)r.x * d.x + (double)r.y * d.y + (double)r.z * d.z;
+    }
+    block_sum2_fu(pa, pb, red);
+    if(threadIdx.x == 0)
+    {
+        part[2] = pa;
+        part[3] = pb;
+    }
+    cluster.sync();
+    if(warp == 0)
+    {
+        double a, b;
+        cluster_sum2(cluster, part, 2, nranks, a, b);
+        if(lane == 0)
+        {
+            b *= s_z;
+            float th = (b < -0.5 * a && b < 0.0) ? (float)(-0.5 * a / b) : 1.f;
+            if(!(th >= 0.f)) th = 0.f;
+            sc[2] = th;
+        }
+    }
+    // nobody reads another CTA's shared memory after this point
+    cluster.sync();
+    const float f = sc[2] * s_z;
+    for(int i = threadIdx.x; i < own; i += FU_THREADS)
+    {
+        float4 z = rz[FU_RPC + i];
+        const float4 d = dl[i];
+        z.x = fmaf(f, d.x, z.x);
+        z.y = fmaf(f, d.y, z.y);
+        z.z = fmaf(f, d.z, z.z);
+        *reinterpret_cast<float4*>(Z + 4 * (size_t)(r0 + i)) = z;
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------
 namespace
@@ -795,6 +1148,71 @@ int net_to_bf16(cudaStream_t s, const float* params, void* wbf)
 {
     k_net_bf16<<<div_up(P_COUNT, NT), NT, 0, s>>>(params, reinterpret_cast<__nv_bfloat16*>(wbf), P_COUNT);
     STG_LAUNCH_CHECK();
+    return 0;
+}
+
+// Cluster size and rows per CTA for the fused forward on a graph with row pointers `row`
+// (host copy): the largest cluster (16, else 8) that can be resident, with at most FU_RPC
+// rows and FU_EPC neighbour entries per CTA.  cl = 0: use the layered kernels.
+int net_fused_plan(const int* row, int n, int* cl, int* rpc)
+{
+    *cl = 0;
+    *rpc = 0;
+    STG_CUDA_TRY(cudaFuncSetAttribute(k_net_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, FU_SMEM));
+    STG_CUDA_TRY(cudaFuncSetAttribute(k_net_fused, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    for(int c : {16, 8})
+    {
+        const int r = (div_up(n, c) + 15) / 16 * 16;
+        if(r > FU_RPC) continue;
+        bool fits = true;
+        for(int q = 0; q < c && fits; q++)
+        {
+            const int a = std::min(q * r, n), b = std::min(a + r, n);
+            fits = row[b] - row[a] <= FU_EPC;
+        }
+        if(!fits) continue;
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = c;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(c);
+        cfg.blockDim = dim3(FU_THREADS);
+        cfg.dynamicSmemBytes = FU_SMEM;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if(cudaOccupancyMaxActiveClusters(&clusters, k_net_fused, &cfg) != cudaSuccess)
+        {
+            cudaGetLastError();
+            continue;
+        }
+        if(clusters < 1) continue;
+        *cl = c;
+        *rpc = r;
+        return 0;
+    }
+    return 0;
+}
+
+int net_forward_fused(cudaStream_t s, const NetGraph& g, const int2* nbp, const float* rc, float* Z, const void* wbf,
+                      const float* params, const int* flags, int cl, int rpc)
+{
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(cl);
+    cfg.blockDim = dim3(FU_THREADS);
+    cfg.dynamicSmemBytes = FU_SMEM;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    STG_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_net_fused, g, nbp, rc, Z, reinterpret_cast<const __nv_bfloat16*>(wbf),
+                                    params, flags, rpc));
     return 0;
 }
 

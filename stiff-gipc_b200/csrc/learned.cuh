@@ -88,10 +88,11 @@ int net_record(cudaStream_t s, const float* R, const float* Z, int n, const doub
 struct NetGraphStore
 {
     int level = 0, n = 0, nnz = 0;
+    int fu_cl = 0, fu_rpc = 0;    // fused forward: cluster size and rows per CTA (0: layered)
     DBuf<int> row, col, cnt, cur;
     DBuf<float> w, oblk, dblk, feat;
     DBuf<long long> key;
-    DBuf<double> tmp;
+    DBuf<int2> fu_nb;             // neighbour entries packed for the fused forward
     NetGraph view() const
     {
         NetGraph g;
@@ -108,5 +109,9 @@ struct NetGraphStore
 };
 int net_build_graph(cudaStream_t s, NetGraphStore& G, int n, int nnzu, const int* urow, const int* ucol,
                     const double* ublk, int* launches);
+// the fused single-launch forward + apply (one thread-block cluster, see k_net_fused)
+int net_fused_plan(const int* row, int n, int* cl, int* rpc);
+int net_forward_fused(cudaStream_t s, const NetGraph& g, const int2* nbp, const float* rc, float* Z, const void* wbf,
+                      const float* params, const int* flags, int cl, int rpc);
 
 }  // namespace stg

@@ -1663,7 +1663,13 @@ static int launch_learned(Solver& S, const PcgDev& c)
                            Ls.rec_cap, Ls.rec_every));
         S.launches++;
     }
-    if(c.net_mode & 1)
+    if((c.net_mode & 1) && Ls.graph.fu_cl > 0)
+    {
+        STG_TRY(net_forward_fused(S.stream, Ls.graph.view(), Ls.graph.nnz > 0 ? Ls.graph.fu_nb.data() : nullptr, R, Z,
+                                  Ls.wbf.data(), Ls.params.data(), c.flags, Ls.graph.fu_cl, Ls.graph.fu_rpc));
+        S.launches++;
+    }
+    else if(c.net_mode & 1)
         STG_TRY(net_forward(S.stream, Ls.graph.view(), R, Z, 1, Ls.buf, Ls.wbf.data(), Ls.params.data(), Z, c.flags,
                             &S.launches));
     return 0;

@@ -107,6 +107,7 @@ def lib():
     L.stg_net_set_params.argtypes = [vp, vp]
     L.stg_net_scratch_bytes.argtypes = [ci, ci]
     L.stg_net_forward.argtypes = [C.POINTER(NetGraphC), vp, vp, ci, vp, vp, vp, C.c_size_t, vp]
+    L.stg_net_apply.argtypes = [C.POINTER(NetGraphC), vp, vp, vp, vp, C.c_size_t, C.POINTER(ci), vp]
     L.stg_net_train_step.argtypes = [C.POINTER(NetGraphC), vp, vp, ci, vp, vp, vp, vp, ci, C.c_float, vp, vp,
                                      C.c_size_t, vp]
     for name in header_symbols():

@@ -83,6 +83,18 @@ def forward(graph: NetGraph, rc, zc, params, samples: int, stream=None, buf=None
     return delta.view(samples, graph.nodes, 4)
 
 
+def apply(graph: NetGraph, rc, z, params, stream=None, buf=None) -> int:
+    """In place z += theta s_z d(rc, z) for one sample (rc, z: [nodes][4] FP32), as inside the
+    PCG loop.  Returns the cluster size of the fused kernel used (0: layered kernels)."""
+    buf = buf if buf is not None else scratch(graph.nodes, 1, rc.device)
+    fused = C.c_int()
+    s = None if stream is None else stream.cuda_stream
+    g = graph.c()
+    check(_L.lib().stg_net_apply(C.byref(g), _ptr(rc), _ptr(z), _ptr(params), _ptr(buf), buf.numel(),
+                                 C.byref(fused), s), "stg_net_apply")
+    return fused.value
+
+
 class Trainer:
     """Adam on the library's kernels; params / moments / gradient are FP32 device tensors."""
 
@@ -152,8 +164,9 @@ def record_samples(solver, sysm, capacity: int = 256, every: int = 1, device="cu
 
 
 def train(trainer: Trainer, data: List[Dataset], steps: int, batch: int = 16, lr: float = 1e-3, seed: int = 0,
-          log_every: int = 0) -> list:
-    """Minibatch Adam over the datasets (one dataset per step, round robin; random samples)."""
+          log_every: int = 0, lr_final: Optional[float] = None) -> list:
+    """Minibatch Adam over the datasets (one dataset per step, round robin; random samples);
+    the step size decays from lr to lr_final on a cosine when lr_final is given."""
     import torch
     rng = np.random.default_rng(seed)
     hist = []
@@ -161,7 +174,8 @@ def train(trainer: Trainer, data: List[Dataset], steps: int, batch: int = 16, lr
         d = data[it % len(data)]
         k = min(batch, d.samples)
         idx = torch.from_numpy(rng.choice(d.samples, size=k, replace=False)).to(d.rc.device)
-        loss = trainer.step(d.graph, d.rc[idx].contiguous(), d.zc[idx].contiguous(), k, lr)
+        a = lr if lr_final is None else lr_final + 0.5 * (lr - lr_final) * (1 + np.cos(np.pi * it / max(steps - 1, 1)))
+        loss = trainer.step(d.graph, d.rc[idx].contiguous(), d.zc[idx].contiguous(), k, a)
         if log_every and (it % log_every == 0 or it == steps - 1):
             hist.append((it, float(loss.mean())))
     return hist

@@ -192,3 +192,36 @@ def test_fallback_to_plain_mas(dev):
     st, _ = _solve(solver, s, dev)
     assert st["status"] == 0 and st["rel_residual"] <= 1.2e-4
     assert st["learned_rejected"] == 1
+
+
+@pytest.mark.parametrize("level", [1, 2])
+def test_fused_apply_matches_layered_forward(dev, level):
+    """The single-launch cluster kernel (the in-loop path) against the layered forward:
+    z + theta s_z d with theta from the layered d."""
+    import torch
+    from stgipc import learned
+    s = cube_system(12)
+    solver = _solver(s, level, dev)
+    _solve(solver, s, dev)
+    G = solver.net_graph()
+    rng = np.random.default_rng(21)
+    n = G.nodes
+    r = np.zeros((n, 4), np.float32)
+    r[:, :3] = rng.standard_normal((n, 3))
+    z = np.zeros((n, 4), np.float32)
+    z[:, :3] = r[:, :3] * rng.uniform(0.5, 2.0, (n, 1))
+    p = learned.init_params(3, head_scale=0.3)
+    P = _t(p, dev)
+    d = learned.forward(G, _t(r, dev), _t(z, dev), P, 1)[0].cpu().numpy().astype(np.float64)
+    sz = np.sqrt((z[:, :3].astype(np.float64) ** 2).sum() / n)
+    a = (r[:, :3] * z[:, :3]).astype(np.float64).sum()
+    b = sz * (r[:, :3] * d[:, :3]).sum()
+    th = -0.5 * a / b if b < -0.5 * a else 1.0
+    want = z[:, :3] + th * sz * d[:, :3]
+    zt = _t(z, dev)
+    cl = learned.apply(G, _t(r, dev), zt, P)
+    got = zt.cpu().numpy()
+    assert cl in (8, 16), "the level fits the fused kernel"
+    corr = want - z[:, :3]
+    assert np.linalg.norm(got[:, :3] - want) <= 5e-3 * np.linalg.norm(corr) + 1e-7
+    assert np.all(got[:, 3] == 0)
