@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--loop", choices=["host", "graph", "persistent"], default="graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-correction solves")
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     return ap.parse_args()
 
@@ -381,6 +382,33 @@ def main():
     h2d = sum(t.numel() * t.element_size() for t in (h_rows, h_cols, h_blocks, h_b))
     d2h = h_x.numel() * h_x.element_size()
 
+    # the learned coarse correction (shipped network, held-out scene) inside the FP32 and
+    # FP64 flexible PCG: iterations and device time beside the plain solves above
+    learned_line = None
+    if args.workload == "hetcube48" and not args.no_learned:
+        from stgipc import learned
+        wpath = learned.default_weights()
+        if os.path.exists(wpath):
+            params, level, meta = learned.load_weights(wpath)
+            P = torch.from_numpy(params).to(dev)
+            learned_line = {"weights": os.path.relpath(wpath, ROOT), "level": level, "train_seeds": meta["seeds"],
+                            "train_samples": meta["samples"]}
+            for prec in ("fp32", "fp64"):
+                cfg = PCGSolverConfig(bank_size=16, precision=prec, stop_rule="relative_residual", global_tol_rate=1e-4,
+                                      refine_interval=args.refine, loop=args.loop, graph_batch=args.batch,
+                                      max_iter_ratio=0.3, learned=True)
+                ls = Solver(cfg, stream=stream)
+                ls.mas_init(sysm.num_verts, sysm.neighbor_start, sysm.neighbor_num, sysm.neighbor_list, pm, rm)
+                ls.net_configure(level)
+                ls.net_set_params(P)
+                for _ in range(max(1, args.warmup)):
+                    solve(ls)
+                st_l = ls.solve_linear_system(rows, cols, blocks, b, x)
+                ms_l = timed(ls, max(1, args.steps // 2))
+                learned_line[prec] = {"ms": ms_l, "iterations": st_l["iterations"], "rel_residual": st_l["rel_residual"],
+                                      "accepted": st_l["learned_accepted"], "rejected": st_l["learned_rejected"]}
+                ls.close()
+
     # roofline of the dominant kernel: the PCG SpMV of the FP32 path, timed live
     solve(fast)
     spmv_ms, spmv_bytes = fast.profile_spmv(reps=100)
@@ -433,6 +461,7 @@ def main():
                          "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650"},
             "cpu_baseline": cpu,
             "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "learned": learned_line,
             "gpu_launches": int(st_fast["kernel_launches"] * args.steps),
             "clocks": clk.summary(),
         }

@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
+import os
 from typing import List, Optional
 
 import numpy as np
@@ -179,3 +180,73 @@ def train(trainer: Trainer, data: List[Dataset], steps: int, batch: int = 16, lr
         if log_every and (it % log_every == 0 or it == steps - 1):
             hist.append((it, float(loss.mean())))
     return hist
+
+
+WEIGHTS = os.path.join(os.path.dirname(__file__), "weights")
+
+
+def default_weights(level: int = 2, n: int = 48) -> str:
+    return os.path.join(WEIGHTS, f"net_hetcube{n}_L{level}.npz")
+
+
+def load_weights(path: str):
+    """(params FP32 [STG_NET_PARAMS], level, metadata dict) from a file ``train`` wrote."""
+    z = np.load(path, allow_pickle=False)
+    meta = {k: z[k].item() if z[k].ndim == 0 else z[k].tolist() for k in z.files if k != "params"}
+    return z["params"].astype(np.float32), int(z["level"]), meta
+
+
+def train_hetcube(n: int = 48, seeds=range(2000, 2008), level: int = 2, steps: int = 12000, batch: int = 16,
+                  lr: float = 1e-3, lr_final: float = 5e-5, capacity: int = 600, every: int = 1, device="cuda",
+                  log=print):
+    """The shipped network's recipe: (residual, error) samples from the plain FP64 solver on
+    heterogeneous cubes with seed-distinct materials (seeds 2000.. ; the benchmark scene uses
+    1005), then Adam on the library's kernels.  Returns (params, metadata)."""
+    import time
+    from . import scenes
+    from .linear_system import PCGSolverConfig, Solver
+    data, t0 = [], time.time()
+    for sd in seeds:
+        sysm = scenes.make_heterogeneous_cube(n=n, seed=int(sd))
+        s = Solver(PCGSolverConfig(precision="fp64", stop_rule="relative_residual", global_tol_rate=1e-4))
+        pm, rm = sysm.slot_maps(16)
+        s.mas_init(sysm.num_verts, sysm.neighbor_start, sysm.neighbor_num, sysm.neighbor_list, pm, rm)
+        s.net_configure(level)
+        d, st = record_samples(s, sysm, capacity=capacity, every=every, device=device)
+        data.append(d)
+        s.close()
+        log(f"seed {sd}: level {level} nodes {d.graph.nodes}, {d.samples} samples ({st['iterations']} iterations)")
+    samples = sum(d.samples for d in data)
+    tr = Trainer(init_params(0), device)
+    loss0 = float(np.mean([tr.evaluate(d.graph, d.rc[:64].contiguous(), d.zc[:64].contiguous(), min(64, d.samples))
+                           for d in data]))
+    hist = train(tr, data, steps, batch=batch, lr=lr, lr_final=lr_final, log_every=max(1, steps // 10))
+    loss1 = float(np.mean([tr.evaluate(d.graph, d.rc[:64].contiguous(), d.zc[:64].contiguous(), min(64, d.samples))
+                           for d in data]))
+    log(f"{samples} samples, {steps} steps in {time.time() - t0:.1f} s: loss {loss0:.4f} -> {loss1:.4f}")
+    meta = dict(level=level, n=n, seeds=[int(s) for s in seeds], steps=steps, batch=batch, lr=lr, lr_final=lr_final,
+                samples=samples, loss_initial=loss0, loss_final=loss1, history=[h[1] for h in hist])
+    return tr.params.cpu().numpy(), meta
+
+
+def _main(argv=None):
+    import argparse
+    ap = argparse.ArgumentParser(description="train the learned coarse correction on heterogeneous cubes")
+    ap.add_argument("cmd", choices=["train"])
+    ap.add_argument("--n", type=int, default=48)
+    ap.add_argument("--seeds", default="2000-2007")
+    ap.add_argument("--level", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=12000)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    lo, _, hi = a.seeds.partition("-")
+    seeds = range(int(lo), int(hi or lo) + 1)
+    params, meta = train_hetcube(n=a.n, seeds=seeds, level=a.level, steps=a.steps)
+    out = a.out or default_weights(a.level, a.n)
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    np.savez(out, params=params, **{k: np.asarray(v) for k, v in meta.items()})
+    print("wrote", out)
+
+
+if __name__ == "__main__":
+    _main()

@@ -225,3 +225,52 @@ def test_fused_apply_matches_layered_forward(dev, level):
     corr = want - z[:, :3]
     assert np.linalg.norm(got[:, :3] - want) <= 5e-3 * np.linalg.norm(corr) + 1e-7
     assert np.all(got[:, 3] == 0)
+
+
+def test_training_lowers_the_energy_loss(dev):
+    """From-scratch training on the GPU kernels: samples recorded by the plain FP64 solver on
+    two seeds, a few hundred Adam steps, the mean energy loss falls well below the bank
+    solve's (-1)."""
+    from stgipc import learned, scenes
+    data = []
+    for sd in (2300, 2301):
+        sysm = scenes.make_heterogeneous_cube(n=16, seed=sd)
+        solver = _solver(sysm, 1, dev, precision="fp64")
+        d, st = learned.record_samples(solver, sysm, capacity=200, every=1)
+        assert d.samples == min(200, st["iterations"])
+        data.append(d)
+    tr = learned.Trainer(learned.init_params(0), dev)
+    ev = lambda: np.mean([tr.evaluate(d.graph, d.rc[:32].contiguous(), d.zc[:32].contiguous(), min(32, d.samples))
+                          for d in data])
+    before = ev()
+    learned.train(tr, data, 400, batch=8, lr=1e-3, lr_final=1e-4)
+    after = ev()
+    assert abs(before + 1.0) < 0.05
+    assert after < before - 0.15, (before, after)
+
+
+def test_shipped_network_gain_on_held_out_scene(dev):
+    """What the shipped network (trained on heterogeneous-cube seeds 2000-2007) gains over
+    plain MAS on the held-out benchmark scene (352,947 DOF, seed 1005): fewer PCG iterations
+    at the same FP64 relative residual, in FP32 and in FP64."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    from stgipc import learned
+    params, level, meta = learned.load_weights(learned.default_weights())
+    assert 1005 not in meta["seeds"]
+    sysm, _ = bench.load_system("hetcube48")
+    P = _t(params, dev)
+    out = {}
+    for prec in ("fp32", "fp64"):
+        plain = _solver(sysm, level, dev, precision=prec)
+        stp, _ = _solve(plain, sysm, dev)
+        lrn = _solver(sysm, level, dev, precision=prec, learned=True)
+        lrn.net_set_params(P)
+        stl, _ = _solve(lrn, sysm, dev)
+        out[prec] = (stp["iterations"], stl["iterations"])
+        assert stl["status"] == 0 and stl["rel_residual"] <= 1e-4
+        assert stl["learned_rejected"] == 0
+        assert stl["iterations"] <= 0.9 * stp["iterations"], out
+    print("iterations plain -> learned:", out)
