@@ -229,16 +229,59 @@ def train_hetcube(n: int = 48, seeds=range(2000, 2008), level: int = 2, steps: i
     return tr.params.cpu().numpy(), meta
 
 
+def solve_hetcube(n: int = 48, seed: int = 1005, precision: str = "fp32", loop: str = "graph", weights=None,
+                  plain: bool = True, device="cuda", log=print):
+    """One heterogeneous-cube Newton system solved with the shipped network (and, with
+    plain=True, without it): iterations, relative residual, solve wall time."""
+    import time
+    import torch
+    from . import scenes
+    from .linear_system import PCGSolverConfig, Solver
+    params, level, _ = load_weights(weights or default_weights())
+    sysm = scenes.make_heterogeneous_cube(n=n, seed=seed)
+    dev = torch.device(device)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    rows, cols, blocks, b = t(sysm.rows), t(sysm.cols), t(sysm.blocks.reshape(-1)), t(sysm.b)
+    pm, rm = sysm.slot_maps(16)
+    out = {}
+    for on in ([False] if plain else []) + [True]:
+        s = Solver(PCGSolverConfig(precision=precision, stop_rule="relative_residual", global_tol_rate=1e-4, loop=loop,
+                                   learned=on))
+        s.mas_init(sysm.num_verts, sysm.neighbor_start, sysm.neighbor_num, sysm.neighbor_list, pm, rm)
+        s.net_configure(level)
+        if on:
+            s.net_set_params(t(params))
+        x = torch.zeros_like(b)
+        s.solve_linear_system(rows, cols, blocks, b, x)
+        torch.cuda.synchronize(dev)
+        t0 = time.time()
+        st = s.solve_linear_system(rows, cols, blocks, b, x)
+        torch.cuda.synchronize(dev)
+        key = "learned" if on else "plain"
+        out[key] = dict(iterations=st["iterations"], rel_residual=st["rel_residual"], ms=(time.time() - t0) * 1e3,
+                        accepted=st["learned_accepted"], rejected=st["learned_rejected"])
+        log(f"{key}: {out[key]}")
+        s.close()
+    return out
+
+
 def _main(argv=None):
     import argparse
-    ap = argparse.ArgumentParser(description="train the learned coarse correction on heterogeneous cubes")
-    ap.add_argument("cmd", choices=["train"])
+    ap = argparse.ArgumentParser(description="train or run the learned coarse correction on heterogeneous cubes")
+    ap.add_argument("cmd", choices=["train", "solve"])
     ap.add_argument("--n", type=int, default=48)
-    ap.add_argument("--seeds", default="2000-2007")
+    ap.add_argument("--seeds", default="2000-2007", help="train: scene seeds")
+    ap.add_argument("--seed", type=int, default=1005, help="solve: scene seed")
     ap.add_argument("--level", type=int, default=2)
     ap.add_argument("--steps", type=int, default=12000)
+    ap.add_argument("--precision", default="fp32")
+    ap.add_argument("--loop", default="graph")
+    ap.add_argument("--learned-only", action="store_true")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
+    if a.cmd == "solve":
+        solve_hetcube(a.n, a.seed, a.precision, a.loop, plain=not a.learned_only)
+        return
     lo, _, hi = a.seeds.partition("-")
     seeds = range(int(lo), int(hi or lo) + 1)
     params, meta = train_hetcube(n=a.n, seeds=seeds, level=a.level, steps=a.steps)
