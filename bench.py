@@ -409,6 +409,14 @@ def main():
                                       "accepted": st_l["learned_accepted"], "rejected": st_l["learned_rejected"]}
                 ls.close()
 
+    # the BCOO tile autotuner on this system: both FP32 tile shapes timed in the loop's kernel
+    tuned = make("fp32")
+    tuned.spmv_tiles(0)
+    solve(tuned)
+    rt_t, us_def, us_alt = tuned.spmv_tiles_info()
+    tuned.close()
+    tiles = {"default_rows_per_tile": 64, "tuned_rows_per_tile": rt_t, "us_per_launch": {"64x4": us_def, "32x8": us_alt}}
+
     # roofline of the dominant kernel: the PCG SpMV of the FP32 path, timed live
     solve(fast)
     spmv_ms, spmv_bytes = fast.profile_spmv(reps=100)
@@ -462,6 +470,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "learned": learned_line,
+            "spmv_tiles": tiles,
             "gpu_launches": int(st_fast["kernel_launches"] * args.steps),
             "clocks": clk.summary(),
         }

@@ -207,6 +207,18 @@ int stg_profile_spmv(stg_handle h, int reps, float* avg_ms, double* bytes);
  * the device stays usable.  Returns STG_OK when the diagnostic ran. */
 int stg_selftest_wait_timeout(int* status, double* seconds);
 
+/* ---- BCOO tile autotuner -------------------------------------------------------------- */
+/* No counterpart in the reference.  Tile shape of the in-loop SpMV: rows_per_tile rows per
+ * tile of the row-sliced full copy, with 256 / rows_per_tile lanes per row (FP32: 64 or 32;
+ * FP64: 32 or 16).  0 = autotune: the next solve of a new system shape (precision, block
+ * rows, unique blocks) times every candidate on that system and keeps the fastest for the
+ * handle; -1 = the precision's default (64 / 32).  Results differ between tile shapes in
+ * the last bits (summation order); a fixed shape keeps solves bitwise reproducible. */
+int stg_spmv_tiles(stg_handle h, int rows_per_tile);
+/* Rows per tile of the last solve, and the autotuner's mean time per launch of each
+ * candidate in microseconds (default shape first; 0 when it has not run). */
+int stg_spmv_tiles_info(stg_handle h, int* rows_per_tile, float* us_default, float* us_alternative);
+
 /* ---- allocation-free SpMV ---------------------------------------------------------- */
 /* No counterpart in the reference.  The same y = a * A * x + b * y as stg_spmv (same
  * kernel, same result bit for bit), for callers that cannot allocate device memory: a host

@@ -725,11 +725,17 @@ __global__ void __launch_bounds__(D_WARPS * 32) k_phase_d16(PcgDev c)
 constexpr int A_CW = 8;            // consumer warps
 constexpr int A_THREADS = (A_CW + 1) * 32;
 
-template <typename T>
+// Tile shapes of the SpMV phase: rows per tile x lanes per row = 8 warps x 32.  The
+// default for each precision is the first of its candidates; the autotuner may pick the
+// other (Solver::spmv_rt).
+template <typename T> constexpr int a_rt_default() { return sizeof(T) == 4 ? 64 : 32; }
+template <typename T> constexpr int a_rt_alt() { return sizeof(T) == 4 ? 32 : 16; }
+
+template <typename T, int RT_ = a_rt_default<T>()>
 struct ATile
 {
     using FP = FullPlanes<T>;
-    static constexpr int RT = sizeof(T) == 4 ? 64 : 32;         // rows per tile
+    static constexpr int RT = RT_;                               // rows per tile
     static constexpr int LPR = 32 * A_CW / RT;                   // consumer lanes per row
     static constexpr int CAP = 20 * RT;                          // entries per stage (even)
     static constexpr int STAGES = 2;
@@ -808,10 +814,10 @@ __device__ __forceinline__ void a_gather(int j, const T* zp, T beta, T& x0, T& x
     x2 += beta * p2;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(A_THREADS, ATile<T>::MIN_CTAS) k_phase_a_tiled(PcgDev c)
+template <typename T, int RTT>
+__global__ void __launch_bounds__(A_THREADS, ATile<T, RTT>::MIN_CTAS) k_phase_a_tiled(PcgDev c)
 {
-    using G = ATile<T>;
+    using G = ATile<T, RTT>;
     using FP = FullPlanes<T>;
     constexpr int RT = G::RT, LPR = G::LPR, CAP = G::CAP;
     extern __shared__ __align__(128) unsigned char asm_[];
@@ -1619,34 +1625,78 @@ static int launch_mas_cd(Solver& S, const PcgDev& c)
 }
 
 
-// tiled phase A: the shared-memory opt-in and one resident wave of CTAs
-template <typename T>
-static int phase_a_grid(int nrows, int* grid)
+// tiled phase A: the shared-memory opt-in and one resident wave of CTAs, per tile shape
+template <typename T, int RT>
+static int phase_a_grid_rt(int nrows, int* grid)
 {
     static thread_local int per_sm = -1;
     if(per_sm < 0)
     {
-        STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_a_tiled<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          ATile<T>::SMEM));
-        STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase_a_tiled<T>, A_THREADS,
-                                                                   ATile<T>::SMEM));
+        STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_a_tiled<T, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          ATile<T, RT>::SMEM));
+        STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_a_tiled<T, RT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          cudaSharedmemCarveoutMaxShared));
+        STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase_a_tiled<T, RT>, A_THREADS,
+                                                                   ATile<T, RT>::SMEM));
     }
-    *grid = std::max(1, std::min(div_up(nrows, ATile<T>::RT), std::max(per_sm, 1) * kSMs));
+    *grid = std::max(1, std::min(div_up(nrows, RT), std::max(per_sm, 1) * kSMs));
     return 0;
+}
+
+template <typename T>
+static int phase_a_grid(int nrows, int rt, int* grid)
+{
+    if(rt == a_rt_alt<T>()) return phase_a_grid_rt<T, a_rt_alt<T>()>(nrows, grid);
+    return phase_a_grid_rt<T, a_rt_default<T>()>(nrows, grid);
 }
 
 template <typename T>
 static int launch_phase_a(const PcgDev& c, cudaStream_t s)
 {
     int grid = 0;
-    STG_TRY(phase_a_grid<T>(c.nrows, &grid));
+    STG_TRY(phase_a_grid<T>(c.nrows, c.a_rt, &grid));
     if(grid != c.grid_a)
     {
         set_error("SpMV phase grid differs from the one phase B sums over");
         return STG_ERR_INVALID;
     }
-    k_phase_a_tiled<T><<<grid, A_THREADS, ATile<T>::SMEM, s>>>(c);
+    if(c.a_rt == a_rt_alt<T>())
+        k_phase_a_tiled<T, a_rt_alt<T>()><<<grid, A_THREADS, ATile<T, a_rt_alt<T>()>::SMEM, s>>>(c);
+    else
+        k_phase_a_tiled<T, a_rt_default<T>()><<<grid, A_THREADS, ATile<T>::SMEM, s>>>(c);
     STG_LAUNCH_CHECK();
+    return 0;
+}
+
+// BCOO tile autotuner: every candidate tile shape of the SpMV phase launched on this system
+// (3 untimed, then `reps` timed with CUDA events); returns the fastest shape and each mean
+template <typename T>
+static int tune_phase_a(Solver& S, PcgDev c, float* us, int* out)
+{
+    const int cand[2] = {a_rt_default<T>(), a_rt_alt<T>()};
+    float best = 0.f;
+    int pick = cand[0];
+    for(int v = 0; v < 2; v++)
+    {
+        c.a_rt = cand[v];
+        STG_TRY(phase_a_grid<T>(c.nrows, c.a_rt, &c.grid_a));
+        for(int i = 0; i < 3; i++) STG_TRY(launch_phase_a<T>(c, S.stream));
+        const int reps = 10;
+        STG_CUDA_TRY(cudaEventRecord(S.ev[4], S.stream));
+        for(int i = 0; i < reps; i++) STG_TRY(launch_phase_a<T>(c, S.stream));
+        STG_CUDA_TRY(cudaEventRecord(S.ev[5], S.stream));
+        STG_CUDA_TRY(cudaEventSynchronize(S.ev[5]));
+        float ms = 0.f;
+        STG_CUDA_TRY(cudaEventElapsedTime(&ms, S.ev[4], S.ev[5]));
+        us[v] = 1e3f * ms / reps;
+        S.launches += 3 + reps;
+        if(v == 0 || us[v] < best)
+        {
+            best = us[v];
+            pick = cand[v];
+        }
+    }
+    *out = pick;
     return 0;
 }
 
@@ -1756,7 +1806,6 @@ static int set_carveouts()
     const int cv = cudaSharedmemCarveoutMaxShared;
     constexpr int BB = B > 0 ? B : 16;
     STG_CUDA_TRY(cudaFuncSetAttribute(k_init<T>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
-    STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_a_tiled<T>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
     STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_b<T, B>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
     STG_CUDA_TRY(cudaFuncSetAttribute(k_replace, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
     STG_CUDA_TRY(cudaFuncSetAttribute(k_restrict01<BB>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
@@ -1774,7 +1823,7 @@ template <typename T, int B>
 static int pcg_run(Solver& S, PcgDev& c, int& h_done)
 {
     STG_TRY((set_carveouts<T, B>()));
-    STG_TRY(phase_a_grid<T>(c.nrows, &c.grid_a));
+    STG_TRY(phase_a_grid<T>(c.nrows, c.a_rt, &c.grid_a));
     c.grid_e = std::max(1, std::min(div_up(c.n, PB), kSMs * 4));  // grid_vec below
     if(c.grid_a > c.slots || c.grid_e > c.slots)
     {
@@ -2112,6 +2161,25 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
     c.prm.stop_rule = cfg.stop_rule;
     c.prm.refine = fp32 ? cfg.refine_interval : 0;
     c.bar = P.bar.data();
+    // SpMV tile shape: fixed, tuned once per system shape, or the precision's default
+    c.a_rt = fp32 ? a_rt_default<float>() : a_rt_default<double>();
+    if(spmv_rt > 0)
+        c.a_rt = spmv_rt;
+    else if(spmv_tune)
+    {
+        if(tuned_prec != (fp32 ? 1 : 0) || tuned_nrows != bcoo.nrows || tuned_nnzb != bcoo.nnzb)
+        {
+            PcgDev t = c;
+            t.grid_e = std::max(1, std::min(div_up(n, PB), kSMs * 4));
+            int r = 0;
+            STG_TRY(fp32 ? tune_phase_a<float>(*this, t, tune_us, &r) : tune_phase_a<double>(*this, t, tune_us, &r));
+            tuned_rt = r;
+            tuned_prec = fp32 ? 1 : 0;
+            tuned_nrows = bcoo.nrows;
+            tuned_nnzb = bcoo.nnzb;
+        }
+        c.a_rt = tuned_rt;
+    }
     const bool net_apply = cfg.learned != 0, net_rec = learned.rec_cap > 0;
     if(net_apply || net_rec)
     {

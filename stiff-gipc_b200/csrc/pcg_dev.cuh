@@ -62,6 +62,7 @@ struct PcgDev
     unsigned* bar;            // persistent barrier: [0] count, [1] generation
     // learned coarse correction: flexible PCG (beta from r_(k+1).(z_(k+1) - z_k), phase E's
     // r.z_old partials at SITE_F); the rest only keys the captured graph
+    int a_rt;                 // rows per tile of the SpMV phase (one of the compiled shapes)
     int flex;
     int net_mode;             // bit 0: network applied, bit 1: samples recorded
     int net_n, net_rec_cap, net_rec_every;

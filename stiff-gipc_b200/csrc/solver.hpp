@@ -158,6 +158,12 @@ struct Solver
     cudaGraph_t pending_if_body = nullptr;
     PcgDev pcg_dev{};             // parameters of the last solve (measurement hook)
     bool pcg_ready = false;
+    // SpMV tile shape: spmv_rt > 0 fixes the rows per tile; spmv_rt == 0 with spmv_tune set
+    // times the candidates at the next solve of a new shape and keeps the fastest
+    int spmv_rt = 0;
+    bool spmv_tune = false;
+    int tuned_rt = 0, tuned_prec = -1, tuned_nrows = -1, tuned_nnzb = -1;
+    float tune_us[2] = {0.f, 0.f};
 
     ~Solver();
 

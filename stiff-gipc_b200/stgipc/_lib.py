@@ -99,6 +99,8 @@ def lib():
     L.stg_profile_spmv.argtypes = [vp, ci, C.POINTER(C.c_float), C.POINTER(cd)]
     L.stg_spmv_noalloc.argtypes = [cd, vp, vp, vp, ci, vp, cd, vp, ci, vp]
     L.stg_selftest_wait_timeout.argtypes = [C.POINTER(ci), C.POINTER(cd)]
+    L.stg_spmv_tiles.argtypes = [vp, ci]
+    L.stg_spmv_tiles_info.argtypes = [vp, C.POINTER(ci), C.POINTER(C.c_float), C.POINTER(C.c_float)]
     L.stg_net_configure.argtypes = [vp, ci]
     L.stg_net_graph_info.argtypes = [vp, C.POINTER(ci), C.POINTER(ci)]
     L.stg_net_export_graph.argtypes = [vp, vp, vp, vp, vp, vp, vp]

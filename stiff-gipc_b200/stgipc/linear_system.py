@@ -192,6 +192,17 @@ class Solver:
         return dict(fine_mask=fine, prefix_orig=pref, coarse_tables=ct.reshape(L, V), going_next=gn,
                     coarse_table=tab.reshape(V, max(L - 1, 1)), level_size=ls)
 
+    # -- BCOO tile autotuner -------------------------------------------------------------------
+    def spmv_tiles(self, rows_per_tile: int):
+        """0: autotune at the next solve of a new shape; -1: default; else a fixed shape."""
+        check(_L.lib().stg_spmv_tiles(self.h, int(rows_per_tile)), "stg_spmv_tiles")
+
+    def spmv_tiles_info(self):
+        """(rows per tile of the last solve, tuner us per launch: default, alternative)."""
+        rt, a, b = C.c_int(), C.c_float(), C.c_float()
+        check(_L.lib().stg_spmv_tiles_info(self.h, C.byref(rt), C.byref(a), C.byref(b)), "stg_spmv_tiles_info")
+        return rt.value, a.value, b.value
+
     # -- learned coarse correction (stg_net_*) ---------------------------------------------
     def net_configure(self, level: int):
         """Coarse level of the network; the next MAS assembly builds its graph."""
