@@ -207,6 +207,25 @@ int stg_profile_spmv(stg_handle h, int reps, float* avg_ms, double* bytes);
  * the device stays usable.  Returns STG_OK when the diagnostic ran. */
 int stg_selftest_wait_timeout(int* status, double* seconds);
 
+/* ---- Hessian producer ------------------------------------------------------------------ */
+/* The triplets and gradient of one implicit-Euler Newton iteration of a tet mesh, on the
+ * GPU: what GIPC hands to GlobalLinearSystem::solve_linear_system (femEnergy.cu:1719-1855
+ * for the elastic part, GIPC.cu:6524-6551 for the plane barrier).  Per tet: stable
+ * Neo-Hookean psi = mu/2 (|F|^2 - 3) + lam/2 (J - 1 - mu/lam)^2 (E per tet, nu), its 9x9
+ * Hessian in F projected to PSD (negative eigenvalues clamped, FP64 Jacobi), times
+ * vol dt^2, as the tet's 10 upper 3x3 blocks (column-major) at triplets 10 t .. 10 t + 9.
+ * Per vertex (triplet 10 tets + v): lumped mass rho vol / 4 plus the barrier Hessians of
+ * the planes it is within dhat of.  b = dt^2 vol P : dF/dx + M (x - x - dt v - dt^2 g) +
+ * barrier gradients, with g = (0, gravity_y, 0).  planes: [nplanes][6] = normal xyz,
+ * offset (plane n.x = offset), dhat, kappa.  All arrays are device arrays; rows / cols /
+ * blocks hold 10 tets + verts triplets, b 3 verts doubles. */
+size_t stg_fem_scratch_bytes(int verts, int tets);
+int stg_fem_newton_system(int verts, const double* rest, const double* pos, const double* vel, int tets,
+                          const int32_t* tet_verts, const double* youngs, double poisson, double density,
+                          double dt, double gravity_y, int nplanes, const double* planes, int32_t* rows,
+                          int32_t* cols, double* blocks, double* b, void* scratch, size_t scratch_bytes,
+                          void* stream);
+
 /* ---- BCOO tile autotuner -------------------------------------------------------------- */
 /* No counterpart in the reference.  Tile shape of the in-loop SpMV: rows_per_tile rows per
  * tile of the row-sliced full copy, with 256 / rows_per_tile lanes per row (FP32: 64 or 32;

@@ -726,3 +726,22 @@ int stg_spmv_tiles_info(stg_handle h, int* rows_per_tile, float* us_default, flo
     if(us_alternative) *us_alternative = h->tune_us[1];
     return STG_OK;
 }
+
+size_t stg_fem_scratch_bytes(int verts, int tets)
+{
+    if(verts < 1 || tets < 0) return 0;
+    return stg::fem_scratch_bytes(verts, tets);
+}
+
+int stg_fem_newton_system(int verts, const double* rest, const double* pos, const double* vel, int tets,
+                          const int32_t* tet_verts, const double* youngs, double poisson, double density,
+                          double dt, double gravity_y, int nplanes, const double* planes, int32_t* rows,
+                          int32_t* cols, double* blocks, double* b, void* scratch, size_t scratch_bytes,
+                          void* stream)
+{
+    GUARD({
+        return stg::fem_newton_system(static_cast<cudaStream_t>(stream), verts, rest, pos, vel, tets, tet_verts, youngs,
+                                      poisson, density, dt, gravity_y, nplanes, planes, rows, cols, blocks, b, scratch,
+                                      scratch_bytes);
+    })
+}

@@ -100,6 +100,9 @@ def lib():
     L.stg_spmv_noalloc.argtypes = [cd, vp, vp, vp, ci, vp, cd, vp, ci, vp]
     L.stg_selftest_wait_timeout.argtypes = [C.POINTER(ci), C.POINTER(cd)]
     L.stg_spmv_tiles.argtypes = [vp, ci]
+    L.stg_fem_scratch_bytes.argtypes = [ci, ci]
+    L.stg_fem_newton_system.argtypes = [ci, vp, vp, vp, ci, vp, vp, cd, cd, cd, cd, ci, vp, vp, vp, vp, vp, vp,
+                                        C.c_size_t, vp]
     L.stg_spmv_tiles_info.argtypes = [vp, C.POINTER(ci), C.POINTER(C.c_float), C.POINTER(C.c_float)]
     L.stg_net_configure.argtypes = [vp, ci]
     L.stg_net_graph_info.argtypes = [vp, C.POINTER(ci), C.POINTER(ci)]
@@ -113,9 +116,10 @@ def lib():
     L.stg_net_train_step.argtypes = [C.POINTER(NetGraphC), vp, vp, ci, vp, vp, vp, vp, ci, C.c_float, vp, vp,
                                      C.c_size_t, vp]
     for name in header_symbols():
-        if name not in ("stg_last_error", "stg_config_default", "stg_net_scratch_bytes"):
+        if name not in ("stg_last_error", "stg_config_default", "stg_net_scratch_bytes", "stg_fem_scratch_bytes"):
             getattr(L, name).restype = ci
     L.stg_net_scratch_bytes.restype = C.c_size_t
+    L.stg_fem_scratch_bytes.restype = C.c_size_t
     _lib = L
     return L
 

@@ -366,12 +366,14 @@ def make_cube_drop(n: int = 16, seed: int = 1001, E: float = 1e5, nu: float = 0.
 def make_heterogeneous_cube(n: int = 48, seed: int = 1005, nu: float = 0.45, rho: float = 1000.0,
                             dt: float = 1.0 / 60.0, e_lo: float = 1e4, e_hi: float = 1e8,
                             regions: int = 8, squash: float = 0.08, jitter: float = 1e-3,
-                            dhat: float = 1e-3, kappa: float = 1e5, slab_speed: float = 1.0) -> NewtonSystem:
+                            dhat: float = 1e-3, kappa: float = 1e5, slab_speed: float = 1.0,
+                            state_only: bool = False) -> NewtonSystem:
     """Heterogeneous cube under a rigid slab: n^3 hexes (6 tets each), per-tet Young's modulus
     log-uniform in [e_lo, e_hi] from ``regions`` seeded Voronoi sites, nu=0.45; one Newton
     iteration of a step where the slab (moving down at ``slab_speed``) has squashed the top by
     ``squash`` m.  The slab and the ground act through IPC plane barriers.  n=48: 117,649
-    vertices, 663,552 tets, 352,947 DOF."""
+    vertices, 663,552 tets, 352,947 DOF.  state_only: return the mesh state and material
+    instead (the inputs of _assemble, or of the GPU Hessian producer stgipc.fem)."""
     rng = np.random.default_rng(seed)
     rest, tets = cube_mesh(n, 1.0, origin=(0.0, 0.0, 0.0))
     rest = rest + rng.uniform(-jitter, jitter, size=rest.shape)
@@ -393,8 +395,11 @@ def make_heterogeneous_cube(n: int = 48, seed: int = 1005, nu: float = 0.45, rho
     top = pos[:, 1].max() + 4e-4
     vel = np.zeros_like(pos)
     vel[:, 1] = -slab_speed * (rest[:, 1])
-    return _assemble(f"hetcube{n}", rest, pos, tets, E_t, nu, rho, dt, vel,
-                     barriers=[((0.0, 1.0, 0.0), 0.0, dhat, kappa), ((0.0, -1.0, 0.0), -top, dhat, kappa)])
+    state = dict(name=f"hetcube{n}", pos_rest=rest, pos=pos, tets=tets, E=E_t, nu=nu, rho=rho, dt=dt, vel=vel,
+                 barriers=[((0.0, 1.0, 0.0), 0.0, dhat, kappa), ((0.0, -1.0, 0.0), -top, dhat, kappa)])
+    if state_only:
+        return state
+    return _assemble(**state)
 
 
 def make_batched_cubes(count: int = 256, seed: int = 1004, n_lo: int = 4, n_hi: int = 24,
