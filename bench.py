@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--loop", choices=["host", "graph", "persistent"], default="graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-correction solves")
+    ap.add_argument("--streams", type=int, default=8, help="batch256: CUDA streams (and host threads) per GPU")
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     return ap.parse_args()
 
@@ -163,6 +164,25 @@ def cpu_solve_ms(sysm, bank, budget_s, fallback_iters=None):
     return ms, n_it, threads, sample
 
 
+def cpu_block_jacobi_ms(sysm, iterations, budget_s):
+    """The CPU baseline the metric names: block-Jacobi CG (Eigen's ConjugateGradient with a
+    3x3 block-Jacobi preconditioner, restated in the C oracle without Eigen) on all host
+    threads: convert (serial C) + CSR and block inverses, then up to `budget_s` seconds of
+    CG; the per-iteration time is scaled to `iterations` (the GPU block-Jacobi PCG's count
+    on the same system to the same stop rule).  Returns (ms, threads, sample text)."""
+    from oracle import oracle as orc
+    orc.build()
+    t0 = time.perf_counter()
+    r, c, b = orc.convert(sysm.rows, sysm.cols, sysm.blocks)
+    t_conv = time.perf_counter() - t0
+    _, k, t_set, t_iter, done, threads, rel = orc.cg_bj_timed_mt(r, c, b, sysm.b, tol=1e-4, budget_s=budget_s)
+    n_it = k if done else iterations
+    ms = (t_conv + t_set + t_iter * n_it) * 1e3
+    sample = (f"oracle block-Jacobi CG: convert ({t_conv:.1f} s, serial) + CSR / inverses + {k} CG iterations on "
+              f"{threads} threads ({'converged' if done else 'time-bounded'}), per-iteration time x {n_it} iterations")
+    return ms, threads, sample
+
+
 def run_reference(args):
     """--impl reference: the CPU oracle port of the reference's MAS-PCG on all host cores."""
     rank = int(os.environ.get("RANK", "0"))
@@ -212,7 +232,7 @@ def run_batch(args):
     mine = shard_by_dof([s.n for s in sysl], world)[rank]
     cfg = PCGSolverConfig(precision="fp32", stop_rule="relative_residual", global_tol_rate=1e-4,
                           refine_interval=args.refine, loop=args.loop)
-    bs = BatchSolver([sysl[i] for i in mine], cfg, device=dev, streams=8)
+    bs = BatchSolver([sysl[i] for i in mine], cfg, device=dev, streams=args.streams)
     main_stream = torch.cuda.current_stream(dev)
 
     def timed(k, e2e=False):
@@ -266,7 +286,7 @@ def run_batch(args):
             "ms_per_step": ms, "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
             "dtype": "f32 (FP64 dots, FP64 residual replacement)", "data": "synthetic",
             "config": {"workload": "batch256", "scenes": len(sysl), "dof_total": int(sum(s.n for s in sysl)),
-                       "dof_rank0": int(sum(sysl[i].n for i in mine)), "streams_per_gpu": 8,
+                       "dof_rank0": int(sum(sysl[i].n for i in mine)), "streams_per_gpu": args.streams,
                        "parallelism": f"scenes sharded by DOF over {world} GPU(s)",
                        "l2": "inputs larger than L2 (2.6 M DOFs, 3.4 GB of triplets); no flush"},
             "iterations_rank0": {"min": min(iters), "max": max(iters), "mean": sum(iters) / len(iters)},
@@ -444,6 +464,17 @@ def main():
         ms_cpu, _, threads, sample = cpu_solve_ms(sysm, args.bank, args.cpu_budget_s,
                                                   fallback_iters=st_plain["iterations"])
         cpu = {"value": ms_cpu, "unit": "ms", "cores": threads, "kind": "port", "sample": sample}
+        # the metric's named CPU baseline: block-Jacobi CG; its iteration count from the GPU's
+        # block-Jacobi PCG on the same system and stop rule
+        bj = Solver(PCGSolverConfig(bank_size=args.bank, precision="fp64", preconditioner="diag",
+                                    stop_rule="relative_residual", global_tol_rate=1e-4, loop=args.loop,
+                                    max_iter_ratio=0.3), stream=stream)
+        st_bj = bj.solve_linear_system(rows, cols, blocks, b, x)
+        bj.close()
+        ms_bj, thr_bj, sample_bj = cpu_block_jacobi_ms(sysm, st_bj["iterations"], args.cpu_budget_s)
+        cpu["block_jacobi_cg"] = {"value": ms_bj, "unit": "ms", "cores": thr_bj, "kind": "port",
+                                  "iterations": st_bj["iterations"], "converged": st_bj["status"] == 0,
+                                  "sample": sample_bj}
 
     if rank == 0:
         line = {

@@ -75,6 +75,10 @@ def lib():
                                  C.c_double, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                  C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L.orc_pcg_mt.restype = C.c_int
+        L.orc_cg_bj_mt.argtypes = [_i32p, _i32p, _f64p, C.c_int, C.c_int, _f64p, _f64p, C.c_double, C.c_double,
+                                   C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int),
+                                   C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.orc_cg_bj_mt.restype = C.c_int
         _lib = L
     return _lib
 
@@ -208,6 +212,21 @@ def pcg_timed_mt(rows, cols, blocks, b, mas: Mas, tol=1e-4, max_iter_ratio=0.3, 
                          np.ascontiguousarray(blocks, np.float64).reshape(-1), rows.size, n,
                          np.ascontiguousarray(b, np.float64), x, mas.h, tol, max_iter_ratio, float(budget_s),
                          C.byref(t_setup), C.byref(t_iter), C.byref(done), C.byref(threads), C.byref(rel))
+    return x, int(k), t_setup.value, t_iter.value, bool(done.value), threads.value, rel.value
+
+
+def cg_bj_timed_mt(rows, cols, blocks, b, tol=1e-4, max_iter_ratio=0.3, budget_s=0.0):
+    """Block-Jacobi CG on all host threads (the Eigen ConjugateGradient + block-Jacobi
+    baseline, restated; stop rule ||r|| <= tol ||b||), for timing.  Returns (x, iterations,
+    seconds of set-up, seconds per iteration, finished, threads, last relative residual)."""
+    n = b.size
+    x = np.zeros(n)
+    t_setup, t_iter, rel = C.c_double(), C.c_double(), C.c_double()
+    done, threads = C.c_int(), C.c_int()
+    k = lib().orc_cg_bj_mt(np.ascontiguousarray(rows, np.int32), np.ascontiguousarray(cols, np.int32),
+                           np.ascontiguousarray(blocks, np.float64).reshape(-1), rows.size, n,
+                           np.ascontiguousarray(b, np.float64), x, tol, max_iter_ratio, float(budget_s),
+                           C.byref(t_setup), C.byref(t_iter), C.byref(done), C.byref(threads), C.byref(rel))
     return x, int(k), t_setup.value, t_iter.value, bool(done.value), threads.value, rel.value
 
 

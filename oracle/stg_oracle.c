@@ -1106,3 +1106,109 @@ int orc_pcg_mt(const int* rows, const int* cols, const double* blocks, int nnzb,
     free(A.ptr); free(A.col); free(A.val);
     return (int)k;
 }
+
+/* Block-Jacobi CG on all host threads, for the CPU baseline the metric names (Eigen's
+ * ConjugateGradient with a 3x3 block-Jacobi preconditioner, restated without Eigen): the
+ * same CSR product as orc_pcg_mt, z = D_i^-1 r_i with the inverses of the diagonal blocks,
+ * stop at ||r|| <= tol ||b||, max_iter or after budget_s seconds (*done = 0).  Returns the
+ * iterations; *t_setup covers the CSR build and the block inverses. */
+int orc_cg_bj_mt(const int* rows, const int* cols, const double* blocks, int nnzb, int n, const double* b, double* x,
+                 double tol, double max_iter_ratio, double budget_s, double* t_setup, double* t_iter, int* done,
+                 int* threads, double* rel)
+{
+    const double ts = now_s();
+    orc_csr A;
+    csr_build(&A, nnzb, rows, cols, blocks, n / 3);
+    const int nb = n / 3;
+    double* Dinv = (double*)calloc((size_t)nb * 9, sizeof(double));
+#pragma omp parallel for schedule(static)
+    for(int i = 0; i < nb; i++)
+    {
+        double D[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  /* column-major diagonal block */
+        for(int e = A.ptr[i]; e < A.ptr[i + 1]; e++)
+            if(A.col[e] == i)
+                for(int q = 0; q < 9; q++) D[q] += A.val[9 * (size_t)e + q];
+        /* inverse of a 3x3 by cofactors (column-major in and out) */
+        const double a = D[0], bq = D[3], c = D[6], d = D[1], ee = D[4], f = D[7], g = D[2], h = D[5], k = D[8];
+        const double det = a * (ee * k - f * h) - bq * (d * k - f * g) + c * (d * h - ee * g);
+        double* O = Dinv + 9 * (size_t)i;
+        if(det != 0.0)
+        {
+            const double id = 1.0 / det;
+            O[0] = (ee * k - f * h) * id;
+            O[3] = (c * h - bq * k) * id;
+            O[6] = (bq * f - c * ee) * id;
+            O[1] = (f * g - d * k) * id;
+            O[4] = (a * k - c * g) * id;
+            O[7] = (c * d - a * f) * id;
+            O[2] = (d * h - ee * g) * id;
+            O[5] = (bq * g - a * h) * id;
+            O[8] = (a * ee - bq * d) * id;
+        }
+        else
+            O[0] = O[4] = O[8] = 1.0;
+    }
+    *t_setup = now_s() - ts;
+    *threads = omp_get_max_threads();
+    double* r = (double*)malloc(sizeof(double) * n);
+    double* z = (double*)malloc(sizeof(double) * n);
+    double* p = (double*)malloc(sizeof(double) * n);
+    double* Ap = (double*)malloc(sizeof(double) * n);
+    const long max_iter = (long)(max_iter_ratio * (double)n);
+#pragma omp parallel for schedule(static)
+    for(int i = 0; i < n; i++)
+    {
+        x[i] = 0;
+        r[i] = b[i];
+    }
+#define BJ_APPLY()                                                                         \
+    do                                                                                     \
+    {                                                                                      \
+        _Pragma("omp parallel for schedule(static)") for(int i = 0; i < nb; i++)           \
+        {                                                                                  \
+            const double* O = Dinv + 9 * (size_t)i;                                        \
+            const double* ri = r + 3 * (size_t)i;                                          \
+            for(int q = 0; q < 3; q++) z[3 * i + q] = O[q] * ri[0] + O[3 + q] * ri[1] + O[6 + q] * ri[2]; \
+        }                                                                                  \
+    } while(0)
+    BJ_APPLY();
+    double rz = dot_mt(r, z, n);
+    memcpy(p, z, sizeof(double) * n);
+    const double bb = dot_mt(b, b, n);
+    const double t0 = now_s();
+    long k, counted = 0;
+    int finished = 0;
+    for(k = 1; k < max_iter; ++k)
+    {
+        csr_spmv(&A, p, Ap);
+        const double alpha = rz / dot_mt(p, Ap, n);
+#pragma omp parallel for schedule(static)
+        for(int i = 0; i < n; i++)
+        {
+            x[i] += alpha * p[i];
+            r[i] -= alpha * Ap[i];
+        }
+        counted = k;
+        const double rr = dot_mt(r, r, n);
+        *rel = bb > 0 ? sqrt(rr / bb) : 0.0;
+        if(rr <= tol * tol * bb)
+        {
+            finished = 1;
+            break;
+        }
+        if(budget_s > 0 && now_s() - t0 > budget_s) break;
+        BJ_APPLY();
+        const double rz_new = dot_mt(r, z, n);
+        const double beta = rz_new / rz;
+#pragma omp parallel for schedule(static)
+        for(int i = 0; i < n; i++) p[i] = z[i] + beta * p[i];
+        rz = rz_new;
+    }
+#undef BJ_APPLY
+    if(k >= max_iter) finished = 1;
+    *t_iter = counted > 0 ? (now_s() - t0) / (double)counted : 0.0;
+    *done = finished;
+    free(r); free(z); free(p); free(Ap); free(Dinv);
+    free(A.ptr); free(A.col); free(A.val);
+    return (int)k;
+}

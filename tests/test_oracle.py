@@ -204,3 +204,28 @@ def test_threaded_timing_pcg_matches_serial():
     assert abs(k2 - st1["iterations"]) <= 1
     assert np.linalg.norm(x2 - x1) <= 1e-6 * np.linalg.norm(x1)
     assert rel <= 1e-6
+
+
+def test_block_jacobi_cg_baseline_converges():
+    """The CPU block-Jacobi CG baseline (threaded) reaches the tolerance and agrees with a
+    direct solve."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+    from conftest import cube_system
+    from oracle import oracle as orc
+    s = cube_system(6)
+    r, c, bl = orc.convert(s.rows, s.cols, s.blocks)
+    x, k, _, _, done, threads, rel = orc.cg_bj_timed_mt(r, c, bl, s.b, tol=1e-8)
+    assert done and rel <= 1e-8 and threads >= 1
+    n = s.b.size
+    I, J, V = [], [], []
+    for kk in range(r.size):
+        B = bl[kk].reshape(3, 3).T
+        for a in range(3):
+            for bb in range(3):
+                I.append(3 * r[kk] + a); J.append(3 * c[kk] + bb); V.append(B[a, bb])
+                if r[kk] != c[kk]:
+                    I.append(3 * c[kk] + bb); J.append(3 * r[kk] + a); V.append(B[a, bb])
+    A = sp.csr_matrix((V, (I, J)), shape=(n, n))
+    xe = spl.spsolve(A.tocsc(), s.b)
+    assert np.linalg.norm(x - xe) <= 1e-6 * np.linalg.norm(xe)
