@@ -216,15 +216,25 @@ int stg_selftest_wait_timeout(int* status, double* seconds);
  * vol dt^2, as the tet's 10 upper 3x3 blocks (column-major) at triplets 10 t .. 10 t + 9.
  * Per vertex (triplet 10 tets + v): lumped mass rho vol / 4 plus the barrier Hessians of
  * the planes it is within dhat of.  b = dt^2 vol P : dF/dx + M (x - x - dt v - dt^2 g) +
- * barrier gradients, with g = (0, gravity_y, 0).  planes: [nplanes][6] = normal xyz,
- * offset (plane n.x = offset), dhat, kappa.  All arrays are device arrays; rows / cols /
- * blocks hold 10 tets + verts triplets, b 3 verts doubles. */
+ * barrier gradients, with g = (0, gravity_y, 0).  When xtilde (the inertial target
+ * x_n + dt v_n + dt^2 g of the step) is given, the kinetic gradient is M (x - xtilde) and
+ * vel is not read; later Newton iterations of a step pass it.  planes: [nplanes][6] =
+ * normal xyz, offset (plane n.x = offset), dhat, kappa.  All arrays are device arrays;
+ * rows / cols / blocks hold 10 tets + verts triplets, b 3 verts doubles. */
 size_t stg_fem_scratch_bytes(int verts, int tets);
-int stg_fem_newton_system(int verts, const double* rest, const double* pos, const double* vel, int tets,
-                          const int32_t* tet_verts, const double* youngs, double poisson, double density,
-                          double dt, double gravity_y, int nplanes, const double* planes, int32_t* rows,
-                          int32_t* cols, double* blocks, double* b, void* scratch, size_t scratch_bytes,
-                          void* stream);
+int stg_fem_newton_system(int verts, const double* rest, const double* pos, const double* vel,
+                          const double* xtilde, int tets, const int32_t* tet_verts, const double* youngs,
+                          double poisson, double density, double dt, double gravity_y, int nplanes,
+                          const double* planes, int32_t* rows, int32_t* cols, double* blocks, double* b,
+                          void* scratch, size_t scratch_bytes, void* stream);
+/* The objective those triplets are the Hessian of (the incremental potential):
+ * sum_tets dt^2 vol psi(F) + 1/2 sum_v m_v |x_v - xtilde_v|^2 + sum kappa b(d^2) over the
+ * (vertex, plane) pairs within dhat, b(s) = -(s - dhat^2)^2 log(s / dhat^2).  *violations
+ * (may be NULL) counts vertices on or behind a plane, where the potential is infinite. */
+int stg_fem_energy(int verts, const double* rest, const double* pos, const double* xtilde, int tets,
+                   const int32_t* tet_verts, const double* youngs, double poisson, double density, double dt,
+                   int nplanes, const double* planes, void* scratch, size_t scratch_bytes, double* energy,
+                   int* violations, void* stream);
 
 /* ---- BCOO tile autotuner -------------------------------------------------------------- */
 /* No counterpart in the reference.  Tile shape of the in-loop SpMV: rows_per_tile rows per

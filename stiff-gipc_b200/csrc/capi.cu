@@ -733,15 +733,26 @@ size_t stg_fem_scratch_bytes(int verts, int tets)
     return stg::fem_scratch_bytes(verts, tets);
 }
 
-int stg_fem_newton_system(int verts, const double* rest, const double* pos, const double* vel, int tets,
-                          const int32_t* tet_verts, const double* youngs, double poisson, double density,
-                          double dt, double gravity_y, int nplanes, const double* planes, int32_t* rows,
-                          int32_t* cols, double* blocks, double* b, void* scratch, size_t scratch_bytes,
-                          void* stream)
+int stg_fem_newton_system(int verts, const double* rest, const double* pos, const double* vel,
+                          const double* xtilde, int tets, const int32_t* tet_verts, const double* youngs,
+                          double poisson, double density, double dt, double gravity_y, int nplanes,
+                          const double* planes, int32_t* rows, int32_t* cols, double* blocks, double* b,
+                          void* scratch, size_t scratch_bytes, void* stream)
 {
     GUARD({
-        return stg::fem_newton_system(static_cast<cudaStream_t>(stream), verts, rest, pos, vel, tets, tet_verts, youngs,
-                                      poisson, density, dt, gravity_y, nplanes, planes, rows, cols, blocks, b, scratch,
-                                      scratch_bytes);
+        return stg::fem_newton_system(static_cast<cudaStream_t>(stream), verts, rest, pos, vel, xtilde, tets, tet_verts,
+                                      youngs, poisson, density, dt, gravity_y, nplanes, planes, rows, cols, blocks, b,
+                                      scratch, scratch_bytes);
+    })
+}
+
+int stg_fem_energy(int verts, const double* rest, const double* pos, const double* xtilde, int tets,
+                   const int32_t* tet_verts, const double* youngs, double poisson, double density, double dt,
+                   int nplanes, const double* planes, void* scratch, size_t scratch_bytes, double* energy,
+                   int* violations, void* stream)
+{
+    GUARD({
+        return stg::fem_energy(static_cast<cudaStream_t>(stream), verts, rest, pos, xtilde, tets, tet_verts, youngs,
+                               poisson, density, dt, nplanes, planes, scratch, scratch_bytes, energy, violations);
     })
 }

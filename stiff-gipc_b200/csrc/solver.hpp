@@ -182,9 +182,12 @@ struct Solver
 
 // Hessian producer (fem.cu): 10 T + V triplets and the gradient of one Newton iteration
 size_t fem_scratch_bytes(int V, int T);
-int fem_newton_system(cudaStream_t s, int V, const double* rest, const double* pos, const double* vel, int T,
-                      const int* tets, const double* E, double nu, double rho, double dt, double gy, int nplanes,
-                      const double* planes, int* rows, int* cols, double* blocks, double* b, void* scratch,
-                      size_t bytes);
+int fem_newton_system(cudaStream_t s, int V, const double* rest, const double* pos, const double* vel,
+                      const double* xtilde, int T, const int* tets, const double* E, double nu, double rho, double dt,
+                      double gy, int nplanes, const double* planes, int* rows, int* cols, double* blocks, double* b,
+                      void* scratch, size_t bytes);
+int fem_energy(cudaStream_t s, int V, const double* rest, const double* pos, const double* xtilde, int T,
+               const int* tets, const double* E, double nu, double rho, double dt, int nplanes, const double* planes,
+               void* scratch, size_t bytes, double* energy, int* violations);
 
 }  // namespace stg

@@ -101,8 +101,10 @@ def lib():
     L.stg_selftest_wait_timeout.argtypes = [C.POINTER(ci), C.POINTER(cd)]
     L.stg_spmv_tiles.argtypes = [vp, ci]
     L.stg_fem_scratch_bytes.argtypes = [ci, ci]
-    L.stg_fem_newton_system.argtypes = [ci, vp, vp, vp, ci, vp, vp, cd, cd, cd, cd, ci, vp, vp, vp, vp, vp, vp,
+    L.stg_fem_newton_system.argtypes = [ci, vp, vp, vp, vp, ci, vp, vp, cd, cd, cd, cd, ci, vp, vp, vp, vp, vp, vp,
                                         C.c_size_t, vp]
+    L.stg_fem_energy.argtypes = [ci, vp, vp, vp, ci, vp, vp, cd, cd, cd, ci, vp, vp, C.c_size_t, C.POINTER(cd),
+                                 C.POINTER(ci), vp]
     L.stg_spmv_tiles_info.argtypes = [vp, C.POINTER(ci), C.POINTER(C.c_float), C.POINTER(C.c_float)]
     L.stg_net_configure.argtypes = [vp, ci]
     L.stg_net_graph_info.argtypes = [vp, C.POINTER(ci), C.POINTER(ci)]

@@ -345,11 +345,12 @@ def _assemble(name, pos_rest, pos, tets, E, nu, rho, dt, vel, barriers, rng_cont
 def make_cube_drop(n: int = 16, seed: int = 1001, E: float = 1e5, nu: float = 0.45,
                    rho: float = 1000.0, dt: float = 1.0 / 60.0, v0: float = -2.0,
                    jitter: float = 1e-3, gap: float = 5e-4, dhat: float = 1e-3,
-                   kappa: float = 1e5) -> NewtonSystem:
+                   kappa: float = 1e5, state_only: bool = False) -> NewtonSystem:
     """Plain FP64 MAS-PCG workload, one Newton step: a 1 m cube of n^3 hexes (6 tets each),
     vertices jittered U(+-jitter) from ``seed``, falling at ``v0`` m/s in y, resting ``gap``
     above a ground plane with an IPC barrier (d_hat, kappa).  n=16: 4,913 vertices,
-    24,576 tets, 14,739 DOF."""
+    24,576 tets, 14,739 DOF.  state_only: the mesh state and material instead (the inputs of
+    _assemble, or of stgipc.newton for a trajectory)."""
     rng = np.random.default_rng(seed)
     pos, tets = cube_mesh(n, 1.0, origin=(0.0, gap, 0.0))
     pos = pos + rng.uniform(-jitter, jitter, size=pos.shape)
@@ -359,8 +360,11 @@ def make_cube_drop(n: int = 16, seed: int = 1001, E: float = 1e5, nu: float = 0.
     E_t = np.full(tets.shape[0], E)
     vel = np.zeros_like(pos)
     vel[:, 1] = v0
-    return _assemble(f"cube{n}_drop", pos, pos, tets, E_t, nu, rho, dt, vel,
-                     barriers=[((0.0, 1.0, 0.0), 0.0, dhat, kappa)])
+    state = dict(name=f"cube{n}_drop", pos_rest=pos, pos=pos, tets=tets, E=E_t, nu=nu, rho=rho, dt=dt, vel=vel,
+                 barriers=[((0.0, 1.0, 0.0), 0.0, dhat, kappa)])
+    if state_only:
+        return state
+    return _assemble(**state)
 
 
 def make_heterogeneous_cube(n: int = 48, seed: int = 1005, nu: float = 0.45, rho: float = 1000.0,
