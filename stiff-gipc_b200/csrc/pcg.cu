@@ -115,6 +115,47 @@ __device__ __forceinline__ double consume_sum(const PcgDev& c, int site, int cou
     return tot;
 }
 
+// Two such reductions in one pass (both partial arrays loaded together, one set of
+// barriers); each result is bitwise the one consume_sum gives.
+template <int BLOCK>
+__device__ __forceinline__ void consume_sum2(const PcgDev& c, int site_a, int count_a, int site_b, int count_b,
+                                             double& ra, double& rb)
+{
+    __shared__ double red[2][BLOCK / 32];
+    __shared__ double tot[2];
+    const double* pa = c.partials + (size_t)site_a * c.slots;
+    const double* pb = c.partials + (size_t)site_b * c.slots;
+    double a = 0, b = 0;
+    for(int t = threadIdx.x; t < count_a || t < count_b; t += BLOCK)
+    {
+        if(t < count_a) a += __ldcg(pa + t);
+        if(t < count_b) b += __ldcg(pb + t);
+    }
+    a = warp_sum(a);
+    b = warp_sum(b);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if(lane == 0)
+    {
+        red[0][warp] = a;
+        red[1][warp] = b;
+    }
+    __syncthreads();
+    if(warp == 0)
+    {
+        double x = lane < BLOCK / 32 ? red[0][lane] : 0.0, y = lane < BLOCK / 32 ? red[1][lane] : 0.0;
+        x = warp_sum(x);
+        y = warp_sum(y);
+        if(lane == 0)
+        {
+            tot[0] = x;
+            tot[1] = y;
+        }
+    }
+    __syncthreads();
+    ra = tot[0];
+    rb = tot[1];
+}
+
 // ---------------------------------------------------------------------------------------
 // block loads (16-byte vector loads of the padded layouts)
 // ---------------------------------------------------------------------------------------
@@ -843,9 +884,12 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T, RTT>::MIN_CTAS) k_phase_a_
     if(done) return;
     // beta = rz_k / rz_(k-1): rz_k from phase E's partials, rz_(k-1) as phase B recorded it
     // (the first iteration has p_0 = 0: beta = 0)
-    const double rz_new = consume_sum<A_THREADS>(c, SITE_E, c.grid_e);
     // flexible PCG (learned correction): beta = r_k.(z_k - z_(k-1)) / r_(k-1).z_(k-1)
-    const double rz_mix = c.flex && (long)s_iter > 0 ? consume_sum<A_THREADS>(c, SITE_F, c.grid_e) : 0.0;
+    double rz_new, rz_mix = 0.0;
+    if(c.flex && (long)s_iter > 0)
+        consume_sum2<A_THREADS>(c, SITE_E, c.grid_e, SITE_F, c.grid_e, rz_new, rz_mix);
+    else
+        rz_new = consume_sum<A_THREADS>(c, SITE_E, c.grid_e);
     const double s_beta = (long)s_iter == 0 ? 0.0 : (rz_new - rz_mix) / rz_old;
     int* meta = reinterpret_cast<int*>(asm_ + G::STAGES * G::STAGE);
     const unsigned sbase = smem_u32(asm_);
@@ -1161,8 +1205,8 @@ template <typename T, int B>
 __global__ void __launch_bounds__(PB, 8) k_phase_b(PcgDev c)
 {
     if(c.flags[F_DONE]) return;
-    const double pq = consume_sum<PB>(c, SITE_A, c.grid_a);
-    const double rz = consume_sum<PB>(c, SITE_E, c.grid_e);
+    double pq, rz;
+    consume_sum2<PB>(c, SITE_A, c.grid_a, SITE_E, c.grid_e, pq, rz);
     double v = 0;
     if(pq > 0.0 && isfinite(pq))  // else breakdown: no update; the last CTA reports it
     {
