@@ -86,6 +86,18 @@ struct DBuf
 
 inline int div_up(long a, long b) { return (int)((a + b - 1) / b); }
 
+// Kernel attributes are per device: true the first time a call site reaches it on the
+// current device (mask: one bit per device, owned by the call site, per host thread).
+inline bool first_on_device(unsigned long long& mask)
+{
+    int d = 0;
+    if(cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 64) return true;
+    const unsigned long long bit = 1ull << d;
+    if(mask & bit) return false;
+    mask |= bit;
+    return true;
+}
+
 // ------------------------------------------------------------------------------------
 // device helpers
 // ------------------------------------------------------------------------------------

@@ -1093,12 +1093,9 @@ Layout layout(int n, int S)
 
 int net_prepare()
 {
-    static thread_local bool done = false;
-    if(!done)
-    {
+    static thread_local unsigned long long done = 0;
+    if(first_on_device(done))
         STG_CUDA_TRY(cudaFuncSetAttribute(k_net_mp, cudaFuncAttributeMaxDynamicSharedMemorySize, MP_SMEM));
-        done = true;
-    }
     return 0;
 }
 

@@ -1650,12 +1650,9 @@ static int launch_mas_cd(Solver& S, const PcgDev& c)
     {
         // warp per bank, TMA-staged; one resident wave of CTAs
         const int smem = D_WARPS * D_WARP_BYTES;
-        static thread_local int attr_done = 0;
-        if(!attr_done)
-        {
+        static thread_local unsigned long long attr_done = 0;
+        if(first_on_device(attr_done))
             STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_d16, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            attr_done = 1;
-        }
         int per_sm = 0;
         STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase_d16, D_WARPS * 32, smem));
         const int grid = std::max(1, std::min(div_up(c.nbanks, D_WARPS), std::max(per_sm, 1) * kSMs));
@@ -1673,8 +1670,12 @@ static int launch_mas_cd(Solver& S, const PcgDev& c)
 template <typename T, int RT>
 static int phase_a_grid_rt(int nrows, int* grid)
 {
-    static thread_local int per_sm = -1;
-    if(per_sm < 0)
+    static thread_local unsigned long long seen = 0;
+    static thread_local int per_sm_dev[64];
+    int dev = 0;
+    STG_CUDA_TRY(cudaGetDevice(&dev));
+    int& per_sm = per_sm_dev[dev & 63];
+    if(first_on_device(seen))
     {
         STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_a_tiled<T, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           ATile<T, RT>::SMEM));
@@ -1845,8 +1846,8 @@ static int record_if_body(Solver& S, const PcgDev& c, int grid_rows, cudaGraph_t
 template <typename T, int B>
 static int set_carveouts()
 {
-    static thread_local bool done = false;
-    if(done) return 0;
+    static thread_local unsigned long long done = 0;
+    if(!first_on_device(done)) return 0;
     const int cv = cudaSharedmemCarveoutMaxShared;
     constexpr int BB = B > 0 ? B : 16;
     STG_CUDA_TRY(cudaFuncSetAttribute(k_init<T>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
@@ -1859,7 +1860,6 @@ static int set_carveouts()
     STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_d<BB>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
     STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_d16, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
     STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_e<T, B>, cudaFuncAttributePreferredSharedMemoryCarveout, cv));
-    done = true;
     return 0;
 }
 
