@@ -213,7 +213,7 @@ def run_batch(args):
     log-uniform in [4, 24] (375 to 46,875 DOFs each, 2.61 M in all), E log-uniform in
     [1e4, 1e7], each pressed 5e-4 into a ground barrier; one Newton solve each to
     ||r|| / ||b|| <= 1e-4 (FP32 path).  Whole scenes are sharded over the ranks by DOF
-    (stgipc.batch.shard_by_dof); each rank solves its shard over 8 streams.  value = ms per
+    (stgipc.batch.shard_by_dof); each rank solves its shard over --streams streams (8).  value = ms per
     batch, max over ranks (total work fixed: strong scaling)."""
     import torch
     import torch.distributed as dist
