@@ -152,3 +152,95 @@ def solve_distributed(systems, rank: int, world: int, solve_shard: Optional[Call
     if missing:
         raise RuntimeError(f"scenes {missing[:8]} were not solved")
     return out  # type: ignore[return-value]
+
+
+# ----------------------------------------------------------------------------------------
+# one system for the whole batch
+# ----------------------------------------------------------------------------------------
+class ConcatenatedBatch:
+    """The scenes of a batch as one block-diagonal system, solved by one handle: one
+    convert, one MAS hierarchy, one assembly and one graph-captured PCG for every scene.
+
+    Vertices, triplets, neighbour lists and MAS partitions of scene s are shifted by the
+    vertex count of the scenes before it, and every partition stays inside its scene, so
+    no bank mixes scenes at level 0; at coarser levels nodes of different scenes may share
+    a bank, but with no edges between them they are never merged and their bank matrix is
+    block-diagonal, so the preconditioner never couples scenes.  The PCG's scalars are
+    global; its stop test uses tol_eff = tol * min_s ||b_s|| / ||b||, so that
+    ||r_s|| <= ||r|| <= tol min_s ||b_s|| <= tol ||b_s|| for every scene s."""
+
+    def __init__(self, systems, config: Optional[PCGSolverConfig] = None, device="cuda", bank: int = 16):
+        import torch
+        self.systems = list(systems)
+        self.device = torch.device(device)
+        nv = [s.num_verts for s in self.systems]
+        self.voff = np.concatenate([[0], np.cumsum(nv)]).astype(np.int64)
+        V = int(self.voff[-1])
+        rows = np.concatenate([s.rows.astype(np.int64) + o for s, o in zip(self.systems, self.voff)]).astype(np.int32)
+        cols = np.concatenate([s.cols.astype(np.int64) + o for s, o in zip(self.systems, self.voff)]).astype(np.int32)
+        blocks = np.concatenate([s.blocks.reshape(-1, 9) for s in self.systems])
+        b = np.concatenate([s.b for s in self.systems])
+        # neighbour lists (CSR) and MAS partitions (Morton blocks of `bank` inside each scene)
+        starts, nums, lists, loff = [], [], [], 0
+        for s, o in zip(self.systems, self.voff):
+            starts.append(s.neighbor_start.astype(np.int64) + loff)
+            nums.append(s.neighbor_num.astype(np.int64))
+            lists.append(s.neighbor_list.astype(np.int64) + o)
+            loff += int(s.neighbor_list.size)
+        part = np.concatenate([np.arange(n) // bank for n in nv])
+        pcount = np.concatenate([[0], np.cumsum([(n + bank - 1) // bank for n in nv])])
+        part = part + np.repeat(pcount[:-1], nv)
+        first = np.searchsorted(part, part)  # first vertex of each vertex's partition
+        part_map = np.full(int(pcount[-1]) * bank, -1, np.int32)
+        slot = part * bank + (np.arange(V) - first)
+        part_map[slot] = np.arange(V, dtype=np.int32)
+        real_map = slot.astype(np.int32)
+        bb = np.array([float(s.b @ s.b) for s in self.systems])
+        self.tol = (config.global_tol_rate if config else 1e-4)
+        tol_eff = self.tol * float(np.sqrt(bb.min() / bb.sum())) if bb.sum() > 0 else self.tol
+        cfg = dataclasses_replace(config or PCGSolverConfig(), bank_size=bank, stop_rule="relative_residual",
+                                  global_tol_rate=tol_eff)
+        self.config = cfg
+        self.solver = Solver(cfg)
+        self.solver.mas_init(V, np.concatenate(starts).astype(np.uint32), np.concatenate(nums).astype(np.uint32),
+                             np.concatenate(lists).astype(np.uint32), part_map, real_map)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
+        self.rows, self.cols, self.blocks, self.b = t(rows), t(cols), t(blocks.reshape(-1)), t(b)
+        self.x = torch.zeros_like(self.b)
+        self.V = V
+
+    def solve(self, stats: bool = True) -> dict:
+        self.x.zero_()
+        return self.solver.solve_linear_system(self.rows, self.cols, self.blocks, self.b, self.x, stats=stats)
+
+    def solution(self, k: int) -> np.ndarray:
+        a, e = 3 * int(self.voff[k]), 3 * int(self.voff[k + 1])
+        return self.x[a:e].cpu().numpy()
+
+    def scene_residuals(self) -> np.ndarray:
+        """||b_s - A_s x_s|| / ||b_s|| of every scene, from the triplets in FP64 (a check
+        outside the solve: every triplet block and its transpose applied with gathers and
+        scatter-adds)."""
+        import torch
+        B = self.blocks.view(-1, 3, 3).transpose(1, 2)  # row-major blocks
+        r = self.rows.long()
+        c = self.cols.long()
+        X = self.x.view(-1, 3)
+        y = torch.zeros_like(X)
+        y.index_add_(0, r, torch.bmm(B, X[c].unsqueeze(2)).squeeze(2))
+        off = r != c
+        y.index_add_(0, c[off], torch.bmm(B[off].transpose(1, 2), X[r[off]].unsqueeze(2)).squeeze(2))
+        d = (self.b.view(-1, 3) - y).pow(2).sum(1)
+        bb = self.b.view(-1, 3).pow(2).sum(1)
+        seg = torch.from_numpy(np.repeat(np.arange(len(self.systems)), np.diff(self.voff))).to(self.device)
+        num = torch.zeros(len(self.systems), dtype=torch.float64, device=self.device).index_add_(0, seg, d)
+        den = torch.zeros(len(self.systems), dtype=torch.float64, device=self.device).index_add_(0, seg, bb)
+        return torch.sqrt(num / den).cpu().numpy()
+
+    def close(self):
+        self.solver.close()
+
+
+def dataclasses_replace(cfg, **kw):
+    import dataclasses
+    return dataclasses.replace(cfg, **kw)

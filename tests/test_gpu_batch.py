@@ -47,3 +47,26 @@ def test_solve_distributed_one_rank_on_gpu(dev):
                             streams=3)
     assert len(out) == len(sysl)
     assert all(o["rel_residual"] <= 1.5e-4 for o in out)
+
+
+def test_concatenated_batch_meets_every_scene_tolerance(dev):
+    """The whole batch as one block-diagonal system (one handle): every scene's own FP64
+    relative residual meets the tolerance, checked with the oracle's convert and SpMV; the
+    solutions agree with the scenes solved one by one to the tolerance's level."""
+    from oracle import oracle as orc
+    from stgipc import PCGSolverConfig, scenes
+    from stgipc.batch import ConcatenatedBatch
+    sysl = scenes.make_batched_cubes(count=12, seed=1004, n_lo=3, n_hi=9)
+    cfg = PCGSolverConfig(precision="fp32", stop_rule="relative_residual", global_tol_rate=1e-4)
+    cb = ConcatenatedBatch(sysl, cfg, device=dev)
+    st = cb.solve()
+    assert st["status"] == 0
+    res_gpu = cb.scene_residuals()
+    for k, s in enumerate(sysl):
+        r, c, bl = orc.convert(s.rows, s.cols, s.blocks)
+        x = cb.solution(k)
+        y = orc.spmv(r, c, bl, x)
+        rel = np.linalg.norm(s.b - y) / np.linalg.norm(s.b)
+        assert rel <= 1.1e-4, (k, rel)
+        assert abs(rel - res_gpu[k]) <= 1e-6 + 1e-3 * rel
+    cb.close()
