@@ -236,6 +236,19 @@ int stg_fem_energy(int verts, const double* rest, const double* pos, const doubl
                    int nplanes, const double* planes, void* scratch, size_t scratch_bytes, double* energy,
                    int* violations, void* stream);
 
+/* ---- independent scenes in one solve ---------------------------------------------------- */
+/* No counterpart in the reference.  The system of the following solves is a block-diagonal
+ * batch of independent scenes on contiguous block-row ranges [row_offsets[s],
+ * row_offsets[s + 1]) (host array of nseg + 1 entries, the last one the block-row count).
+ * Every scene runs its own PCG recurrence (its own alpha, beta and stop test
+ * ||r_s|| <= tol ||b_s||) inside the one graph-captured loop, which ends when every scene
+ * is done; a finished scene's rows stop changing.  Needs the relative-residual stop rule,
+ * the host or graph loop, no ABD bodies and no learned correction.  nseg = 0: one system. */
+int stg_set_segments(stg_handle h, const int32_t* row_offsets, int nseg);
+/* Per scene of the last solve (host arrays of nseg): iterations until its stop test held
+ * (0 if it never did) and ||r_s|| / ||b_s|| of its recurrence at the end. */
+int stg_segment_stats(stg_handle h, int* iterations, double* rel_residual);
+
 /* ---- BCOO tile autotuner -------------------------------------------------------------- */
 /* No counterpart in the reference.  Tile shape of the in-loop SpMV: rows_per_tile rows per
  * tile of the row-sliced full copy, with 256 / rows_per_tile lanes per row (FP32: 64 or 32;

@@ -756,3 +756,62 @@ int stg_fem_energy(int verts, const double* rest, const double* pos, const doubl
                                poisson, density, dt, nplanes, planes, scratch, scratch_bytes, energy, violations);
     })
 }
+
+int stg_set_segments(stg_handle h, const int32_t* row_offsets, int nseg)
+{
+    CHECK_HANDLE(h);
+    GUARD({
+        if(nseg < 0 || (nseg > 0 && !row_offsets))
+        {
+            stg::set_error("stg_set_segments: invalid arguments");
+            return STG_ERR_INVALID;
+        }
+        if(nseg == 0)
+        {
+            h->nseg = 0;
+            h->seg_off_host.clear();
+            return STG_OK;
+        }
+        if(row_offsets[0] != 0)
+        {
+            stg::set_error("stg_set_segments: the first offset must be 0");
+            return STG_ERR_INVALID;
+        }
+        for(int q = 0; q < nseg; q++)
+            if(row_offsets[q + 1] <= row_offsets[q])
+            {
+                stg::set_error("stg_set_segments: offsets must increase");
+                return STG_ERR_INVALID;
+            }
+        const int nrows = row_offsets[nseg];
+        std::vector<int> of(nrows);
+        for(int q = 0; q < nseg; q++)
+            for(int r = row_offsets[q]; r < row_offsets[q + 1]; r++) of[r] = q;
+        STG_TRY(h->seg_off.resize(nseg + 1));
+        STG_TRY(h->seg_of_row.resize(nrows));
+        STG_CUDA_TRY(cudaMemcpyAsync(h->seg_off.data(), row_offsets, sizeof(int) * (nseg + 1), cudaMemcpyHostToDevice, h->stream));
+        STG_CUDA_TRY(cudaMemcpyAsync(h->seg_of_row.data(), of.data(), sizeof(int) * nrows, cudaMemcpyHostToDevice, h->stream));
+        STG_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        h->seg_off_host.assign(row_offsets, row_offsets + nseg + 1);
+        h->nseg = nseg;
+        h->graph_dirty = true;
+        return STG_OK;
+    })
+}
+
+int stg_segment_stats(stg_handle h, int* iterations, double* rel_residual)
+{
+    CHECK_HANDLE(h);
+    if(h->nseg == 0 || h->seg_host.size() < (size_t)stg::SEG_N * h->nseg)
+    {
+        stg::set_error("stg_segment_stats: no scenes solved");
+        return STG_ERR_NOT_READY;
+    }
+    for(int q = 0; q < h->nseg; q++)
+    {
+        const double* S = h->seg_host.data() + (size_t)stg::SEG_N * q;
+        if(iterations) iterations[q] = (int)S[stg::SG_ITER];
+        if(rel_residual) rel_residual[q] = S[stg::SG_BB] > 0 ? std::sqrt(S[stg::SG_RR] / S[stg::SG_BB]) : 0.0;
+    }
+    return STG_OK;
+}

@@ -372,7 +372,10 @@ __device__ __forceinline__ double phase_b_mas(const PcgDev& c, int gt, int gn, d
         if(v >= 0)
         {
             double d0, d1, d2;
-            axpy_row<T>(c, pn, q, alpha, fem_row + v, d0, d1, d2, acc);
+            const int row = fem_row + v;
+            const double a = c.seg_of_row ? __ldcg(c.seg + SEG_N * c.seg_of_row[row] + SG_ALPHA) : alpha;
+            axpy_row<T>(c, pn, q, a, row, d0, d1, d2, acc);
+            if(c.seg_of_row) c.seg_row[(size_t)c.nrows + row] = d0 * d0 + d1 * d1 + d2 * d2;
             r0 = (float)d0;
             r1 = (float)d1;
             r2 = (float)d2;
@@ -421,7 +424,9 @@ __device__ __forceinline__ double phase_b_plain(const PcgDev& c, int gt, int gn,
     for(int i = gt; i < c.nrows; i += gn)
     {
         double d0, d1, d2;
-        axpy_row<T>(c, pn, q, alpha, i, d0, d1, d2, acc);
+        const double a = c.seg_of_row ? __ldcg(c.seg + SEG_N * c.seg_of_row[i] + SG_ALPHA) : alpha;
+        axpy_row<T>(c, pn, q, a, i, d0, d1, d2, acc);
+        if(c.seg_of_row) c.seg_row[(size_t)c.nrows + i] = d0 * d0 + d1 * d1 + d2 * d2;
     }
     return acc;
 }
@@ -1012,6 +1017,8 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T, RTT>::MIN_CTAS) k_phase_a_
             }
             T y0 = T(0), y1 = T(0), y2 = T(0), pn0 = T(0), pn1 = T(0), pn2 = T(0);
             bool hit = false;
+            // scenes: the row's own beta (its neighbours are in the same scene)
+            const T bta = (c.seg_of_row && i < r1) ? (T)__ldcg(c.seg + SEG_N * c.seg_of_row[i] + SG_BETA) : beta;
             for(int e0 = sub; e0 < d; e0 += 4 * LPR)
             {
                 T h8[4], x[4][3];
@@ -1036,7 +1043,7 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T, RTT>::MIN_CTAS) k_phase_a_
                 }
 #pragma unroll
                 for(int u = 0; u < 4; u++)
-                    if(e0 + u * LPR < d) a_gather<T>(j[u], zp, beta, x[u][0], x[u][1], x[u][2]);
+                    if(e0 + u * LPR < d) a_gather<T>(j[u], zp, bta, x[u][0], x[u][1], x[u][2]);
 #pragma unroll
                 for(int u = 0; u < 4; u++)
                 {
@@ -1077,10 +1084,12 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T, RTT>::MIN_CTAS) k_phase_a_
             T p2 = __shfl_sync(0xffffffffu, pn2, src);
             if(sub == 0 && i < r1)
             {
-                if(!hm) a_gather<T>(i, zp, beta, p0, p1, p2);
+                if(!hm) a_gather<T>(i, zp, bta, p0, p1, p2);
                 st4(zpn + 8 * (size_t)i + 4, p0, p1, p2);
                 st4(q + 4 * (size_t)i, y0, y1, y2);
-                acc += (double)p0 * (double)y0 + (double)p1 * (double)y1 + (double)p2 * (double)y2;
+                const double pq = (double)p0 * (double)y0 + (double)p1 * (double)y1 + (double)p2 * (double)y2;
+                acc += pq;
+                if(c.seg_of_row) c.seg_row[i] = pq;
             }
         }
         if(failed && lane == 0)
@@ -1138,7 +1147,9 @@ __device__ __forceinline__ double phase_e_mas(const PcgDev& c, int gt, int gn)
         const int row = fem_row + v;
         st4(zp + 8 * (size_t)row, (T)c0, (T)c1, (T)c2);
         const double* r = c.r + 3 * (size_t)row;
-        acc += r[0] * (double)(T)c0 + r[1] * (double)(T)c1 + r[2] * (double)(T)c2;
+        const double rz = r[0] * (double)(T)c0 + r[1] * (double)(T)c1 + r[2] * (double)(T)c2;
+        acc += rz;
+        if(c.seg_of_row) c.seg_row[2 * (size_t)c.nrows + row] = rz;
     }
     return acc + abd_apply<T>(c, zp, gt, gn);
 }
@@ -1161,7 +1172,9 @@ __device__ __forceinline__ double phase_e_plain(const PcgDev& c, int gt, int gn)
             z2 = D[2] * r0 + D[5] * r1 + D[8] * r2;
         }
         st4(zp + 8 * (size_t)bi, (T)z0, (T)z1, (T)z2);
-        acc += r0 * (double)(T)z0 + r1 * (double)(T)z1 + r2 * (double)(T)z2;
+        const double rz = r0 * (double)(T)z0 + r1 * (double)(T)z1 + r2 * (double)(T)z2;
+        acc += rz;
+        if(c.seg_of_row) c.seg_row[2 * (size_t)c.nrows + bi] = rz;
     }
     return acc + abd_apply<T>(c, zp, gt, gn);
 }
@@ -1355,6 +1368,100 @@ __global__ void __launch_bounds__(PB, 8) k_phase_e(PcgDev c, int op)
         }
         const double bo = block_sum<PB>(vo, red);
         if(threadIdx.x == 0) c.partials[(size_t)SITE_F * c.slots + blockIdx.x] = bo;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// independent scenes (PcgDev::seg_of_row): one CTA per scene sums the scene's per-row
+// contributions in row order and updates its scalars
+//   SEG_INIT after the first preconditioner application: r.z, b.b, beta = 0
+//   SEG_A    after the SpMV phase: p.q, alpha = r.z / p.q (0 once the scene is done)
+//   SEG_B    after the x / r update: r.r and the scene's stop test; the last CTA ends the
+//            loop when every scene is done
+//   SEG_E    after the preconditioner: beta = r.z_new / r.z, r.z = r.z_new
+// ---------------------------------------------------------------------------------------
+enum SegMode : int
+{
+    SEG_INIT = 0,
+    SEG_A = 1,
+    SEG_B = 2,
+    SEG_E = 3
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(PB) k_seg(PcgDev c)
+{
+    __shared__ double red[PB / 32];
+    __shared__ bool last;
+    if(MODE != SEG_INIT && __ldcg(c.flags + F_DONE)) return;
+    const int sc = blockIdx.x;
+    const int r0 = c.seg_row_off[sc], r1 = c.seg_row_off[sc + 1];
+    double* S = c.seg + SEG_N * (size_t)sc;
+    const double* src = c.seg_row + (size_t)(MODE == SEG_A ? 0 : (MODE == SEG_B ? 1 : 2)) * c.nrows;
+    double v = 0, bb = 0;
+    for(int i = r0 + threadIdx.x; i < r1; i += PB) v += __ldcg(src + i);
+    if(MODE == SEG_INIT)
+        for(int i = 3 * r0 + threadIdx.x; i < 3 * r1; i += PB) bb += c.b[i] * c.b[i];
+    v = block_sum<PB>(v, red);
+    if(MODE == SEG_INIT) bb = block_sum<PB>(bb, red);
+    if(threadIdx.x == 0)
+    {
+        if(MODE == SEG_INIT)
+        {
+            S[SG_RZ] = v;
+            S[SG_BB] = bb;
+            S[SG_BETA] = 0.0;
+            S[SG_ALPHA] = 0.0;
+            S[SG_RR] = bb;
+            S[SG_DONE] = bb > 0.0 ? 0.0 : 1.0;
+            S[SG_ITER] = 0.0;
+        }
+        else if(MODE == SEG_A)
+        {
+            S[SG_PQ] = v;
+            // a scene whose p.q is not positive stops (no update), the others go on
+            const bool go = S[SG_DONE] == 0.0 && v > 0.0 && isfinite(v);
+            S[SG_ALPHA] = go ? S[SG_RZ] / v : 0.0;
+            if(!go && S[SG_DONE] == 0.0)
+            {
+                S[SG_DONE] = 1.0;
+                S[SG_ITER] = __ldcg(c.scal + SS_ITER);
+            }
+        }
+        else if(MODE == SEG_E)
+        {
+            if(S[SG_DONE] == 0.0) S[SG_BETA] = S[SG_RZ] != 0.0 ? v / S[SG_RZ] : 0.0;
+            S[SG_RZ] = v;
+        }
+        else
+        {
+            S[SG_RR] = v;
+            if(S[SG_DONE] == 0.0 && v <= c.seg_tol2 * S[SG_BB])
+            {
+                S[SG_DONE] = 1.0;
+                S[SG_ITER] = __ldcg(c.scal + SS_ITER);
+            }
+            __threadfence();
+            last = atomicAdd(c.counters + 6, 1u) == (unsigned)(gridDim.x - 1);
+        }
+    }
+    if(MODE != SEG_B) return;
+    __syncthreads();
+    if(!last) return;
+    __threadfence();
+    double open = 0;
+    for(int q = threadIdx.x; q < c.nseg; q += PB) open += __ldcg(c.seg + SEG_N * (size_t)q + SG_DONE) == 0.0 ? 1.0 : 0.0;
+    open = block_sum<PB>(open, red);
+    if(threadIdx.x == 0)
+    {
+        if(open == 0.0)
+        {
+            c.flags[F_DONE] = 1;
+            c.flags[F_STATUS] = 0;
+            if(c.use_cond) cudaGraphSetConditional(c.h_while, 0u);
+        }
+        c.counters[6] = 0u;
+        __threadfence();
     }
 }
 
@@ -1776,9 +1883,21 @@ static int launch_iteration(Solver& S, const PcgDev& c, int grid_vec, int grid_r
     cudaStream_t s = S.stream;
     const bool fp32 = sizeof(T) == 4;
     STG_TRY(launch_phase_a<T>(c, s));
+    if(c.seg_of_row)
+    {
+        k_seg<SEG_A><<<c.nseg, PB, 0, s>>>(c);
+        STG_LAUNCH_CHECK();
+        S.launches++;
+    }
     k_phase_b<T, B><<<B > 0 ? std::max(1, std::min(div_up(c.M, PB), kSMs * 4)) : grid_vec, PB, 0, s>>>(c);
     STG_LAUNCH_CHECK();
     S.launches += 2;
+    if(c.seg_of_row)
+    {
+        k_seg<SEG_B><<<c.nseg, PB, 0, s>>>(c);
+        STG_LAUNCH_CHECK();
+        S.launches++;
+    }
     if(fp32 && c.prm.refine > 0)
     {
         if(in_graph_cond)
@@ -1818,6 +1937,12 @@ static int launch_iteration(Solver& S, const PcgDev& c, int grid_vec, int grid_r
     k_phase_e<T, B><<<grid_vec, PB, 0, s>>>(c, POST_BETA);
     STG_LAUNCH_CHECK();
     S.launches++;
+    if(c.seg_of_row)
+    {
+        k_seg<SEG_E><<<c.nseg, PB, 0, s>>>(c);
+        STG_LAUNCH_CHECK();
+        S.launches++;
+    }
     return 0;
 }
 
@@ -1898,6 +2023,12 @@ static int pcg_run(Solver& S, PcgDev& c, int& h_done)
     k_phase_e<T, B><<<grid_vec, PB, 0, s>>>(c, POST_INIT_RZ);
     STG_LAUNCH_CHECK();
     S.launches++;
+    if(c.seg_of_row)
+    {
+        k_seg<SEG_INIT><<<c.nseg, PB, 0, s>>>(c);
+        STG_LAUNCH_CHECK();
+        S.launches++;
+    }
 
     int h_flags[4] = {0, 0, 0, 0};
     const long max_iter = c.prm.max_iter;
@@ -2224,6 +2355,25 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
         }
         c.a_rt = tuned_rt;
     }
+    if(nseg > 0)
+    {
+        if(seg_off_host.back() != bcoo.nrows || abd_bodies > 0 || cfg.loop_mode == STG_LOOP_PERSISTENT ||
+           cfg.learned || cfg.stop_rule != STG_STOP_RELATIVE_RESIDUAL)
+        {
+            set_error("stg_pcg_solve: scenes need their offsets to end at the block-row count, no ABD bodies, the host "
+                      "or graph loop, no learned correction and the relative-residual stop rule");
+            return STG_ERR_INVALID;
+        }
+        STG_TRY(seg_row.resize(3 * (size_t)bcoo.nrows));
+        STG_TRY(seg_scal.resize((size_t)SEG_N * nseg));
+        c.seg_of_row = seg_of_row.data();
+        c.seg_row_off = seg_off.data();
+        c.seg = seg_scal.data();
+        c.seg_row = seg_row.data();
+        c.nseg = nseg;
+        c.seg_tol2 = cfg.tol * cfg.tol;
+        c.prm.tol = 0.0;  // the scenes' own tests end the loop
+    }
     const bool net_apply = cfg.learned != 0, net_rec = learned.rec_cap > 0;
     if(net_apply || net_rec)
     {
@@ -2314,6 +2464,12 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
         st->replacements = h_flags[F_REPL];
         st->learned_accepted = h_flags[F_LACC];
         st->learned_rejected = h_flags[F_LREJ];
+    }
+    if(nseg > 0)
+    {
+        seg_host.resize((size_t)SEG_N * nseg);
+        STG_CUDA_TRY(cudaMemcpyAsync(seg_host.data(), seg_scal.data(), sizeof(double) * SEG_N * nseg, cudaMemcpyDeviceToHost, s));
+        STG_CUDA_TRY(cudaStreamSynchronize(s));
     }
     return status;
 }

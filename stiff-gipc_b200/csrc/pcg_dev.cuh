@@ -5,6 +5,11 @@
 namespace stg
 {
 constexpr int kMaxLevelsDev = 6;
+// per-scene scalar slots of PcgDev::seg
+enum : int
+{
+    SG_RZ = 0, SG_PQ = 1, SG_ALPHA = 2, SG_BETA = 3, SG_RR = 4, SG_BB = 5, SG_DONE = 6, SG_ITER = 7, SEG_N = 8
+};
 
 // Everything a phase needs, passed by value.
 struct PcgDev
@@ -63,6 +68,14 @@ struct PcgDev
     // learned coarse correction: flexible PCG (beta from r_(k+1).(z_(k+1) - z_k), phase E's
     // r.z_old partials at SITE_F); the rest only keys the captured graph
     int a_rt;                 // rows per tile of the SpMV phase (one of the compiled shapes)
+    // independent systems (scenes) on contiguous block-row ranges, each with its own PCG
+    // scalars and stop test; null seg_of_row: one system
+    const int* seg_of_row;    // [nrows] scene of each block row
+    const int* seg_row_off;   // [nseg + 1] first block row of each scene
+    double* seg;              // [nseg][SEG_N] per-scene scalars (SG_* slots)
+    double* seg_row;          // [3][nrows] per-row p.q, r.r, r.z contributions
+    int nseg;
+    double seg_tol2;          // per-scene stop: r.r <= seg_tol2 * b.b
     int flex;
     int net_mode;             // bit 0: network applied, bit 1: samples recorded
     int net_n, net_rec_cap, net_rec_every;

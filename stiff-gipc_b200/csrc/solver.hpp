@@ -160,6 +160,12 @@ struct Solver
     bool pcg_ready = false;
     // SpMV tile shape: spmv_rt > 0 fixes the rows per tile; spmv_rt == 0 with spmv_tune set
     // times the candidates at the next solve of a new shape and keeps the fastest
+    // independent scenes on contiguous block-row ranges (stg_set_segments)
+    int nseg = 0;
+    std::vector<int> seg_off_host;    // [nseg + 1]
+    std::vector<double> seg_host;     // [nseg][SEG_N] after the last solve
+    DBuf<int> seg_off, seg_of_row;
+    DBuf<double> seg_scal, seg_row;
     int spmv_rt = 0;
     bool spmv_tune = false;
     int tuned_rt = 0, tuned_prec = -1, tuned_nrows = -1, tuned_nnzb = -1;

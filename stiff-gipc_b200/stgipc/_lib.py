@@ -100,6 +100,8 @@ def lib():
     L.stg_spmv_noalloc.argtypes = [cd, vp, vp, vp, ci, vp, cd, vp, ci, vp]
     L.stg_selftest_wait_timeout.argtypes = [C.POINTER(ci), C.POINTER(cd)]
     L.stg_spmv_tiles.argtypes = [vp, ci]
+    L.stg_set_segments.argtypes = [vp, vp, ci]
+    L.stg_segment_stats.argtypes = [vp, vp, vp]
     L.stg_fem_scratch_bytes.argtypes = [ci, ci]
     L.stg_fem_newton_system.argtypes = [ci, vp, vp, vp, vp, ci, vp, vp, cd, cd, cd, cd, ci, vp, vp, vp, vp, vp, vp,
                                         C.c_size_t, vp]

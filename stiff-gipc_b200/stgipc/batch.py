@@ -107,6 +107,11 @@ class BatchSolver:
         d2h = sum(t["x"].numel() * t["x"].element_size() for _, _, t, _ in self.items)
         return h2d, d2h
 
+    def scene_stats(self):
+        """(iterations, recurrence relative residual) per scene of the last solve
+        (per-scene mode)."""
+        return self.solver.segment_stats()
+
     def solution(self, k: int) -> np.ndarray:
         return self.items[k][2]["x"].cpu().numpy()
 
@@ -165,11 +170,15 @@ class ConcatenatedBatch:
     vertex count of the scenes before it, and every partition stays inside its scene, so
     no bank mixes scenes at level 0; at coarser levels nodes of different scenes may share
     a bank, but with no edges between them they are never merged and their bank matrix is
-    block-diagonal, so the preconditioner never couples scenes.  The PCG's scalars are
-    global; its stop test uses tol_eff = tol * min_s ||b_s|| / ||b||, so that
+    block-diagonal, so the preconditioner never couples scenes.
+
+    per_scene=True (stg_set_segments): every scene runs its own recurrence (alpha, beta,
+    stop test ||r_s|| <= tol ||b_s||) inside the one loop.  per_scene=False: one recurrence
+    with global scalars and the stop test tightened to tol min_s ||b_s|| / ||b||, so that
     ||r_s|| <= ||r|| <= tol min_s ||b_s|| <= tol ||b_s|| for every scene s."""
 
-    def __init__(self, systems, config: Optional[PCGSolverConfig] = None, device="cuda", bank: int = 16):
+    def __init__(self, systems, config: Optional[PCGSolverConfig] = None, device="cuda", bank: int = 16,
+                 per_scene: bool = True):
         import torch
         self.systems = list(systems)
         self.device = torch.device(device)
@@ -197,13 +206,16 @@ class ConcatenatedBatch:
         real_map = slot.astype(np.int32)
         bb = np.array([float(s.b @ s.b) for s in self.systems])
         self.tol = (config.global_tol_rate if config else 1e-4)
-        tol_eff = self.tol * float(np.sqrt(bb.min() / bb.sum())) if bb.sum() > 0 else self.tol
+        self.per_scene = per_scene
+        tol_eff = self.tol if per_scene else (self.tol * float(np.sqrt(bb.min() / bb.sum())) if bb.sum() > 0 else self.tol)
         cfg = dataclasses_replace(config or PCGSolverConfig(), bank_size=bank, stop_rule="relative_residual",
                                   global_tol_rate=tol_eff)
         self.config = cfg
         self.solver = Solver(cfg)
         self.solver.mas_init(V, np.concatenate(starts).astype(np.uint32), np.concatenate(nums).astype(np.uint32),
                              np.concatenate(lists).astype(np.uint32), part_map, real_map)
+        if per_scene:
+            self.solver.set_segments(self.voff.astype(np.int32))
         t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
         self.rows, self.cols, self.blocks, self.b = t(rows), t(cols), t(blocks.reshape(-1)), t(b)
         self.x = torch.zeros_like(self.b)
@@ -212,6 +224,11 @@ class ConcatenatedBatch:
     def solve(self, stats: bool = True) -> dict:
         self.x.zero_()
         return self.solver.solve_linear_system(self.rows, self.cols, self.blocks, self.b, self.x, stats=stats)
+
+    def scene_stats(self):
+        """(iterations, recurrence relative residual) per scene of the last solve
+        (per-scene mode)."""
+        return self.solver.segment_stats()
 
     def solution(self, k: int) -> np.ndarray:
         a, e = 3 * int(self.voff[k]), 3 * int(self.voff[k + 1])

@@ -192,6 +192,25 @@ class Solver:
         return dict(fine_mask=fine, prefix_orig=pref, coarse_tables=ct.reshape(L, V), going_next=gn,
                     coarse_table=tab.reshape(V, max(L - 1, 1)), level_size=ls)
 
+    # -- independent scenes in one solve (stg_set_segments) --------------------------------------
+    def set_segments(self, row_offsets):
+        """Block-row offsets of the scenes of a block-diagonal batch (nseg + 1 entries);
+        None or empty: one system."""
+        if row_offsets is None or len(row_offsets) == 0:
+            check(_L.lib().stg_set_segments(self.h, None, 0), "stg_set_segments")
+            self._nseg = 0
+            return
+        off = np.ascontiguousarray(row_offsets, np.int32)
+        check(_L.lib().stg_set_segments(self.h, off.ctypes.data, int(off.size - 1)), "stg_set_segments")
+        self._nseg = int(off.size - 1)
+
+    def segment_stats(self):
+        """(iterations, relative residual of the recurrence) per scene of the last solve."""
+        it = np.zeros(self._nseg, np.int32)
+        rel = np.zeros(self._nseg, np.float64)
+        check(_L.lib().stg_segment_stats(self.h, it.ctypes.data, rel.ctypes.data), "stg_segment_stats")
+        return it, rel
+
     # -- BCOO tile autotuner -------------------------------------------------------------------
     def spmv_tiles(self, rows_per_tile: int):
         """0: autotune at the next solve of a new shape; -1: default; else a fixed shape."""
