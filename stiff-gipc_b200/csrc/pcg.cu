@@ -50,6 +50,9 @@ enum Site : int
     SITE_INIT_RZ = 5,
     SITE_F = 6  // r_(k+1).z_k of phase E (flexible PCG)
 };
+// last-CTA counters (PcgDev::counters): one per reduction site finished by its producer,
+// plus the scenes' stop test (k_seg<SEG_B>)
+constexpr int CNT_SEG = 6;
 
 // ---------------------------------------------------------------------------------------
 // reductions: last CTA finishes, optionally drives the graph's conditional nodes
@@ -1442,7 +1445,7 @@ __global__ void __launch_bounds__(PB) k_seg(PcgDev c)
                 S[SG_ITER] = __ldcg(c.scal + SS_ITER);
             }
             __threadfence();
-            last = atomicAdd(c.counters + 6, 1u) == (unsigned)(gridDim.x - 1);
+            last = atomicAdd(c.counters + CNT_SEG, 1u) == (unsigned)(gridDim.x - 1);
         }
     }
     if(MODE != SEG_B) return;
@@ -1460,7 +1463,7 @@ __global__ void __launch_bounds__(PB) k_seg(PcgDev c)
             c.flags[F_STATUS] = 0;
             if(c.use_cond) cudaGraphSetConditional(c.h_while, 0u);
         }
-        c.counters[6] = 0u;
+        c.counters[CNT_SEG] = 0u;
         __threadfence();
     }
 }
