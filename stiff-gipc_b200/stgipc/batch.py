@@ -162,6 +162,37 @@ def solve_distributed(systems, rank: int, world: int, solve_shard: Optional[Call
 # ----------------------------------------------------------------------------------------
 # one system for the whole batch
 # ----------------------------------------------------------------------------------------
+def concat_inputs(systems, bank: int = 16) -> dict:
+    """The host arrays of the block-diagonal system of `systems`: triplets with block rows
+    shifted by the vertices of the scenes before, concatenated gradients, CSR neighbour
+    lists shifted the same way, and Morton partitions of `bank` vertices that never cross a
+    scene (part_map with -1 padding, real_map = slot of each vertex, as set_mas_partition
+    lays them out).  voff[s] is the first vertex (block row) of scene s."""
+    nv = [s.num_verts for s in systems]
+    voff = np.concatenate([[0], np.cumsum(nv)]).astype(np.int64)
+    V = int(voff[-1])
+    rows = np.concatenate([s.rows.astype(np.int64) + o for s, o in zip(systems, voff)]).astype(np.int32)
+    cols = np.concatenate([s.cols.astype(np.int64) + o for s, o in zip(systems, voff)]).astype(np.int32)
+    blocks = np.concatenate([s.blocks.reshape(-1, 9) for s in systems])
+    b = np.concatenate([s.b for s in systems])
+    starts, nums, lists, loff = [], [], [], 0
+    for s, o in zip(systems, voff):
+        starts.append(s.neighbor_start.astype(np.int64) + loff)
+        nums.append(s.neighbor_num.astype(np.int64))
+        lists.append(s.neighbor_list.astype(np.int64) + o)
+        loff += int(s.neighbor_list.size)
+    part = np.concatenate([np.arange(n) // bank for n in nv])
+    pcount = np.concatenate([[0], np.cumsum([(n + bank - 1) // bank for n in nv])])
+    part = part + np.repeat(pcount[:-1], nv)
+    first = np.searchsorted(part, part)  # first vertex of each vertex's partition
+    part_map = np.full(int(pcount[-1]) * bank, -1, np.int32)
+    slot = part * bank + (np.arange(V) - first)
+    part_map[slot] = np.arange(V, dtype=np.int32)
+    return dict(voff=voff, V=V, rows=rows, cols=cols, blocks=blocks, b=b, part_map=part_map,
+                real_map=slot.astype(np.int32), neighbor_start=np.concatenate(starts).astype(np.uint32),
+                neighbor_num=np.concatenate(nums).astype(np.uint32), neighbor_list=np.concatenate(lists).astype(np.uint32))
+
+
 class ConcatenatedBatch:
     """The scenes of a batch as one block-diagonal system, solved by one handle: one
     convert, one MAS hierarchy, one assembly and one graph-captured PCG for every scene.
@@ -182,28 +213,12 @@ class ConcatenatedBatch:
         import torch
         self.systems = list(systems)
         self.device = torch.device(device)
-        nv = [s.num_verts for s in self.systems]
-        self.voff = np.concatenate([[0], np.cumsum(nv)]).astype(np.int64)
-        V = int(self.voff[-1])
-        rows = np.concatenate([s.rows.astype(np.int64) + o for s, o in zip(self.systems, self.voff)]).astype(np.int32)
-        cols = np.concatenate([s.cols.astype(np.int64) + o for s, o in zip(self.systems, self.voff)]).astype(np.int32)
-        blocks = np.concatenate([s.blocks.reshape(-1, 9) for s in self.systems])
-        b = np.concatenate([s.b for s in self.systems])
-        # neighbour lists (CSR) and MAS partitions (Morton blocks of `bank` inside each scene)
-        starts, nums, lists, loff = [], [], [], 0
-        for s, o in zip(self.systems, self.voff):
-            starts.append(s.neighbor_start.astype(np.int64) + loff)
-            nums.append(s.neighbor_num.astype(np.int64))
-            lists.append(s.neighbor_list.astype(np.int64) + o)
-            loff += int(s.neighbor_list.size)
-        part = np.concatenate([np.arange(n) // bank for n in nv])
-        pcount = np.concatenate([[0], np.cumsum([(n + bank - 1) // bank for n in nv])])
-        part = part + np.repeat(pcount[:-1], nv)
-        first = np.searchsorted(part, part)  # first vertex of each vertex's partition
-        part_map = np.full(int(pcount[-1]) * bank, -1, np.int32)
-        slot = part * bank + (np.arange(V) - first)
-        part_map[slot] = np.arange(V, dtype=np.int32)
-        real_map = slot.astype(np.int32)
+        cat = concat_inputs(self.systems, bank)
+        self.voff = cat["voff"]
+        V = cat["V"]
+        rows, cols, blocks, b = cat["rows"], cat["cols"], cat["blocks"], cat["b"]
+        part_map, real_map = cat["part_map"], cat["real_map"]
+        starts, nums, lists = [cat["neighbor_start"]], [cat["neighbor_num"]], [cat["neighbor_list"]]
         bb = np.array([float(s.b @ s.b) for s in self.systems])
         self.tol = (config.global_tol_rate if config else 1e-4)
         self.per_scene = per_scene

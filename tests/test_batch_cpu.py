@@ -91,3 +91,39 @@ def test_solve_distributed_gloo_two_ranks(tmp_path):
     # the same as solving everything on one rank
     ref = _oracle_shard(_scenes(7))
     assert r0["out"] == ref
+
+
+def test_concatenated_inputs():
+    """The block-diagonal batch's host arrays: triplets and neighbours shifted per scene,
+    every partition inside one scene, part_map / real_map inverse to each other and equal
+    to each scene's own slot maps shifted by its partitions."""
+    from stgipc import scenes
+    from stgipc.batch import concat_inputs
+    sysl = scenes.make_batched_cubes(count=5, seed=1004, n_lo=2, n_hi=5)
+    cat = concat_inputs(sysl, 16)
+    voff = cat["voff"]
+    V = cat["V"]
+    assert V == sum(s.num_verts for s in sysl)
+    pm, rm = cat["part_map"], cat["real_map"]
+    assert np.all(pm[rm] == np.arange(V))
+    assert np.count_nonzero(pm >= 0) == V
+    scene_of = np.repeat(np.arange(len(sysl)), np.diff(voff))
+    for bank in range(pm.size // 16):
+        members = pm[16 * bank:16 * bank + 16]
+        members = members[members >= 0]
+        assert np.unique(scene_of[members]).size <= 1
+    soff = 0
+    for k, s in enumerate(sysl):
+        pm_s, rm_s = s.slot_maps(16)
+        np.testing.assert_array_equal(rm[voff[k]:voff[k + 1]], rm_s + soff)
+        soff += pm_s.size
+        a, e = 3 * voff[k], 3 * voff[k + 1]
+        np.testing.assert_array_equal(cat["b"][a:e], s.b)
+    r = cat["rows"]
+    assert np.all(scene_of[r] == scene_of[cat["cols"]])  # no coupling block between scenes
+    nl = cat["neighbor_list"].astype(np.int64)
+    ns = cat["neighbor_start"].astype(np.int64)
+    nn = cat["neighbor_num"].astype(np.int64)
+    for v in range(0, V, 7):
+        nb = nl[ns[v]:ns[v] + nn[v]]
+        assert np.all(scene_of[nb] == scene_of[v])
