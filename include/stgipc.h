@@ -86,8 +86,9 @@ typedef struct stg_stats
     int levels;             /* MAS levelnum                                          */
     int total_clusters;     /* MAS totalNumberClusters                               */
     int replacements;       /* FP64 residual replacements (FP32 mode)                */
-    int learned_accepted;   /* residual replacements at which the FP64 residual had
-                               fallen since the previous one with the learned correction on */
+    int learned_accepted;   /* checks (residual replacements, or every refine_interval
+                               FP64 iterations) at which the FP64 residual had fallen since
+                               the previous one with the learned correction on          */
     int learned_rejected;   /* ... had not: the correction was switched off (0 or 1)   */
     float ms_convert;       /* device time per phase (CUDA events; 0 if not timed)   */
     float ms_mas_build;
@@ -287,8 +288,9 @@ int stg_spmv_noalloc(double a, const double* blocks, const int32_t* rows,
  * network (hidden width 64, BF16 weights, FP32 accumulation) over the nodes of one coarse
  * MAS level predicts a correction of that level's bank solve: z_l = D_l^-1 r_l + s d(r_l),
  * inside a flexible PCG (beta = r_k.(z_k - z_(k-1)) / r_(k-1).z_(k-1)).  At every FP64
- * residual replacement the correction must have lowered the true residual since the
- * previous one, else the solve continues with plain MAS (stg_stats.learned_*).
+ * residual replacement (FP32 path), or every refine_interval iterations of the FP64
+ * recurrence (FP64 path), the FP64 residual must have fallen since the previous check,
+ * else the solve continues with plain MAS (stg_stats.learned_*).
  * Parameters are one FP32 vector of STG_NET_PARAMS floats, every weight matrix stored
  * [out][in]: W0 [64][16] at 0, b0 [64] at 1024, W1..W3 [64][128] at 1088 + 8192 k, b1..b3
  * [64] at 25664 + 64 k, Wo [8][64] at 25856, bo [8] at 26368 (outputs 3..7 unused). */

@@ -2403,6 +2403,7 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
         }
         STG_TRY(net_prepare());
         c.flex = net_apply ? 1 : 0;
+        c.prm.judge = (net_apply && c.prm.refine == 0) ? std::max(1, cfg.refine_interval) : 0;
         c.net_mode = (net_apply ? 1 : 0) | (net_rec ? 2 : 0);
         c.net_n = learned.graph.n;
         c.net_rec_cap = learned.rec_cap;

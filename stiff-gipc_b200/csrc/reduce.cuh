@@ -12,6 +12,8 @@ struct PcgParams
     long max_iter;     // (long)(max_iter_ratio * n) as PCGSolver::solve computes it
     int stop_rule;     // 0: |rz| <= tol * rz0 (reference), 1: ||r|| <= tol ||b||
     int refine;        // FP32 mode residual replacement interval (0 = off)
+    int judge;         // learned correction without replacements (FP64): judge the recursive
+                       // FP64 residual every `judge` iterations (0 = off)
 };
 
 enum PostOp : int
@@ -104,6 +106,18 @@ __device__ __forceinline__ void post_op(int op, int slot, double total, double* 
             {
                 k += 1;
                 scal[SS_ITER] = (double)k;
+                if(p.judge > 0 && flags[F_LEARN] && k % p.judge == 0)
+                {
+                    // FP64 recurrence: its residual judges the learned correction directly
+                    if(total < scal[SS_LRR])
+                        flags[F_LACC] += 1;
+                    else
+                    {
+                        flags[F_LREJ] += 1;
+                        flags[F_LEARN] = 0;
+                    }
+                    scal[SS_LRR] = total;
+                }
             }
             bool conv;
             if(p.stop_rule == 0)
