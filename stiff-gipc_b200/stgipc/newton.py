@@ -14,6 +14,8 @@ from __future__ import annotations
 import dataclasses
 from typing import List, Optional
 
+import numpy as np
+
 from .fem import FemScene
 
 
@@ -81,10 +83,29 @@ def step(scene: FemScene, solver, tol: float = 1e-6, max_newton: int = 30) -> St
     return StepStats(it, pcg, halvings, min_plane_distance(scene, x))
 
 
+def save_checkpoint(path: str, positions, velocities, step: int):
+    """A trajectory checkpoint: positions and velocities after each step so far (FP64,
+    [steps][V][3]) and the number of steps they cover."""
+    np.savez(path, pos=np.asarray(positions), vel=np.asarray(velocities), step=np.int64(step))
+
+
+def resume_state(state: dict, path: str, step: Optional[int] = None) -> dict:
+    """The scene state after step `step` (default: the last one) of a checkpoint: the
+    material, mesh and barriers of `state`, positions and velocities from the file."""
+    z = np.load(path)
+    k = int(z["step"]) if step is None else int(step)
+    out = dict(state)
+    out["pos"] = z["pos"][k - 1].copy()
+    out["vel"] = z["vel"][k - 1].copy()
+    return out
+
+
 def trajectory(state: dict, steps: int, config=None, tol: float = 1e-6, device="cuda", bank: int = 16,
-               solver_hook=None):
+               solver_hook=None, checkpoint: Optional[str] = None):
     """Run `steps` implicit-Euler steps from a scene state (stgipc.scenes ..., state_only=True);
-    returns (positions after each step as host arrays, step statistics)."""
+    returns (positions after each step as host arrays, step statistics).  With
+    `checkpoint`, positions and velocities of every step are written there after each step
+    (resume with resume_state)."""
     from . import scenes
     from .linear_system import PCGSolverConfig, Solver
     scene = FemScene(state, device=device)
@@ -95,9 +116,12 @@ def trajectory(state: dict, steps: int, config=None, tol: float = 1e-6, device="
     solver.mas_init(V, start, num, nlist, pm, rm)
     if solver_hook:
         solver_hook(solver)
-    out, stats = [], []
-    for _ in range(steps):
+    out, vels, stats = [], [], []
+    for k in range(steps):
         stats.append(step(scene, solver, tol))
         out.append(scene.pos.cpu().numpy().copy())
+        vels.append(scene.vel.cpu().numpy().copy())
+        if checkpoint:
+            save_checkpoint(checkpoint, out, vels, k + 1)
     solver.close()
     return out, stats

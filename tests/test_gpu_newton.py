@@ -69,3 +69,18 @@ def test_trajectory_fp32_matches_fp64_without_interpenetration(dev):
     # the cube reached the ground: the barrier was active (within dhat) at some step
     assert min(s.min_plane_distance for s in s64) < 1e-3
     assert all(s.newton_iterations < 30 for s in s64 + s32)
+
+
+def test_trajectory_checkpoint_resume(dev, tmp_path):
+    """A trajectory resumed from the checkpoint after step 2 reproduces the uninterrupted
+    run's later steps bit for bit (the solve and the producer are deterministic)."""
+    from stgipc import PCGSolverConfig, newton, scenes
+    st = scenes.make_cube_drop(n=5, seed=2502, state_only=True)
+    cfg = PCGSolverConfig(precision="fp32", stop_rule="relative_residual", global_tol_rate=1e-4)
+    ck = str(tmp_path / "traj.npz")
+    full, _ = newton.trajectory(st, 4, cfg, device=dev, checkpoint=ck)
+    z = np.load(ck)
+    assert int(z["step"]) == 4 and z["pos"].shape == (4, st["pos"].shape[0], 3)
+    rest, _ = newton.trajectory(newton.resume_state(st, ck, step=2), 2, cfg, device=dev)
+    np.testing.assert_array_equal(rest[0], full[2])
+    np.testing.assert_array_equal(rest[1], full[3])
