@@ -83,3 +83,32 @@ def test_concatenated_batch_meets_every_scene_tolerance(dev, per_scene, prec, lo
         assert np.all(rels <= 1e-4) and np.all(its > 0)
         assert st["iterations"] == its.max()
     cb.close()
+
+
+def test_per_scene_recurrences_match_each_scene_alone(dev):
+    """With FP64 block-Jacobi (no coarse levels, so each scene's preconditioner is exactly its
+    own) every scene's recurrence inside the concatenated solve is the scene's own PCG: the
+    same iteration count as the oracle solving the scene alone (+-1 for summation order) and
+    the same solution."""
+    from oracle import oracle as orc
+    from stgipc import PCGSolverConfig, scenes
+    from stgipc.batch import ConcatenatedBatch
+    sysl = scenes.make_batched_cubes(count=8, seed=1007, n_lo=3, n_hi=8)
+    cfg = PCGSolverConfig(precision="fp64", preconditioner="diag", stop_rule="relative_residual",
+                          global_tol_rate=1e-6)
+    cb = ConcatenatedBatch(sysl, cfg, device=dev, per_scene=True)
+    st = cb.solve()
+    its, rels = cb.scene_stats()
+    assert st["iterations"] == its.max()
+    for k, s in enumerate(sysl):
+        r, c, bl = orc.convert(s.rows, s.cols, s.blocks)
+        # uncapped: the batch's iteration cap is 0.3 n of the whole batch, not of the scene
+        xe, se, _, done = orc.pcg_timed(r, c, bl, s.b, use_diag=True, tol=1e-6, stop_rule="relative",
+                                        max_iter_ratio=100.0)
+        assert done and se["rel_residual"] <= 1.1e-6
+        assert abs(int(its[k]) - se["iterations"]) <= 1, (k, its[k], se["iterations"])
+        x = cb.solution(k)
+        # equal counts: the same iterates up to FP64 summation order
+        tol = 1e-7 if int(its[k]) == se["iterations"] else 1e-5
+        assert np.linalg.norm(x - xe) <= tol * np.linalg.norm(xe), (k, np.linalg.norm(x - xe) / np.linalg.norm(xe))
+    cb.close()
