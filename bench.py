@@ -280,6 +280,9 @@ def run_batch_concat(args, sysl, mine, cfg, dev, world, rank, local):
             "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(st["kernel_launches"] * args.steps), "clocks": clk.summary()}))
     cb.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 
