@@ -272,10 +272,15 @@ int stg_spmv_tiles_info(stg_handle h, int* rows_per_tile, float* us_default, flo
  * held by every GPU that loads the library until the process exits.  Systems larger than
  * STG_NOALLOC_MAX_ROWS block rows (n / 3) or STG_NOALLOC_MAX_BLOCKS upper blocks are
  * rejected with STG_ERR_INVALID.  All calls share that array: calls that overlap on the
- * GPU (two host threads, or two streams) race and give wrong results.  The first call on
- * each device resolves the array's address on that device; make it before any stream
- * capture.  `stream` is a cudaStream_t (NULL: the legacy default stream); the call returns
- * after the stream has finished the product. */
+ * GPU (two host threads, or two streams) race and give wrong results.  Every pointer must
+ * be memory of the current device (STG_ERR_INVALID otherwise).  The first call on each
+ * device resolves the array's address on that device; under lazy module loading (the
+ * CUDA 12 default) that first call may also be when the array is reserved, so a caller
+ * that hands the rest of HBM to its own pool makes a call with n == 0 first (it does only
+ * this set-up), or sets CUDA_MODULE_LOADING=EAGER.  `stream` is a cudaStream_t (NULL: the
+ * legacy default stream).  The call is synchronous: it reads the input check back to the
+ * host and returns after the stream has finished the product, so it cannot be called
+ * inside a stream capture. */
 #define STG_NOALLOC_MAX_ROWS 131072
 #define STG_NOALLOC_MAX_BLOCKS 1048576
 #define STG_NOALLOC_SCRATCH_BYTES (256 + 3 * 4 * 131136 + 8 * 1048576)

@@ -257,8 +257,14 @@ int Solver::spmv(double a, const double* x, double b, double* y)
 // host threads, or two streams) race on the array and give wrong results.
 //
 // Set-up: the first call on each device resolves the array's device address with
-// cudaGetSymbolAddress (with that device current) and caches it; make that first call
-// before any stream capture.
+// cudaGetSymbolAddress (with that device current) and caches it.  Under lazy module
+// loading (the CUDA 12 default) the array is only reserved when this file's module loads,
+// which can be that first call; a call with n == 0 does the set-up and nothing else, so a
+// caller that must have every reservation made before its own pool takes the GPU's memory
+// makes such a call first (or runs with CUDA_MODULE_LOADING=EAGER).
+//
+// Every call validates its input on the device and reads the verdict back, then waits for
+// the product: it is synchronous, and cannot be made inside a stream capture.
 // ---------------------------------------------------------------------------------------
 namespace
 {
@@ -317,9 +323,27 @@ int spmv_noalloc(double a, const double* blocks, const int* rows, const int* col
                   std::to_string(STG_NOALLOC_MAX_BLOCKS) + "; use stg_spmv");
         return STG_ERR_INVALID;
     }
-    if(nrows == 0) return STG_OK;
     unsigned char* base = nullptr;
     STG_TRY(noalloc_scratch(&base));
+    if(nrows == 0) return STG_OK;
+    // every array must live on the current device (or be reachable from it as managed
+    // memory): a kernel given another GPU's pointers would fault or read the wrong memory
+    int dev = -1;
+    STG_CUDA_TRY(cudaGetDevice(&dev));
+    const void* ptrs[5] = {x, y, nnzb > 0 ? blocks : nullptr, nnzb > 0 ? (const void*)rows : nullptr,
+                           nnzb > 0 ? (const void*)cols : nullptr};
+    for(const void* p : ptrs)
+    {
+        if(!p) continue;
+        cudaPointerAttributes at{};
+        STG_CUDA_TRY(cudaPointerGetAttributes(&at, p));
+        if(!(at.type == cudaMemoryTypeManaged || (at.type == cudaMemoryTypeDevice && at.device == dev)))
+        {
+            set_error("stg_spmv_noalloc: an input or output is not device memory of the current device " +
+                      std::to_string(dev));
+            return STG_ERR_INVALID;
+        }
+    }
     int* counters = reinterpret_cast<int*>(base + kNaCounters);
     int* row_ptr = reinterpret_cast<int*>(base + kNaRowPtr);
     int* t_ptr = reinterpret_cast<int*>(base + kNaTPtr);

@@ -76,11 +76,24 @@ def spmv_noalloc(a, blocks, rows, cols, nnzb, x, b, y, stream=None):
     For callers that cannot allocate device memory; sizes up to STG_NOALLOC_MAX_ROWS block
     rows and STG_NOALLOC_MAX_BLOCKS blocks.  Calls share one fixed device scratch array, so
     calls that overlap on the GPU race.  `stream` is a torch.cuda.Stream or None (legacy
-    default stream)."""
+    default stream).  The call is synchronous and cannot be captured in a CUDA graph."""
+    import torch
     _require_cuda(blocks, rows, cols, x, y)
+    if len({t.device for t in (blocks, rows, cols, x, y)}) != 1:
+        raise ValueError("spmv_noalloc: all tensors must be on one device")
+    if blocks.dtype != torch.float64 or x.dtype != torch.float64 or y.dtype != torch.float64:
+        raise ValueError("spmv_noalloc: blocks, x and y must be float64")
+    if rows.dtype != torch.int32 or cols.dtype != torch.int32:
+        raise ValueError("spmv_noalloc: rows and cols must be int32")
+    nnzb = int(nnzb)
+    if x.numel() != y.numel() or blocks.numel() < 9 * nnzb or rows.numel() < nnzb or cols.numel() < nnzb:
+        raise ValueError("spmv_noalloc: x and y must have the same size, blocks 9 nnzb and rows/cols nnzb entries")
+    if stream is not None and stream.device != y.device:
+        raise ValueError("spmv_noalloc: stream is on another device")
     s = None if stream is None else stream.cuda_stream
-    check(_L.lib().stg_spmv_noalloc(float(a), _ptr(blocks), _ptr(rows), _ptr(cols), int(nnzb), _ptr(x), float(b),
-                                    _ptr(y), int(y.numel()), s), "stg_spmv_noalloc")
+    with torch.cuda.device(y.device):
+        check(_L.lib().stg_spmv_noalloc(float(a), _ptr(blocks), _ptr(rows), _ptr(cols), nnzb, _ptr(x), float(b),
+                                        _ptr(y), int(y.numel()), s), "stg_spmv_noalloc")
 
 
 class Solver:

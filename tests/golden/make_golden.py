@@ -1,8 +1,10 @@
 """Regenerate the golden fixtures from the reference's shipped assets.
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>
 
-Reads Assets/sorted_mesh/{cube,bunny2}_sorted.16.{msh,part} and cloth_high_sorted.16.{obj,part}
+The reference checkout is the first argument, or the STG_REFERENCE_ROOT environment
+variable.  Reads Assets/sorted_mesh/{cube,bunny2,high_mat}_sorted.16.{msh,part} and
+cloth_high_sorted.16.{obj,part}
 (the METIS-partitioned, partition-sorted meshes the reference ships; produced by
 MeshProcess/metis_partition/src/metis_sort.cpp) and stores their element connectivity,
 vertex positions and per-vertex partition ids as compressed .npz files next to this script.
@@ -57,7 +59,7 @@ def read_part(path):
 
 def main(ref_root):
     sm = os.path.join(ref_root, "Assets", "sorted_mesh")
-    for name in ("cube", "bunny2"):
+    for name in ("cube", "bunny2", "high_mat"):
         pos, tets = read_msh(os.path.join(sm, f"{name}_sorted.16.msh"))
         part = read_part(os.path.join(sm, f"{name}_sorted.16.part"))
         assert part.size == pos.shape[0], (name, part.size, pos.shape)
@@ -71,4 +73,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("STG_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py <reference checkout>  (or set STG_REFERENCE_ROOT)")
+    main(root)

@@ -30,7 +30,8 @@ def _case(n, seed, dev):
 
 def test_noalloc_matches_spmv_two_calls(dev):
     """Two calls in a row (a larger system, then a smaller one, so stale scratch from the
-    first would show in the second) agree with stg_spmv within the SpMV tests' tolerance."""
+    first would show in the second) give stg_spmv's products bit for bit: both run the same
+    kernel over transpose lists sorted the same way."""
     from stgipc import PCGSolverConfig, Solver
     from stgipc.linear_system import spmv_noalloc
     solver = Solver(PCGSolverConfig())
@@ -41,7 +42,7 @@ def test_noalloc_matches_spmv_two_calls(dev):
         y_na = _t(y0, dev)
         spmv_noalloc(a, blocks, rows, cols, nnzb, x, b, y_na)
         ye, yg = y_ref.cpu().numpy(), y_na.cpu().numpy()
-        assert np.max(np.abs(yg - ye)) <= 1e-13 * np.max(np.abs(ye)), n
+        assert np.array_equal(yg, ye), (n, np.max(np.abs(yg - ye)))
 
 
 def test_noalloc_rejects_oversize_and_bad_input(dev):
@@ -60,3 +61,16 @@ def test_noalloc_rejects_oversize_and_bad_input(dev):
                             0.0, y.data_ptr(), y.numel(), None)
     assert st == _lib.STG_ERR_INVALID and b"unsorted" in L.stg_last_error()
     assert np.array_equal(y.cpu().numpy(), y0)
+    # a zero-size call only resolves the scratch array on the current device
+    assert L.stg_spmv_noalloc(1.0, None, None, None, 0, None, 0.0, None, 0, None) == _lib.STG_OK
+    # host memory is not device memory of the current device
+    xh = np.zeros(y.numel())
+    st = L.stg_spmv_noalloc(1.0, blocks.data_ptr(), rows.data_ptr(), cols.data_ptr(), nnzb, xh.ctypes.data,
+                            0.0, y.data_ptr(), y.numel(), None)
+    assert st == _lib.STG_ERR_INVALID and b"current device" in L.stg_last_error()
+    # the Python wrapper checks dtypes and sizes before calling
+    from stgipc.linear_system import spmv_noalloc
+    with pytest.raises(ValueError):
+        spmv_noalloc(1.0, blocks.float(), rows, cols, nnzb, x, 0.0, y)
+    with pytest.raises(ValueError):
+        spmv_noalloc(1.0, blocks, rows, cols, nnzb, x[:-3], 0.0, y)
