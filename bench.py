@@ -556,9 +556,20 @@ def main():
                                   "iterations": st_bj["iterations"], "converged": st_bj["status"] == 0,
                                   "sample": sample_bj}
 
+    # the metric's own comparison: learned + FP32 against plain FP64 MAS-PCG, target <= 0.5 x
+    learned_ms = learned_line["fp32"]["ms"] if learned_line and "fp32" in learned_line else None
+    target = {"rule": "learned+FP32 solve <= 0.5 x plain FP64 MAS-PCG solve (target_ratio >= 2)",
+              "plain_fp64_ms": ms_plain, "learned_fp32_ms": learned_ms,
+              "target_ratio": (ms_plain / learned_ms) if learned_ms else None,
+              "target_met": bool(learned_ms and ms_plain / learned_ms >= 2.0),
+              "plain_fp32_ratio": ms_plain / ms_fast}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": ms_fast, "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "value_is": "the FP32-storage MAS-PCG solve without the learned correction (the faster FP32 solve); "
+                        "the learned+FP32 solve is target.learned_fp32_ms",
+            "target_ratio": target["target_ratio"], "target_met": target["target_met"], "target": target,
             "warmup": args.warmup, "ms_per_step": ms_fast, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (FP64 dots, FP64 residual replacement)", "data": "synthetic",
             "config": {"workload": args.workload, "desc": desc, "dof": sysm.n, "nnzb": st_fast["nnzb"],

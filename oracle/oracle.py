@@ -47,6 +47,8 @@ def lib():
         L.orc_mas_create.argtypes = [C.c_int, C.c_int, _u32p, _u32p, _u32p, C.c_int, _i32p, C.c_int, _i32p, C.c_int]
         L.orc_mas_create.restype = C.c_void_p
         L.orc_mas_destroy.argtypes = [C.c_void_p]
+        L.orc_mas_set_order.argtypes = [C.c_void_p, C.c_int]
+        L.orc_mas_set_order.restype = None
         L.orc_mas_levels.argtypes = [C.c_void_p]
         L.orc_mas_levels.restype = C.c_int
         L.orc_mas_total_clusters.argtypes = [C.c_void_p]
@@ -108,10 +110,18 @@ def spmv(rows, cols, blocks, x, a=1.0, b=0.0, y=None):
     return y
 
 
-class Mas:
-    """Oracle MAS preconditioner (one instance per mesh)."""
+ORDER_WALK, ORDER_FIXED = 0, 1
 
-    def __init__(self, bank, num_verts, nstart, nnum, nlist, part_map, real_map, node_offset=0):
+
+class Mas:
+    """Oracle MAS preconditioner (one instance per mesh).
+
+    order: ORDER_FIXED (default) sums the coarse bank matrices, the multilevel residual and
+    the bank-solve rows in one fixed order, the one the GPU kernels use; ORDER_WALK follows
+    the reference's loops literally (its atomics taken in loop order).  The reference itself
+    leaves these orders undefined (atomics); see stg_oracle.c."""
+
+    def __init__(self, bank, num_verts, nstart, nnum, nlist, part_map, real_map, node_offset=0, order=ORDER_FIXED):
         self.bank = bank
         self.V = num_verts
         self.M = part_map.size
@@ -119,6 +129,7 @@ class Mas:
         self._keep += [np.ascontiguousarray(part_map, np.int32), np.ascontiguousarray(real_map, np.int32)]
         s, n_, l_, pm, rm = self._keep
         self.h = lib().orc_mas_create(bank, num_verts, s, n_, l_, l_.size, pm, pm.size, rm, node_offset)
+        lib().orc_mas_set_order(self.h, order)
         self.L = lib().orc_mas_levels(self.h)
 
     def __del__(self):

@@ -40,6 +40,32 @@
 
 #define ORC_MAX_LEVELS 6
 
+/* Summation orders of the MAS.  The reference forms the coarse bank matrices with FP64
+ * atomicAdd (PrepareHessian_bcoo, MASPreconditioner.cu:1849-2075) and the multilevel residual
+ * with float atomicAdd (__buildMultiLevelR_optimized_new, :729-847), so its sums have no
+ * defined order, and the dot products inside the bank solves (_schwarzLocalXSym6, :957-1027)
+ * are a warp reduction whose contraction into FMAs the compiler chooses.
+ *   ORC_ORDER_WALK  follows the reference's loops literally: every fine entry and every
+ *                   fine residual is walked up the levels (lambda 1 / lambda 2, the atomics
+ *                   taken in loop order), pivots divide (`/= rt`), bank rows are summed
+ *                   column by column.
+ *   ORC_ORDER_FIXED (default) fixes one order, the one the sm_100a kernels use, so that the
+ *                   two can be compared bit for bit:
+ *     - level l+1 bank matrices from the level-l Galerkin operator A_l, one level at a time:
+ *       each upper entry of A_l (in sorted order) is mapped to its coarse pair and oriented
+ *       upper, and duplicates are summed in that order (orc_convert);
+ *     - Gauss-Jordan rows are scaled by the correctly rounded reciprocal of the pivot;
+ *     - the residual of a level-(l+1) node is the FP32 sum, from 0 and in lane order, of the
+ *       members of its level-l component;
+ *     - 16-vertex bank rows: two partial sums of eight 3x3 blocks each, half h over the
+ *       column blocks 8h + ((j + a) mod 8), j = 0..7, each block added with three FMAs
+ *       (columns 0, 1, 2); then half 0 + half 1;
+ *     - 32-vertex bank rows: the 32 block products (fma(P2, x2, fma(P1, x1, P0 x0))) are
+ *       summed by an xor butterfly over 32 lanes (offsets 16, 8, 4, 2, 1);
+ *     - prolongation: level 0 + level 1 + ... in FP32, as the reference. */
+#define ORC_ORDER_WALK 0
+#define ORC_ORDER_FIXED 1
+
 /* ------------------------------------------------------------------------------------ */
 /* 3x3 helpers; blocks are column-major (Eigen Matrix3d): element (i,j) at [j*3+i]       */
 /* ------------------------------------------------------------------------------------ */
@@ -152,8 +178,10 @@ typedef struct
     int* coarse_tables;        /* [L*V]              */
     int* going_next;           /* [L*V + M]          */
     int* coarse_table;         /* [V*(L-1)] (itable) */
+    unsigned* closed;          /* [total_clusters] closure masks of the coarse nodes (levels >= 1) */
     int level_size[2 * (ORC_MAX_LEVELS + 1)];
     int total_clusters;
+    int order;                 /* ORC_ORDER_FIXED (default) or ORC_ORDER_WALK */
     /* matrices */
     int nbanks;                /* total_clusters / bank */
     double* mat;               /* [nbanks * nsym * 9] FP64 packed upper (column-major 3x3) */
@@ -187,6 +215,7 @@ void orc_mas_destroy(orc_mas* m)
     free(m->part_map); free(m->real_map); free(m->fine_mask); free(m->next_mask);
     free(m->prefix_orig); free(m->prefix_sum_orig); free(m->next_prefix); free(m->next_prefix_sum);
     free(m->coarse_tables); free(m->going_next); free(m->coarse_table); free(m->mat); free(m->inv);
+    free(m->closed);
     free(m);
 }
 
@@ -221,8 +250,11 @@ orc_mas* orc_mas_create(int bank, int V, const unsigned* nstart, const unsigned*
     m->coarse_tables = (int*)calloc((size_t)m->L * V, sizeof(int));
     m->going_next = (int*)calloc((size_t)m->L * V + M, sizeof(int));
     m->coarse_table = (int*)calloc((size_t)V * (m->L > 1 ? m->L - 1 : 1), sizeof(int));
+    m->order = ORC_ORDER_FIXED;
     return m;
 }
+
+void orc_mas_set_order(orc_mas* m, int order) { m->order = order; }
 
 int orc_mas_levels(const orc_mas* m) { return m->L; }
 int orc_mas_total_clusters(const orc_mas* m) { return m->total_clusters; }
@@ -399,6 +431,8 @@ int orc_mas_build(orc_mas* m, const int* pairs, int ncp)
         }
     }
 
+    free(m->closed);
+    m->closed = (unsigned*)calloc((size_t)(m->L + 1) * (M > V ? M : V) + 64, sizeof(unsigned));
     for(int level = 1; level < L; level++)
     {
         memset(m->next_mask, 0, sizeof(unsigned) * V);
@@ -437,6 +471,7 @@ int orc_mas_build(orc_mas* m, const int* pairs, int ncp)
             {
                 unsigned c = closure(orig, l, orig[l]);
                 m->next_mask[b * B + l] = c;
+                m->closed[level_begin + b * B + l] = c;
                 if(__builtin_popcount(c & lanemask_lt(l)) == 0) comps++;
             }
             m->next_prefix[b] = (unsigned)comps;
@@ -515,7 +550,10 @@ int orc_select_range(int nnzb, const int* rows, const int* cols, int offset, int
 
 static inline double* mblk(orc_mas* m, int gid_bank, int idx) { return m->mat + ((size_t)gid_bank * nsym(m->bank) + idx) * 9; }
 
-/* In-place Gauss-Jordan inverse of one bank (__inverse6_P96x96, MASPreconditioner.cu:630-726). */
+/* In-place Gauss-Jordan inverse of one bank (__inverse6_P96x96, MASPreconditioner.cu:630-726).
+ * The pivot row is divided by the pivot (ORC_ORDER_WALK, `/= rt` as in the reference) or
+ * multiplied by its correctly rounded reciprocal (ORC_ORDER_FIXED); the elimination is
+ * fma(-colm[k], A[j][i], A[k][i]), the contraction of the reference's `+= rate * ...`. */
 static void invert_bank(orc_mas* m, int bk, double* A, double* colm)
 {
     const int B = m->bank, N = 3 * B;
@@ -536,7 +574,13 @@ static void invert_bank(orc_mas* m, int bk, double* A, double* colm)
         double rt = A[(size_t)j * N + j];
         for(int i = 0; i < N; i++) colm[i] = A[(size_t)i * N + j];
         for(int i = 0; i < N; i++) A[(size_t)i * N + j] = (i == j) ? 1.0 : 0.0;
-        for(int i = 0; i < N; i++) A[(size_t)j * N + i] /= rt;
+        if(m->order == ORC_ORDER_FIXED)
+        {
+            const double rinv = 1.0 / rt;
+            for(int i = 0; i < N; i++) A[(size_t)j * N + i] *= rinv;
+        }
+        else
+            for(int i = 0; i < N; i++) A[(size_t)j * N + i] /= rt;
         for(int k = 0; k < N; k++)
         {
             if(k == j) continue;
@@ -561,6 +605,80 @@ static void invert_bank(orc_mas* m, int bk, double* A, double* colm)
         }
 }
 
+/* An upper entry (u <= v) with value H mapped to the coarse pair (a, b) and oriented upper:
+ * a < b: H; a > b: H^T at (b, a); a == b: H (u == v) or H + H^T (u < v).  The level-(l+1)
+ * Galerkin entry P^T A P sums these over the level-l entries. */
+static void coarse_triplet(int u, int v, int a, int b, const double* H, int* orow, int* ocol, double* oblk)
+{
+    if(a < b || (a == b && u == v))
+        memcpy(oblk, H, 9 * sizeof(double));
+    else if(a > b)
+    {
+        for(int i = 0; i < 3; i++)
+            for(int j = 0; j < 3; j++) oblk[j * 3 + i] = H[i * 3 + j];
+        int t = a; a = b; b = t;
+    }
+    else
+        for(int i = 0; i < 3; i++)
+            for(int j = 0; j < 3; j++) oblk[j * 3 + i] = H[j * 3 + i] + H[i * 3 + j];
+    *orow = a;
+    *ocol = b;
+}
+
+/* ORC_ORDER_FIXED assembly: the bank-diagonal blocks of every level's Galerkin operator, one
+ * level at a time (A_1 from the fine entries, A_(l+1) from A_l).  The level-0 in-bank entries
+ * with slot(col) < slot(row) are left out of A_0 as lambda 1 leaves them out of the bank
+ * matrix (MASPreconditioner.cu:1849-1944), which lambda 2 then propagates (:1946-2075). */
+static void assemble_levels(orc_mas* m, const int* rows, const int* cols, const double* blocks,
+                            const int* sel, int nsel, int offset)
+{
+    const int B = m->bank, L = m->L;
+    int* trow = (int*)malloc(sizeof(int) * (size_t)(nsel > 0 ? nsel : 1));
+    int* tcol = (int*)malloc(sizeof(int) * (size_t)(nsel > 0 ? nsel : 1));
+    double* tblk = (double*)malloc(sizeof(double) * 9 * (size_t)(nsel > 0 ? nsel : 1));
+    int* arow = (int*)malloc(sizeof(int) * (size_t)(nsel > 0 ? nsel : 1));
+    int* acol = (int*)malloc(sizeof(int) * (size_t)(nsel > 0 ? nsel : 1));
+    double* ablk = (double*)malloc(sizeof(double) * 9 * (size_t)(nsel > 0 ? nsel : 1));
+    int nt = 0;
+    for(int I = 0; I < nsel; I++)
+    {
+        const int k = sel[I];
+        const double* H = blocks + 9 * (size_t)k;
+        const int rr = rows[k] - offset, cc = cols[k] - offset;
+        const int sc = m->real_map[cc], sr = m->real_map[rr];
+        if(sc / B == sr / B)
+        {
+            if(sc < sr) continue;
+            memcpy(mblk(m, sc / B, upper_index(B, sr % B, sc % B)), H, 9 * sizeof(double));
+        }
+        if(L > 1)
+        {
+            coarse_triplet(rr, cc, m->coarse_tables[rr], m->coarse_tables[cc], H, trow + nt, tcol + nt,
+                           tblk + 9 * (size_t)nt);
+            nt++;
+        }
+    }
+    for(int level = 1; level < L && nt > 0; level++)
+    {
+        const int begin = m->level_size[2 * level + 1];
+        const int na = orc_convert(nt, trow, tcol, tblk, arow, acol, ablk);
+        for(int e = 0; e < na; e++)
+        {
+            const int ga = begin + arow[e], gb = begin + acol[e];
+            if(ga / B != gb / B) continue;
+            memcpy(mblk(m, ga / B, upper_index(B, ga % B, gb % B)), ablk + 9 * (size_t)e, 9 * sizeof(double));
+        }
+        if(level + 1 >= L) break;
+        const int begin_next = m->level_size[2 * (level + 1) + 1];
+        for(int e = 0; e < na; e++)
+            coarse_triplet(arow[e], acol[e], m->going_next[begin + arow[e]] - begin_next,
+                           m->going_next[begin + acol[e]] - begin_next, ablk + 9 * (size_t)e, trow + e, tcol + e,
+                           tblk + 9 * (size_t)e);
+        nt = na;
+    }
+    free(trow); free(tcol); free(tblk); free(arow); free(acol); free(ablk);
+}
+
 /* setPreconditioner_bcoo after ReorderRealtime: PrepareHessian_bcoo + inverse
  * (MASPreconditioner.cu:1829-2075, 2207-2245).  `sel` lists the BCOO entries of the FEM
  * range (orc_select_range); `offset` is the FEM block offset. */
@@ -572,6 +690,11 @@ void orc_mas_assemble(orc_mas* m, const int* rows, const int* cols, const double
     free(m->mat); free(m->inv);
     m->mat = (double*)calloc((size_t)m->nbanks * NS * 9, sizeof(double));
     m->inv = (float*)calloc((size_t)m->nbanks * NS * 9, sizeof(float));
+    if(m->order == ORC_ORDER_FIXED)
+    {
+        assemble_levels(m, rows, cols, blocks, sel, nsel, offset);
+        goto invert;
+    }
 
     /* lambda 1 (MASPreconditioner.cu:1849-1944) */
     for(int I = 0; I < nsel; I++)
@@ -662,6 +785,7 @@ void orc_mas_assemble(orc_mas* m, const int* rows, const int* cols, const double
     }
 
     /* __inverse6_P96x96 over every bank of every level */
+invert:
     {
         const int N = 3 * B;
         double* A = (double*)malloc(sizeof(double) * N * N);
@@ -680,10 +804,130 @@ void orc_mas_export_matrices(const orc_mas* m, double* mat, float* inv)
     if(inv) memcpy(inv, m->inv, cnt * sizeof(float));
 }
 
+/* ORC_ORDER_FIXED: sum, from 0 and in lane order, of the lanes of `msk` in the bank whose
+ * values start at R + 3 * base */
+static void lane_sum(const float* R, int base, unsigned msk, int B, float out[3])
+{
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    for(int b = 0; b < B; b++)
+        if(msk & (1u << b))
+        {
+            a0 += R[3 * (size_t)(base + b)];
+            a1 += R[3 * (size_t)(base + b) + 1];
+            a2 += R[3 * (size_t)(base + b) + 2];
+        }
+    out[0] = a0; out[1] = a1; out[2] = a2;
+}
+
+/* element (i, k) of block (a, c) of a packed upper bank inverse (column-major 3x3 blocks;
+ * a lower block is the transpose of its mirror) */
+static inline float pblk(const float* P, int B, int a, int c, int i, int k)
+{
+    return c >= a ? P[(size_t)upper_index(B, a, c) * 9 + k * 3 + i] : P[(size_t)upper_index(B, c, a) * 9 + i * 3 + k];
+}
+
+/* ORC_ORDER_FIXED bank solve z_a = sum_c P_ac r_c of one bank (see the order notes above) */
+static void bank_solve_fixed(const float* P, const float* R, int B, float* Z)
+{
+    for(int a = 0; a < B; a++)
+    {
+        float z[3];
+        if(B == 16)
+        {
+            float zh[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+            for(int h = 0; h < 2; h++)
+                for(int j = 0; j < 8; j++)
+                {
+                    const int c = 8 * h + ((j + a) & 7);
+                    const float* x = R + 3 * c;
+                    for(int i = 0; i < 3; i++)
+                    {
+                        float acc = zh[h][i];
+                        acc = fmaf(pblk(P, B, a, c, i, 0), x[0], acc);
+                        acc = fmaf(pblk(P, B, a, c, i, 1), x[1], acc);
+                        acc = fmaf(pblk(P, B, a, c, i, 2), x[2], acc);
+                        zh[h][i] = acc;
+                    }
+                }
+            for(int i = 0; i < 3; i++) z[i] = zh[0][i] + zh[1][i];
+        }
+        else
+        {
+            float v[32][3];
+            for(int c = 0; c < 32; c++)
+            {
+                const float* x = R + 3 * c;
+                for(int i = 0; i < 3; i++)
+                    v[c][i] = fmaf(pblk(P, B, a, c, i, 2), x[2], fmaf(pblk(P, B, a, c, i, 1), x[1], pblk(P, B, a, c, i, 0) * x[0]));
+            }
+            for(int o = 16; o > 0; o >>= 1)
+            {
+                float w[32][3];
+                for(int l = 0; l < 32; l++)
+                    for(int i = 0; i < 3; i++) w[l][i] = v[l][i] + v[l ^ o][i];
+                memcpy(v, w, sizeof(v));
+            }
+            for(int i = 0; i < 3; i++) z[i] = v[0][i];
+        }
+        for(int i = 0; i < 3; i++) Z[3 * a + i] = z[i];
+    }
+}
+
+static void mas_apply_fixed(const orc_mas* m, const double* r, double* z)
+{
+    const int B = m->bank, V = m->V, M = m->M, L = m->L, T = m->total_clusters, NS = nsym(B);
+    float* R = (float*)calloc((size_t)T * 3 + 3 * 32, sizeof(float));
+    float* Zc = (float*)calloc((size_t)T * 3 + 3 * 32, sizeof(float));
+    for(int s = 0; s < M; s++)
+    {
+        int v = m->part_map[s];
+        if(v < 0) continue;
+        for(int c = 0; c < 3; c++) R[3 * (size_t)s + c] = (float)r[3 * v + c];
+    }
+    if(L > 1)
+        for(int s = 0; s < M; s++)
+        {
+            const int v = m->part_map[s];
+            if(v < 0) continue;
+            const unsigned msk = m->fine_mask[v];
+            if(__builtin_popcount(msk & lanemask_lt(s % B)) != 0) continue;
+            lane_sum(R, s / B * B, msk, B, R + 3 * (size_t)m->going_next[v]);
+        }
+    for(int level = 1; level < L - 1; level++)
+    {
+        const int number = m->level_size[2 * level], begin = m->level_size[2 * level + 1];
+        for(int i = 0; i < number; i++)
+        {
+            const unsigned msk = m->closed[begin + i];
+            if(__builtin_popcount(msk & lanemask_lt(i % B)) != 0) continue;
+            lane_sum(R, begin + i / B * B, msk, B, R + 3 * (size_t)m->going_next[begin + i]);
+        }
+    }
+    for(int bk = 0; bk < T / B; bk++)
+        bank_solve_fixed(m->inv + (size_t)bk * NS * 9, R + 3 * (size_t)bk * B, B, Zc + 3 * (size_t)bk * B);
+    for(int v = 0; v < V; v++)
+    {
+        const int s = m->real_map[v];
+        float cz[3] = {Zc[3 * (size_t)s], Zc[3 * (size_t)s + 1], Zc[3 * (size_t)s + 2]};
+        for(int l = 1; l < L; l++)
+        {
+            const int now = m->coarse_table[(size_t)v * (L - 1) + l - 1];
+            for(int c = 0; c < 3; c++) cz[c] += Zc[3 * (size_t)now + c];
+        }
+        for(int c = 0; c < 3; c++) z[3 * v + c] = (double)cz[c];
+    }
+    free(R); free(Zc);
+}
+
 /* preconditioning (MASPreconditioner.cu:2248-2289): restrict (729-847), local solves
  * (957-1027), prolong (850-879).  r, z: FEM sub-range, 3V doubles. */
 void orc_mas_apply(const orc_mas* m, const double* r, double* z)
 {
+    if(m->order == ORC_ORDER_FIXED)
+    {
+        mas_apply_fixed(m, r, z);
+        return;
+    }
     const int B = m->bank, V = m->V, M = m->M, L = m->L, T = m->total_clusters;
     float* R = (float*)calloc((size_t)T * 3, sizeof(float));
     float* Zc = (float*)calloc((size_t)T * 3, sizeof(float));

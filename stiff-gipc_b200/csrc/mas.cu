@@ -19,6 +19,7 @@
 // atomics, and the coarse-level Galerkin blocks are formed level by level with the
 // deterministic sort/merge of convert.cu instead of FP64 atomics (see the assembly section).
 #include "solver.hpp"
+#include "bank_dev.cuh"
 
 namespace stg
 {
@@ -425,7 +426,9 @@ __global__ void k_mas_extract(const int* __restrict__ rows, const int* __restric
 // __inverse6_P96x96 (MASPreconditioner.cu:630-726): in-place Gauss-Jordan without pivoting
 // of each bank's dense 3B x 3B matrix in FP64 (zero diagonal -> 1 for padding), lower
 // triangle of the diagonal 3x3 blocks mirrored from the upper one, upper blocks stored FP32.
-// One CTA per bank, thread i owns column i.
+// One CTA per bank, thread i owns column i.  The pivot row is scaled by the correctly rounded
+// reciprocal of the pivot (the reference divides; k_mas_invert16 does the same as here, so
+// both bank sizes follow one order, the CPU oracle's ORC_ORDER_FIXED).
 template <int B>
 __global__ void __launch_bounds__(3 * B) k_mas_invert(const double* __restrict__ mat, float* inv, int nbanks)
 {
@@ -456,7 +459,7 @@ __global__ void __launch_bounds__(3 * B) k_mas_invert(const double* __restrict__
         __syncthreads();
         A[i * N + j] = (i == j) ? 1.0 : 0.0;
         __syncthreads();
-        A[j * N + i] /= rt;
+        A[j * N + i] = __dmul_rn(A[j * N + i], 1.0 / rt);
         __syncthreads();
         const double aji = A[j * N + i];
         for(int k = 0; k < N; k++)
@@ -486,8 +489,8 @@ __global__ void __launch_bounds__(3 * B) k_mas_invert(const double* __restrict__
 // made a per-element division three times slower) and publish it; then every tile updates
 // itself with fma(-colm[k], A[j][i], A[k][i]) as k_mas_invert does.  The broadcasts are
 // double-buffered (two barriers per pivot).  Scaling by the reciprocal instead of dividing
-// changes the last bit of some FP64 entries; the FP32 inverses agree with the per-element
-// division to within the tests' 2e-5.
+// changes the last bit of some FP64 entries against the reference's per-element division;
+// k_mas_invert scales the same way, and the CPU oracle (ORC_ORDER_FIXED) restates it.
 __global__ void __launch_bounds__(256) k_mas_invert16(const double* __restrict__ mat, float* inv, int nbanks)
 {
     constexpr int B = 16;
@@ -539,7 +542,7 @@ __global__ void __launch_bounds__(256) k_mas_invert16(const double* __restrict__
             {
                 const int col = 3 * bj + cc;
                 const double x = col == j ? 1.0 : (pr == 0 ? a[0][cc] : (pr == 1 ? a[1][cc] : a[2][cc]));
-                const double v = x * rinv;
+                const double v = __dmul_rn(x, rinv);
                 rowj[buf][col] = v;
                 if(pr == 0)
                     a[0][cc] = v;
@@ -665,15 +668,40 @@ __global__ void k_mas_restrict_lx(float* R, const unsigned* __restrict__ closed,
 }
 
 // _schwarzLocalXSym6 (MASPreconditioner.cu:957-1027): z_b = P_b r_b for every bank of every
-// level.  The packed FP32 inverse (4.9 KB for B=16, 19 KB for B=32) is staged in shared
-// memory with 16-byte loads; thread (a, c) forms block (a,c) * r_c and the B lanes of row a
-// reduce with shuffles in a fixed order.
-template <int B>
-__global__ void __launch_bounds__(B * B) k_mas_schwarz(const float* __restrict__ inv, const float* __restrict__ R, float* Z,
-                                                       const int* done)
+// level, with the row arithmetic of bank_dev.cuh (the PCG loop's phase D gives the same bits).
+// 16-banks: one warp per bank (4 per CTA), lane (a, h) forms half h of block row a; the
+// packed inverse (4,896 B) and the 16 residual slots are staged per warp with 16-byte loads.
+constexpr int SCHWARZ16_WARPS = 4;
+
+__global__ void __launch_bounds__(SCHWARZ16_WARPS * 32) k_mas_schwarz16(const float* __restrict__ inv,
+                                                                        const float* __restrict__ R, float* Z,
+                                                                        int nbanks, const int* done)
 {
     if(done && *done) return;
-    constexpr int NS = B * (B + 1) / 2;
+    __shared__ __align__(16) float P[SCHWARZ16_WARPS][136 * 9];
+    __shared__ float4 rs[SCHWARZ16_WARPS][16];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bk = blockIdx.x * SCHWARZ16_WARPS + w;
+    if(bk >= nbanks) return;
+    const float4* src = reinterpret_cast<const float4*>(inv + (size_t)bk * 136 * 9);
+    float4* dst = reinterpret_cast<float4*>(P[w]);
+    for(int t = lane; t < 136 * 9 / 4; t += 32) dst[t] = __ldg(src + t);
+    if(lane < 16) rs[w][lane] = *reinterpret_cast<const float4*>(R + 4 * ((size_t)bk * 16 + lane));
+    __syncwarp();
+    const int a = lane & 15, h = lane >> 4;
+    float z0, z1, z2;
+    bank16_half(P[w], rs[w], a, h, z0, z1, z2);
+    bank16_join(z0, z1, z2);
+    if(h == 0) st4(Z + ((size_t)bk * 16 + a) * 4, z0, z1, z2);
+}
+
+// 32-banks: one CTA of 1,024 threads per bank, thread (a, c) forms the block product of
+// block (a, c) and the 32 lanes of row a sum them with the xor butterfly.
+__global__ void __launch_bounds__(1024) k_mas_schwarz32(const float* __restrict__ inv, const float* __restrict__ R,
+                                                        float* Z, const int* done)
+{
+    if(done && *done) return;
+    constexpr int B = 32, NS = B * (B + 1) / 2;
     __shared__ __align__(16) float P[NS * 9];
     __shared__ float r[3 * B];
     const int bk = blockIdx.x;
@@ -683,29 +711,10 @@ __global__ void __launch_bounds__(B * B) k_mas_schwarz(const float* __restrict__
     if(threadIdx.x < B) ld4(R + 4 * ((size_t)bk * B + threadIdx.x), r[3 * threadIdx.x], r[3 * threadIdx.x + 1], r[3 * threadIdx.x + 2]);
     __syncthreads();
     const int a = threadIdx.x / B, c = threadIdx.x % B;
-    const float x0 = r[3 * c], x1 = r[3 * c + 1], x2 = r[3 * c + 2];
+    const int lo = min(a, c), hi = max(a, c);
     float z0, z1, z2;
-    if(c >= a)
-    {
-        const float* Pb = P + upper_index(B, a, c) * 9;  // column-major
-        z0 = Pb[0] * x0 + Pb[3] * x1 + Pb[6] * x2;
-        z1 = Pb[1] * x0 + Pb[4] * x1 + Pb[7] * x2;
-        z2 = Pb[2] * x0 + Pb[5] * x1 + Pb[8] * x2;
-    }
-    else
-    {
-        const float* Pb = P + upper_index(B, c, a) * 9;  // transposed
-        z0 = Pb[0] * x0 + Pb[1] * x1 + Pb[2] * x2;
-        z1 = Pb[3] * x0 + Pb[4] * x1 + Pb[5] * x2;
-        z2 = Pb[6] * x0 + Pb[7] * x1 + Pb[8] * x2;
-    }
-#pragma unroll
-    for(int o = B / 2; o > 0; o >>= 1)
-    {
-        z0 += __shfl_xor_sync(0xffffffffu, z0, o);
-        z1 += __shfl_xor_sync(0xffffffffu, z1, o);
-        z2 += __shfl_xor_sync(0xffffffffu, z2, o);
-    }
+    blk_mul3(P + upper_index(B, lo, hi) * 9, c < a, r[3 * c], r[3 * c + 1], r[3 * c + 2], z0, z1, z2);
+    warp_butterfly3(z0, z1, z2);
     if(c == 0) st4(Z + ((size_t)bk * B + a) * 4, z0, z1, z2);
 }
 
@@ -1066,7 +1075,11 @@ int mas_restrict_solve_t(Solver& S, const double* r, const int* done)
         STG_LAUNCH_CHECK();
         S.launches++;
     }
-    k_mas_schwarz<B><<<m.nbanks, B * B, 0, s>>>(m.inv.data(), m.R.data(), m.Z.data(), done);
+    if(B == 16)
+        k_mas_schwarz16<<<div_up(m.nbanks, SCHWARZ16_WARPS), SCHWARZ16_WARPS * 32, 0, s>>>(m.inv.data(), m.R.data(),
+                                                                                          m.Z.data(), m.nbanks, done);
+    else
+        k_mas_schwarz32<<<m.nbanks, 1024, 0, s>>>(m.inv.data(), m.R.data(), m.Z.data(), done);
     STG_LAUNCH_CHECK();
     S.launches++;
     return 0;

@@ -34,6 +34,7 @@
 #include "solver.hpp"
 #include "reduce.cuh"
 #include "spmv_core.cuh"
+#include "bank_dev.cuh"
 
 namespace stg
 {
@@ -557,58 +558,65 @@ __device__ __forceinline__ void phase_c(const PcgDev& c, int l0, int l1, int gt,
     }
 }
 
-// D: bank solves for banks [b0, b1) with stride `bstep`, one bank per pass of the CTA.
-// PB threads = 256: for B = 16 one thread per (row lane, col lane); for B = 32 each thread
-// handles 4 (row, col) pairs.  The packed inverse is staged in shared memory with 16-byte loads.
+// D: bank solves for banks b0, b0 + bstep, ... < b1, with the arithmetic of bank_dev.cuh.
+// B = 16: the CTA's eight warps take one bank each per pass (warp w the w-th bank of the
+// pass), the packed inverse (4,896 B) and residual slots staged per warp with 16-byte loads.
+// B = 32: one bank per pass of the CTA (PB = 256 threads, 4 (row, col) pairs each).
 template <int B>
 __device__ __forceinline__ void phase_d(const PcgDev& c, int b0, int b1, int bstep)
 {
-    constexpr int NS = B * (B + 1) / 2;
-    __shared__ __align__(16) float P[NS * 9];
-    __shared__ float rr[3 * B];
-    for(int bk = b0; bk < b1; bk += bstep)
+    if constexpr(B == 16)
     {
-        const float4* src = reinterpret_cast<const float4*>(c.inv + (size_t)bk * NS * 9);
-        float4* dst = reinterpret_cast<float4*>(P);
-        for(int t = threadIdx.x; t < NS * 9 / 4; t += PB) dst[t] = __ldg(src + t);
-        if(threadIdx.x < B) ld4(c.R + 4 * ((size_t)bk * B + threadIdx.x), rr[3 * threadIdx.x], rr[3 * threadIdx.x + 1],
-                                rr[3 * threadIdx.x + 2]);
-        __syncthreads();
-        constexpr int REP = (B * B + PB - 1) / PB;
-#pragma unroll
-        for(int rep = 0; rep < REP; rep++)
+        constexpr int W = PB / 32;
+        __shared__ __align__(16) float P16[W][136 * 9];
+        __shared__ float4 r16[W][16];
+        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        for(int bk = b0 + w * bstep; bk < b1; bk += W * bstep)
         {
-            const int pair = threadIdx.x + rep * PB;
-            const int a = pair / B, cc = pair % B;
-            const float x0 = rr[3 * cc], x1 = rr[3 * cc + 1], x2 = rr[3 * cc + 2];
+            const float4* src = reinterpret_cast<const float4*>(c.inv + (size_t)bk * 136 * 9);
+            float4* dst = reinterpret_cast<float4*>(P16[w]);
+            for(int t = lane; t < 136 * 9 / 4; t += 32) dst[t] = __ldg(src + t);
+            if(lane < 16) r16[w][lane] = *reinterpret_cast<const float4*>(c.R + 4 * ((size_t)bk * 16 + lane));
+            __syncwarp();
+            const int a = lane & 15, h = lane >> 4;
             float z0, z1, z2;
-            if(cc >= a)
-            {
-                const float* Pb = P + (B * a - a * (a + 1) / 2 + cc) * 9;
-                z0 = Pb[0] * x0 + Pb[3] * x1 + Pb[6] * x2;
-                z1 = Pb[1] * x0 + Pb[4] * x1 + Pb[7] * x2;
-                z2 = Pb[2] * x0 + Pb[5] * x1 + Pb[8] * x2;
-            }
-            else
-            {
-                const float* Pb = P + (B * cc - cc * (cc + 1) / 2 + a) * 9;
-                z0 = Pb[0] * x0 + Pb[1] * x1 + Pb[2] * x2;
-                z1 = Pb[3] * x0 + Pb[4] * x1 + Pb[5] * x2;
-                z2 = Pb[6] * x0 + Pb[7] * x1 + Pb[8] * x2;
-            }
-#pragma unroll
-            for(int o = (B < 32 ? B : 32) / 2; o > 0; o >>= 1)
-            {
-                z0 += __shfl_xor_sync(0xffffffffu, z0, o);
-                z1 += __shfl_xor_sync(0xffffffffu, z1, o);
-                z2 += __shfl_xor_sync(0xffffffffu, z2, o);
-            }
-            if(cc == 0)
-            {
-                st4(c.Z + ((size_t)bk * B + a) * 4, z0, z1, z2);
-            }
+            bank16_half(P16[w], r16[w], a, h, z0, z1, z2);
+            bank16_join(z0, z1, z2);
+            if(h == 0) st4(c.Z + ((size_t)bk * 16 + a) * 4, z0, z1, z2);
+            __syncwarp();
         }
-        __syncthreads();
+    }
+    else
+    {
+        constexpr int NS = B * (B + 1) / 2;
+        __shared__ __align__(16) float P[NS * 9];
+        __shared__ float rr[3 * B];
+        for(int bk = b0; bk < b1; bk += bstep)
+        {
+            const float4* src = reinterpret_cast<const float4*>(c.inv + (size_t)bk * NS * 9);
+            float4* dst = reinterpret_cast<float4*>(P);
+            for(int t = threadIdx.x; t < NS * 9 / 4; t += PB) dst[t] = __ldg(src + t);
+            if(threadIdx.x < B) ld4(c.R + 4 * ((size_t)bk * B + threadIdx.x), rr[3 * threadIdx.x], rr[3 * threadIdx.x + 1],
+                                    rr[3 * threadIdx.x + 2]);
+            __syncthreads();
+            constexpr int REP = (B * B + PB - 1) / PB;
+#pragma unroll
+            for(int rep = 0; rep < REP; rep++)
+            {
+                const int pair = threadIdx.x + rep * PB;
+                const int a = pair / B, cc = pair % B;
+                const float x0 = rr[3 * cc], x1 = rr[3 * cc + 1], x2 = rr[3 * cc + 2];
+                const int lo = min(a, cc), hi = max(a, cc);
+                float z0, z1, z2;
+                blk_mul3(P + (B * lo - lo * (lo + 1) / 2 + hi) * 9, cc < a, x0, x1, x2, z0, z1, z2);
+                warp_butterfly3(z0, z1, z2);
+                if(cc == 0)
+                {
+                    st4(c.Z + ((size_t)bk * B + a) * 4, z0, z1, z2);
+                }
+            }
+            __syncthreads();
+        }
     }
 }
 
@@ -728,30 +736,15 @@ __global__ void __launch_bounds__(D_WARPS * 32) k_phase_d16(PcgDev c)
             ph0 ^= 1u;
         const float* P = reinterpret_cast<const float*>(cur);
         const float* rs = reinterpret_cast<const float*>(cur + D_PBYTES);
+        // bank16_half's order with the block offsets precomputed (bank_dev.cuh)
         float z0 = 0.f, z1 = 0.f, z2 = 0.f;
 #pragma unroll
         for(int j = 0; j < 8; j++)
         {
-            const float* H = P + koff[j];  // column-major 3x3
             const float4 r = *reinterpret_cast<const float4*>(rs + rcol[j]);
-            const float h0 = H[0], h1 = H[1], h2 = H[2], h3 = H[3], h4 = H[4], h5 = H[5], h6 = H[6], h7 = H[7],
-                        h8 = H[8];
-            if(tmask & (1u << j))
-            {
-                z0 += h0 * r.x + h1 * r.y + h2 * r.z;
-                z1 += h3 * r.x + h4 * r.y + h5 * r.z;
-                z2 += h6 * r.x + h7 * r.y + h8 * r.z;
-            }
-            else
-            {
-                z0 += h0 * r.x + h3 * r.y + h6 * r.z;
-                z1 += h1 * r.x + h4 * r.y + h7 * r.z;
-                z2 += h2 * r.x + h5 * r.y + h8 * r.z;
-            }
+            blk_fma3(P + koff[j], (tmask >> j) & 1u, r.x, r.y, r.z, z0, z1, z2);
         }
-        z0 += __shfl_xor_sync(0xffffffffu, z0, 16);
-        z1 += __shfl_xor_sync(0xffffffffu, z1, 16);
-        z2 += __shfl_xor_sync(0xffffffffu, z2, 16);
+        bank16_join(z0, z1, z2);
         if(h == 0) st4(c.Z + ((size_t)bk * 16 + a) * 4, z0, z1, z2);
         __syncwarp();
     }

@@ -164,6 +164,41 @@ def test_mas_inverse_is_inverse():
         assert err < 1e-3, (bk, err)
 
 
+@pytest.mark.parametrize("case", ["cube16_b16", "cube16_b32", "bunny2_contacts"])
+def test_fixed_order_matches_reference_walk(case):
+    """The oracle's fixed summation order (the GPU's) against the literal walk of the
+    reference's loops (PrepareHessian_bcoo's lambdas, per-element pivot division, fine
+    residuals added to every level): the same operator up to rounding.  Bank matrices to
+    1e-11 of each bank's largest entry, inverses to 1e-5 of it, one application to 1e-5 of
+    its largest entry, and the reference-rule PCG to the same iterations and 1e-6."""
+    from oracle import oracle as orc
+    from stgipc import scenes
+    if case == "bunny2_contacts":
+        s, part = fixture_system("bunny2")
+        bank, cp = 16, random_contacts(s.num_verts, 2000, seed=13)
+        pm, rm = scenes.slot_maps_from_parts(part, bank)
+    else:
+        s = cube_system(16)
+        bank, cp = int(case[-2:]), None
+        pm, rm = s.slot_maps(bank)
+    r, c, b = orc.convert(s.rows, s.cols, s.blocks)
+    out = {}
+    for order in (orc.ORDER_WALK, orc.ORDER_FIXED):
+        m = orc.Mas(bank, s.num_verts, s.neighbor_start, s.neighbor_num, s.neighbor_list, pm, rm, order=order)
+        m.build(cp)
+        m.assemble(r, c, b)
+        mat, inv = m.matrices()
+        z = m.apply(np.random.default_rng(5).standard_normal(s.n))
+        x, st = orc.pcg(r, c, b, s.b, mas=m)
+        out[order] = (mat, inv, z, x, st["iterations"])
+    (m0, i0, z0, x0, k0), (m1, i1, z1, x1, k1) = out[orc.ORDER_WALK], out[orc.ORDER_FIXED]
+    assert np.max(np.abs(m1 - m0) / (np.abs(m0).max(axis=(1, 2), keepdims=True) + 1e-300)) <= 1e-11
+    assert np.max(np.abs(i1 - i0) / (np.abs(i0).max(axis=(1, 2), keepdims=True) + 1e-30)) <= 1e-5
+    assert np.max(np.abs(z1 - z0)) <= 1e-5 * np.max(np.abs(z0))
+    assert k1 == k0
+    assert np.linalg.norm(x1 - x0) <= 1e-6 * np.linalg.norm(x0)
+
+
 def test_pcg_matches_scipy_solution():
     from oracle import oracle as orc
     s = cube_system(8)
