@@ -673,17 +673,23 @@ __device__ __forceinline__ void d16_issue(const PcgDev& c, char* stage, unsigned
     tma_load_1d(stage + D_PBYTES, c.R + (size_t)bk * 16 * 4, D_RBYTES, bar);
 }
 
-__global__ void __launch_bounds__(D_WARPS * 32) k_phase_d16(PcgDev c)
+// Banks [b0, b1).  guarded: only on residual-replacement iterations (host loop).
+__global__ void __launch_bounds__(D_WARPS * 32) k_phase_d16(PcgDev c, int b0, int b1, int guarded)
 {
     if(c.flags[F_DONE]) return;
+    if(guarded)
+    {
+        const long k = (long)c.scal[SS_ITER];
+        if(c.prm.refine <= 0 || k % c.prm.refine != 0) return;
+    }
     extern __shared__ __align__(128) char dsm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     char* base = dsm + (size_t)warp * D_WARP_BYTES;
     char* const stage0 = base;
     char* const stage1 = base + D_BUF;
     const unsigned bar0 = smem_u32(base + 2 * D_BUF), bar1 = bar0 + 8;
-    const int gw = blockIdx.x * D_WARPS + warp, nw = gridDim.x * D_WARPS;
-    if(gw >= c.nbanks) return;
+    const int gw = b0 + blockIdx.x * D_WARPS + warp, nw = gridDim.x * D_WARPS;
+    if(gw >= b1) return;
     // this lane's eight blocks: word offset of block k in the packed upper order and
     // whether it is used transposed (the stored block is (cc, a) with cc < a)
     const int a = lane & 15, h = lane >> 4;
@@ -708,18 +714,18 @@ __global__ void __launch_bounds__(D_WARPS * 32) k_phase_d16(PcgDev c)
     __syncwarp();
     unsigned ph0 = 0u, ph1 = 0u;
     int buf = 0;
-    for(int bk = gw; bk < c.nbanks; bk += nw, buf ^= 1)
+    for(int bk = gw; bk < b1; bk += nw, buf ^= 1)
     {
         char* const cur = buf ? stage1 : stage0;
         const unsigned bcur = buf ? bar1 : bar0, bnext = buf ? bar0 : bar1;
         // prefetch the next bank into the other stage (its previous contents are consumed)
         const int nxt = bk + nw;
-        if(lane == 0 && nxt < c.nbanks)
+        if(lane == 0 && nxt < b1)
         {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             d16_issue(c, buf ? stage0 : stage1, bnext, nxt);
         }
-        if(!mbar_wait(bcur, buf ? ph1 : ph0))
+        if(!__all_sync(0xffffffffu, mbar_wait(bcur, buf ? ph1 : ph0)))
         {
             if(lane == 0)
             {
@@ -727,7 +733,7 @@ __global__ void __launch_bounds__(D_WARPS * 32) k_phase_d16(PcgDev c)
                 atomicExch(c.flags + F_DONE, 1);
             }
             // let any copy still in flight land before the CTA's shared memory is released
-            if(nxt < c.nbanks) mbar_wait(bnext, buf ? ph0 : ph1);
+            if(nxt < b1) mbar_wait(bnext, buf ? ph0 : ph1);
             return;
         }
         if(buf)
@@ -748,6 +754,217 @@ __global__ void __launch_bounds__(D_WARPS * 32) k_phase_d16(PcgDev c)
         if(h == 0) st4(c.Z + ((size_t)bk * 16 + a) * 4, z0, z1, z2);
         __syncwarp();
     }
+}
+
+// ---------------------------------------------------------------------------------------
+// B + D0 (16-vertex banks; graph and host loops): phase B fused with the level-0 bank
+// solves.  One warp per level-0 bank (BD_WARPS per CTA, persistent over the banks), with a
+// two-stage ring per warp filled by bulk copies (cp.async.bulk, completion on an mbarrier):
+// a stage holds the bank's packed inverse and, when the bank's 16 slots are 16 consecutive
+// block rows (the Morton ordering), their p, q, x and r.  Nothing in a stage depends on the
+// p.q / r.z sums, so lane 0 starts the warp's first copy before the partials are summed, and
+// the next bank's copy before the current bank is computed.  Lanes 0..15 then update x and r
+// of the bank's slots (other slot maps, and a partial last bank, load their rows directly),
+// restrict the level-0 components into level 1 in lane order (as phase_b_mas), and the whole
+// warp solves the bank from the residual slots in shared memory in the order of
+// bank_dev.cuh.  The level-0 residual slots are not stored: nothing after this phase reads
+// them (a residual replacement restricts again and solves level 0 with k_phase_d16).
+// ---------------------------------------------------------------------------------------
+constexpr int BD_WARPS = 4;
+constexpr int BD_THREADS = BD_WARPS * 32;
+
+template <typename T>
+struct BdStage
+{
+    static constexpr int P = D_PBYTES;                         // packed inverse
+    static constexpr int PSLOT = P;                            // 16 zp slots {z, p} of the rows
+    static constexpr int Q = PSLOT + 16 * 8 * (int)sizeof(T);  // 16 q slots
+    static constexpr int X = Q + 16 * 4 * (int)sizeof(T);      // 16 x 3 FP64
+    static constexpr int R = X + 16 * 3 * 8;                   // 16 x 3 FP64
+    static constexpr int BYTES = R + 16 * 3 * 8;               // one stage (16-byte multiple)
+    static constexpr int AXPY = BYTES - P;
+    static constexpr int WARP = 2 * BYTES + D_RBYTES + 16;     // two stages, 16 slots, two mbarriers
+};
+
+// x_i += a p_i, r_i -= a q_i for the three dofs of one block row; adds |r_i|^2 to acc
+__device__ __forceinline__ void axpy_vals(double a, const double p[3], const double q[3], double x[3], double r[3],
+                                          double& acc)
+{
+#pragma unroll
+    for(int d = 0; d < 3; d++)
+    {
+        x[d] = fma(a, p[d], x[d]);
+        r[d] = fma(-a, q[d], r[d]);
+    }
+    acc = fma(r[2], r[2], fma(r[1], r[1], fma(r[0], r[0], acc)));
+}
+
+template <typename T>
+__device__ __forceinline__ void bd_issue(const PcgDev& c, const T* pn, const T* q, char* stage, unsigned bar, int bk,
+                                         int fem_row, bool staged_rows)
+{
+    using S = BdStage<T>;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                 "r"((unsigned)(staged_rows ? S::BYTES : S::P))
+                 : "memory");
+    tma_load_1d(stage, c.inv + (size_t)bk * 136 * 9, S::P, bar);
+    if(staged_rows)
+    {
+        const size_t row0 = (size_t)fem_row + 16 * (size_t)bk;
+        tma_load_1d(stage + S::PSLOT, pn + 8 * row0, 16 * 8 * sizeof(T), bar);
+        tma_load_1d(stage + S::Q, q + 4 * row0, 16 * 4 * sizeof(T), bar);
+        tma_load_1d(stage + S::X, c.x + 3 * row0, 16 * 3 * 8, bar);
+        tma_load_1d(stage + S::R, c.r + 3 * row0, 16 * 3 * 8, bar);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BD_THREADS) k_phase_bd16(PcgDev c)
+{
+    using S = BdStage<T>;
+    if(c.flags[F_DONE]) return;
+    extern __shared__ __align__(128) char bsm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    char* const base = bsm + (size_t)warp * S::WARP;
+    float4* const rs = reinterpret_cast<float4*>(base + 2 * S::BYTES);
+    const unsigned bar0 = smem_u32(base + 2 * S::BYTES + D_RBYTES), bar1 = bar0 + 8;
+    const int nb0 = c.M / 16;
+    const int gw = blockIdx.x * BD_WARPS + warp, nw = gridDim.x * BD_WARPS;
+    const T* pn = zpbuf<T>(c, iter_parity(c) ^ 1);
+    const T* q = reinterpret_cast<const T*>(c.q);
+    const int fem_row = c.fem_dof / 3;
+    // a bank's rows are staged when its 16 slots are 16 consecutive rows (and the caller's x
+    // is 16-byte aligned, as bulk copies need)
+    const bool aligned = ((reinterpret_cast<uintptr_t>(c.x) | reinterpret_cast<uintptr_t>(c.r)) & 15) == 0;
+    auto staged = [&](int bk) { return aligned && c.identity && 16 * bk + 16 <= c.V; };
+    if(lane == 0 && gw < nb0)
+    {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        bd_issue<T>(c, pn, q, base, bar0, gw, fem_row, staged(gw));
+    }
+    double pq, rz;
+    consume_sum2<BD_THREADS>(c, SITE_A, c.grid_a, SITE_E, c.grid_e, pq, rz);
+    const bool ok = pq > 0.0 && isfinite(pq);  // else breakdown: no update; the last CTA reports it
+    const double alpha = ok ? rz / pq : 0.0;
+    double acc = 0;
+    unsigned ph0 = 0u, ph1 = 0u;
+    int buf = 0;
+    bool failed = false;
+    for(int bk = gw; bk < nb0; bk += nw, buf ^= 1)
+    {
+        char* const cur = buf ? base + S::BYTES : base;
+        const unsigned bcur = buf ? bar1 : bar0, bnext = buf ? bar0 : bar1;
+        const int nxt = bk + nw;
+        if(lane == 0 && nxt < nb0)
+        {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            bd_issue<T>(c, pn, q, buf ? base : base + S::BYTES, bnext, nxt, fem_row, staged(nxt));
+        }
+        if(!__all_sync(0xffffffffu, mbar_wait(bcur, buf ? ph1 : ph0)))
+        {
+            failed = true;
+            // let the copy still in flight land before the CTA's shared memory is released
+            if(lane == 0 && nxt < nb0) mbar_wait(bnext, buf ? ph0 : ph1);
+            break;
+        }
+        if(buf)
+            ph1 ^= 1u;
+        else
+            ph0 ^= 1u;
+        // x / r update and the level-0 -> 1 restriction of the bank's slots (lanes 0..15)
+        const int s = 16 * bk + lane;
+        const int v = lane >= 16 ? -1 : (c.identity ? (s < c.V ? s : -1) : c.part_map[s]);
+        float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+        unsigned msk = 0;
+        if(v >= 0 && ok)
+        {
+            const int row = fem_row + v;
+            double pv[3], qv[3], xv[3], rv[3];
+            if(staged(bk))
+            {
+                const T* ps = reinterpret_cast<const T*>(cur + S::PSLOT) + 8 * lane + 4;
+                const T* qs = reinterpret_cast<const T*>(cur + S::Q) + 4 * lane;
+                const double* xs = reinterpret_cast<const double*>(cur + S::X) + 3 * lane;
+                const double* rr = reinterpret_cast<const double*>(cur + S::R) + 3 * lane;
+#pragma unroll
+                for(int d = 0; d < 3; d++)
+                {
+                    pv[d] = (double)ps[d];
+                    qv[d] = (double)qs[d];
+                    xv[d] = xs[d];
+                    rv[d] = rr[d];
+                }
+            }
+            else
+            {
+                T p0, p1, p2, q0, q1, q2;
+                ld4(pn + 8 * (size_t)row + 4, p0, p1, p2);
+                ld4(q + 4 * (size_t)row, q0, q1, q2);
+                pv[0] = (double)p0; pv[1] = (double)p1; pv[2] = (double)p2;
+                qv[0] = (double)q0; qv[1] = (double)q1; qv[2] = (double)q2;
+#pragma unroll
+                for(int d = 0; d < 3; d++)
+                {
+                    xv[d] = c.x[3 * (size_t)row + d];
+                    rv[d] = c.r[3 * (size_t)row + d];
+                }
+            }
+            const double a = c.seg_of_row ? __ldcg(c.seg + SEG_N * c.seg_of_row[row] + SG_ALPHA) : alpha;
+            double rr2 = 0.0;
+            axpy_vals(a, pv, qv, xv, rv, rr2);
+            acc += rr2;
+#pragma unroll
+            for(int d = 0; d < 3; d++)
+            {
+                c.x[3 * (size_t)row + d] = xv[d];
+                c.r[3 * (size_t)row + d] = rv[d];
+            }
+            if(c.seg_of_row) c.seg_row[(size_t)c.nrows + row] = rr2;
+            r0 = (float)rv[0];
+            r1 = (float)rv[1];
+            r2 = (float)rv[2];
+            msk = c.fine_mask[v];
+        }
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+        for(int bb = 0; bb < 16; bb++)
+        {
+            const float x0 = group_shfl<16>(r0, bb);
+            const float x1 = group_shfl<16>(r1, bb);
+            const float x2 = group_shfl<16>(r2, bb);
+            if(msk & (1u << bb))
+            {
+                a0 += x0;
+                a1 += x1;
+                a2 += x2;
+            }
+        }
+        if(v >= 0 && ok && __popc(msk & lanemask_lt(lane)) == 0)
+            st4(c.R + 4 * (size_t)c.going_next[v], a0, a1, a2);
+        if(lane < 16) rs[lane] = make_float4(r0, r1, r2, 0.f);
+        __syncwarp();
+        // the bank solve: z = P r_0 from the staged inverse
+        float z0, z1, z2;
+        bank16_half(reinterpret_cast<const float*>(cur), rs, lane & 15, lane >> 4, z0, z1, z2);
+        bank16_join(z0, z1, z2);
+        if(lane < 16) st4(c.Z + ((size_t)bk * 16 + lane) * 4, z0, z1, z2);
+        __syncwarp();
+    }
+    if(failed && lane == 0)
+    {
+        atomicExch(c.flags + F_STATUS, 6);  // STG_ERR_TIMEOUT
+        atomicExch(c.flags + F_DONE, 1);
+    }
+    // the ABD range: plain axpy
+    if(ok)
+        for(int i = blockIdx.x * BD_THREADS + threadIdx.x; i < c.abd_bodies * 4; i += gridDim.x * BD_THREADS)
+        {
+            double d0, d1, d2;
+            axpy_row<T>(c, pn, q, alpha, i, d0, d1, d2, acc);
+        }
+    finish_reduction<BD_THREADS>(c, acc, SITE_B, POST_CHECK_PQ, 0, pq, rz);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -995,7 +1212,7 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T, RTT>::MIN_CTAS) k_phase_a_
             const int s = k % G::STAGES;
             const int r0 = rb + k * RT, r1 = min(r0 + RT, re);
             const int i = r0 + rloc;
-            if(!mbar_wait(bar_full + 8 * s, (k / G::STAGES) & 1))
+            if(!__all_sync(0xffffffffu, mbar_wait(bar_full + 8 * s, (k / G::STAGES) & 1)))
             {
                 failed = true;
                 break;
@@ -1732,8 +1949,48 @@ int selftest_wait(int* status, double* seconds)
 // host driver
 // ---------------------------------------------------------------------------------------
 // MAS levels >= 2 restriction (C1 parallel, C2 one CTA) and the bank solves (D)
+// the 16-bank solves of banks [b0, b1): warp per bank, TMA-staged; one resident wave of CTAs
+static int launch_d16(Solver& S, const PcgDev& c, int b0, int b1, int guarded)
+{
+    if(b1 <= b0) return 0;
+    const int smem = D_WARPS * D_WARP_BYTES;
+    static thread_local unsigned long long attr_done = 0;
+    if(first_on_device(attr_done))
+        STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_d16, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 0;
+    STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase_d16, D_WARPS * 32, smem));
+    const int grid = std::max(1, std::min(div_up(b1 - b0, D_WARPS), std::max(per_sm, 1) * kSMs));
+    k_phase_d16<<<grid, D_WARPS * 32, smem, S.stream>>>(c, b0, b1, guarded);
+    STG_LAUNCH_CHECK();
+    S.launches++;
+    return 0;
+}
+
+// phase B fused with the level-0 bank solves (16-banks): one resident wave of CTAs
+template <typename T>
+static int launch_bd16(Solver& S, const PcgDev& c)
+{
+    const int smem = BD_WARPS * BdStage<T>::WARP;
+    static thread_local unsigned long long attr_done = 0;
+    if(first_on_device(attr_done))
+    {
+        STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_bd16<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_bd16<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          cudaSharedmemCarveoutMaxShared));
+    }
+    int per_sm = 0;
+    STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase_bd16<T>, BD_THREADS, smem));
+    const int grid = std::max(1, std::min(div_up(c.M / 16, BD_WARPS), std::max(per_sm, 1) * kSMs));
+    k_phase_bd16<T><<<grid, BD_THREADS, smem, S.stream>>>(c);
+    STG_LAUNCH_CHECK();
+    S.launches++;
+    return 0;
+}
+
+// Restriction of the coarse levels and the bank solves of banks [d_from, nbanks) (d_from =
+// M / 16 when phase B has solved level 0 already).
 template <int B>
-static int launch_mas_cd(Solver& S, const PcgDev& c)
+static int launch_mas_cd(Solver& S, const PcgDev& c, int d_from = 0)
 {
     cudaStream_t s = S.stream;
     if(c.L > 2)
@@ -1749,20 +2006,8 @@ static int launch_mas_cd(Solver& S, const PcgDev& c)
         STG_LAUNCH_CHECK();
         S.launches++;
     }
-    if(B == 16)
-    {
-        // warp per bank, TMA-staged; one resident wave of CTAs
-        const int smem = D_WARPS * D_WARP_BYTES;
-        static thread_local unsigned long long attr_done = 0;
-        if(first_on_device(attr_done))
-            STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_d16, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        int per_sm = 0;
-        STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase_d16, D_WARPS * 32, smem));
-        const int grid = std::max(1, std::min(div_up(c.nbanks, D_WARPS), std::max(per_sm, 1) * kSMs));
-        k_phase_d16<<<grid, D_WARPS * 32, smem, s>>>(c);
-    }
-    else
-        k_phase_d<B><<<std::max(1, std::min(c.nbanks, kSMs * 8)), PB, 0, s>>>(c);
+    if(B == 16) return launch_d16(S, c, d_from, c.nbanks, 0);
+    k_phase_d<B><<<std::max(1, std::min(c.nbanks, kSMs * 8)), PB, 0, s>>>(c);
     STG_LAUNCH_CHECK();
     S.launches++;
     return 0;
@@ -1885,9 +2130,18 @@ static int launch_iteration(Solver& S, const PcgDev& c, int grid_vec, int grid_r
         STG_LAUNCH_CHECK();
         S.launches++;
     }
-    k_phase_b<T, B><<<B > 0 ? std::max(1, std::min(div_up(c.M, PB), kSMs * 4)) : grid_vec, PB, 0, s>>>(c);
-    STG_LAUNCH_CHECK();
-    S.launches += 2;
+    if(B == 16)
+    {
+        // B fused with the level-0 bank solves
+        STG_TRY(launch_bd16<T>(S, c));
+        S.launches++;
+    }
+    else
+    {
+        k_phase_b<T, B><<<B > 0 ? std::max(1, std::min(div_up(c.M, PB), kSMs * 4)) : grid_vec, PB, 0, s>>>(c);
+        STG_LAUNCH_CHECK();
+        S.launches += 2;
+    }
     if(c.seg_of_row)
     {
         k_seg<SEG_B><<<c.nseg, PB, 0, s>>>(c);
@@ -1926,9 +2180,11 @@ static int launch_iteration(Solver& S, const PcgDev& c, int grid_vec, int grid_r
                 STG_LAUNCH_CHECK();
                 S.launches++;
             }
+            // the fused B solved level 0 before the replacement: solve it again
+            if(B == 16) STG_TRY(launch_d16(S, c, 0, c.M / 16, 1));
         }
     }
-    if(B > 0) STG_TRY(launch_mas_cd<(B > 0 ? B : 16)>(S, c));
+    if(B > 0) STG_TRY(launch_mas_cd<(B > 0 ? B : 16)>(S, c, B == 16 ? c.M / 16 : 0));
     if(c.net_mode) STG_TRY(launch_learned(S, c));
     k_phase_e<T, B><<<grid_vec, PB, 0, s>>>(c, POST_BETA);
     STG_LAUNCH_CHECK();
@@ -1954,11 +2210,13 @@ static int record_if_body(Solver& S, const PcgDev& c, int grid_rows, cudaGraph_t
         k_restrict01<(B > 0 ? B : 16)><<<std::max(1, std::min(div_up(c.M, PB), kSMs * 4)), PB, 0, s>>>(c, 0);
         e1 = cudaGetLastError();
     }
+    int rc = 0;
+    if(B == 16 && e1 == cudaSuccess) rc = launch_d16(S, c, 0, c.M / 16, 0);
     cudaGraph_t out = body;
     cudaError_t e2 = cudaStreamEndCapture(s, &out);
     STG_CUDA_TRY(e1);
     STG_CUDA_TRY(e2);
-    return 0;
+    return rc;
 }
 
 // Every kernel of the iteration asks for the same shared-memory carveout (the largest), so

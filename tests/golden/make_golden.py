@@ -9,7 +9,10 @@ cloth_high_sorted.16.{obj,part}
 MeshProcess/metis_partition/src/metis_sort.cpp) and stores their element connectivity,
 vertex positions and per-vertex partition ids as compressed .npz files next to this script.
 These pin the CEMAS ordering inputs (partId per vertex, vertices grouped by part) for the
-MAS hierarchy tests; nothing else is taken from the reference.
+MAS hierarchy tests.  The unsorted meshes they were made from (Assets/tetMesh/{cube,bunny2,
+high_mat}.msh, Assets/triMesh/cloth_high.obj) are stored as *_input.npz (positions, elements)
+for the METIS regeneration test (tests/test_metis_cpu.py); nothing else is taken from the
+reference.
 """
 from __future__ import annotations
 
@@ -22,20 +25,17 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def read_msh(path):
-    """gmsh 2.2 ASCII: $Nodes (id x y z), $Elements (id type ntags [tags] v...), tets are type 4."""
+    """gmsh 2.2 ASCII as the reference's TetMesh loader reads it (MeshProcess/metis_partition/
+    src/mesh.cpp:265-335): a node is the last three fields of its line, an element the last
+    four (Assets/tetMesh/bunny2.msh declares two tags per element but writes none)."""
     with open(path) as f:
         lines = f.read().split("\n")
     i = lines.index("$Nodes")
     nn = int(lines[i + 1])
-    pos = np.array([[float(t) for t in lines[i + 2 + k].split()[1:4]] for k in range(nn)])
+    pos = np.array([[float(t) for t in lines[i + 2 + k].split()[-3:]] for k in range(nn)])
     j = lines.index("$Elements")
     ne = int(lines[j + 1])
-    tets = []
-    for k in range(ne):
-        t = lines[j + 2 + k].split()
-        if int(t[1]) == 4:
-            ntag = int(t[2])
-            tets.append([int(v) - 1 for v in t[3 + ntag:3 + ntag + 4]])
+    tets = [[int(v) - 1 for v in lines[j + 2 + k].split()[-4:]] for k in range(ne)]
     return pos, np.array(tets, dtype=np.int32)
 
 
@@ -70,6 +70,12 @@ def main(ref_root):
     assert part.size == pos.shape[0]
     np.savez_compressed(os.path.join(HERE, "cloth_high_sorted16.npz"), pos=pos.astype(np.float32), tris=tris, part=part)
     print("cloth_high", pos.shape[0], "verts", tris.shape[0], "tris")
+    # the unsorted meshes the METIS ordering starts from (Assets/tetMesh, Assets/triMesh)
+    for name in ("cube", "bunny2", "high_mat"):
+        pos, tets = read_msh(os.path.join(ref_root, "Assets", "tetMesh", f"{name}.msh"))
+        np.savez_compressed(os.path.join(HERE, f"{name}_input.npz"), pos=pos.astype(np.float32), elems=tets)
+    pos, tris = read_obj(os.path.join(ref_root, "Assets", "triMesh", "cloth_high.obj"))
+    np.savez_compressed(os.path.join(HERE, "cloth_high_input.npz"), pos=pos.astype(np.float32), elems=tris)
 
 
 if __name__ == "__main__":

@@ -144,13 +144,19 @@ def test_mas_hierarchy_bit_exact_morton(dev, bank, with_contacts):
     _compare_hierarchy(om, solver, pm)
 
 
+@pytest.mark.parametrize("name", ["bunny2", "high_mat"])
 @pytest.mark.parametrize("with_contacts", [False, True])
-def test_mas_hierarchy_bit_exact_metis_fixture(dev, with_contacts):
-    """bunny2 as the reference ships it: METIS 16-vertex partitions, partition-sorted."""
-    s, part = fixture_system("bunny2")
+def test_mas_hierarchy_bit_exact_metis_fixture(dev, name, with_contacts):
+    """The reference's METIS-sorted meshes as it ships them: 16-vertex partitions (bunny2:
+    19,193 vertices in 1,280 parts; high_mat: 45,000 in 3,000), partition-sorted.  The
+    hierarchy, and the bank matrices and inverses assembled on it, are bit-exact."""
+    s, part = fixture_system(name)
     cp = random_contacts(s.num_verts, 2000, seed=12) if with_contacts else None
     om, solver, pm, _ = _mas_pair(s, 16, part=part, contacts=cp, dev=dev)
     _compare_hierarchy(om, solver, pm)
+    em, ei = om.matrices()
+    gm, gi = solver.export_matrices()
+    assert np.array_equal(gm, em) and np.array_equal(gi, ei)
 
 
 @pytest.mark.parametrize("bank", [16, 32])
