@@ -513,9 +513,10 @@ def main():
     tuned = make("fp32")
     tuned.spmv_tiles(0)
     solve(tuned)
-    rt_t, us_def, us_alt = tuned.spmv_tiles_info()
+    rt_t, us_def, us_alt, us_halo = tuned.spmv_tiles_info()
     tuned.close()
-    tiles = {"default_rows_per_tile": 64, "tuned_rows_per_tile": rt_t, "us_per_launch": {"64x4": us_def, "32x8": us_alt}}
+    tiles = {"default_rows_per_tile": 64, "tuned": "halo" if rt_t == -2 else f"{rt_t} rows per tile",
+             "us_per_launch": {"tiled 64x4": us_def, "tiled 32x8": us_alt, "halo 64x4": us_halo}}
 
     # roofline of the dominant kernel: the PCG SpMV of the FP32 path, timed live
     solve(fast)

@@ -208,6 +208,15 @@ int stg_profile_spmv(stg_handle h, int reps, float* avg_ms, double* bytes);
  * the device stays usable.  Returns STG_OK when the diagnostic ran. */
 int stg_selftest_wait_timeout(int* status, double* seconds);
 
+/* ---- Morton keys ----------------------------------------------------------------------- */
+/* Replaces _calcVertMChash (StiffGIPC/GIPC.cu:453-502) with hash_code type -1 and expand_bits
+ * (GIPC.cu:183-208): keys[i] = (code << 32) | i, code the 30-bit interleave (x << 2 | y << 1 | z)
+ * of the position's cell at 1024 cells per axis of the bounding box of all n positions
+ * (normalised, clamped to [0, 1023], truncated).  Ascending keys give the Morton vertex
+ * order of the MAS banks.  pos: device double[3n]; keys: device uint64[n]; stream: a
+ * cudaStream_t (NULL: the legacy default stream).  Asynchronous on the stream. */
+int stg_morton_keys(int n, const double* pos, uint64_t* keys, void* stream);
+
 /* ---- Hessian producer ------------------------------------------------------------------ */
 /* The triplets and gradient of one implicit-Euler Newton iteration of a tet mesh, on the
  * GPU: what GIPC hands to GlobalLinearSystem::solve_linear_system (femEnergy.cu:1719-1855
@@ -251,16 +260,21 @@ int stg_set_segments(stg_handle h, const int32_t* row_offsets, int nseg);
 int stg_segment_stats(stg_handle h, int* iterations, double* rel_residual);
 
 /* ---- BCOO tile autotuner -------------------------------------------------------------- */
-/* No counterpart in the reference.  Tile shape of the in-loop SpMV: rows_per_tile rows per
+/* No counterpart in the reference.  Kernel of the in-loop SpMV: rows_per_tile rows per
  * tile of the row-sliced full copy, with 256 / rows_per_tile lanes per row (FP32: 64 or 32;
- * FP64: 32 or 16).  0 = autotune: the next solve of a new system shape (precision, block
- * rows, unique blocks) times every candidate on that system and keeps the fastest for the
- * handle; -1 = the precision's default (64 / 32).  Results differ between tile shapes in
- * the last bits (summation order); a fixed shape keeps solves bitwise reproducible. */
+ * FP64: 32 or 16), or -2: the halo kernel (fixed tiles whose column operands are staged in
+ * shared memory).  0 = autotune: the next solve of a new shape class (precision, block rows,
+ * unique blocks) times every candidate (both tile shapes, and the halo kernel when its
+ * windows fit) on that system; the choice is kept for that shape class by every handle of
+ * the process.  -1 = the precision's default shape (64 / 32).  Results differ between
+ * candidates in the last bits (summation order); a fixed choice keeps solves bitwise
+ * reproducible across processes. */
 int stg_spmv_tiles(stg_handle h, int rows_per_tile);
-/* Rows per tile of the last solve, and the autotuner's mean time per launch of each
- * candidate in microseconds (default shape first; 0 when it has not run). */
-int stg_spmv_tiles_info(stg_handle h, int* rows_per_tile, float* us_default, float* us_alternative);
+/* Rows per tile of the last solve (-2: the halo kernel), and the autotuner's mean time per
+ * launch of each candidate in microseconds (0 when it has not run or the candidate did not
+ * fit). */
+int stg_spmv_tiles_info(stg_handle h, int* rows_per_tile, float* us_default, float* us_alternative,
+                        float* us_halo);
 
 /* ---- allocation-free SpMV ---------------------------------------------------------- */
 /* No counterpart in the reference.  The same y = a * A * x + b * y as stg_spmv (same

@@ -36,6 +36,9 @@
 #include "spmv_core.cuh"
 #include "bank_dev.cuh"
 
+#include <map>
+#include <mutex>
+
 namespace stg
 {
 
@@ -360,55 +363,103 @@ __device__ __forceinline__ void axpy_row(const PcgDev& c, const T* pn, const T* 
     acc += r0 * r0 + r1 * r1 + r2 * r2;
 }
 
+// One level-0 slot of phase B (MAS): its row's p, q, x, r, closed mask and level-1 parent,
+// loaded before alpha is known (the loads do not depend on it)
+template <typename T>
+struct BSlot
+{
+    int v = -1;
+    T p[3], q[3];
+    double x[3], r[3];
+    unsigned msk = 0u;
+    int gnext = 0;
+};
+
+template <typename T>
+__device__ __forceinline__ void b_load(const PcgDev& c, const T* pn, const T* q, int s, BSlot<T>& L)
+{
+    L.v = c.identity ? (s < c.V ? s : -1) : (s < c.M ? c.part_map[s] : -1);
+    if(L.v < 0) return;
+    const size_t row = (size_t)(c.fem_dof / 3) + L.v;
+    ld4(pn + 8 * row + 4, L.p[0], L.p[1], L.p[2]);
+    ld4(q + 4 * row, L.q[0], L.q[1], L.q[2]);
+#pragma unroll
+    for(int d = 0; d < 3; d++)
+    {
+        L.x[d] = c.x[3 * row + d];
+        L.r[d] = c.r[3 * row + d];
+    }
+    L.msk = c.fine_mask[L.v];
+    L.gnext = c.going_next[L.v];
+}
+
+// x_i += alpha p_i, r_i -= alpha q_i of the slot, the level-0 residual slot and the level-0 ->
+// 1 restriction (each component of a level-0 bank sums its members in lane order); every lane
+// of the warp calls it (group shuffles).  Returns the slot's |r_i|^2.
 template <typename T, int B>
-__device__ __forceinline__ double phase_b_mas(const PcgDev& c, int gt, int gn, double alpha)
+__device__ __forceinline__ double b_update(const PcgDev& c, BSlot<T>& L, int s, double alpha)
+{
+    float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+    double rr = 0.0;
+    if(L.v >= 0)
+    {
+        const size_t row = (size_t)(c.fem_dof / 3) + L.v;
+        const double a = c.seg_of_row ? __ldcg(c.seg + SEG_N * c.seg_of_row[row] + SG_ALPHA) : alpha;
+#pragma unroll
+        for(int d = 0; d < 3; d++)
+        {
+            L.x[d] = fma(a, (double)L.p[d], L.x[d]);
+            L.r[d] = fma(-a, (double)L.q[d], L.r[d]);
+            c.x[3 * row + d] = L.x[d];
+            c.r[3 * row + d] = L.r[d];
+        }
+        rr = fma(L.r[2], L.r[2], fma(L.r[1], L.r[1], L.r[0] * L.r[0]));
+        if(c.seg_of_row) c.seg_row[(size_t)c.nrows + row] = rr;
+        r0 = (float)L.r[0];
+        r1 = (float)L.r[1];
+        r2 = (float)L.r[2];
+    }
+    if(s < c.M) st4(c.R + 4 * (size_t)s, r0, r1, r2);
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+    for(int bb = 0; bb < B; bb++)
+    {
+        const float x0 = group_shfl<B>(r0, bb);
+        const float x1 = group_shfl<B>(r1, bb);
+        const float x2 = group_shfl<B>(r2, bb);
+        if(L.msk & (1u << bb))
+        {
+            a0 += x0;
+            a1 += x1;
+            a2 += x2;
+        }
+    }
+    if(L.v >= 0 && __popc(L.msk & lanemask_lt(s % B)) == 0) st4(c.R + 4 * (size_t)L.gnext, a0, a1, a2);
+    return rr;
+}
+
+// B (MAS): x / r update over the FEM range in level-0 slot order + level-0/1 restriction;
+// plain axpy over the ABD range.  `first` (with have_first): slot gt's loads, issued by the
+// caller before alpha was known.  Returns this thread's share of r.r.
+template <typename T, int B>
+__device__ __forceinline__ double phase_b_mas(const PcgDev& c, int gt, int gn, double alpha, BSlot<T>& first,
+                                              bool have_first)
 {
     const T* pn = zpbuf<T>(c, iter_parity(c) ^ 1);
     const T* q = reinterpret_cast<const T*>(c.q);
     double acc = 0;
     const int span = (c.M + 31) / 32 * 32;
-    const int fem_row = c.fem_dof / 3;
-    for(int s = gt; s < span; s += gn)
+    int s = gt;
+    if(have_first && s < span)
     {
-        const int v = c.identity ? (s < c.V ? s : -1) : (s < c.M ? c.part_map[s] : -1);
-        float r0 = 0.f, r1 = 0.f, r2 = 0.f;
-        unsigned msk = 0;
-        if(v >= 0)
-        {
-            double d0, d1, d2;
-            const int row = fem_row + v;
-            const double a = c.seg_of_row ? __ldcg(c.seg + SEG_N * c.seg_of_row[row] + SG_ALPHA) : alpha;
-            axpy_row<T>(c, pn, q, a, row, d0, d1, d2, acc);
-            if(c.seg_of_row) c.seg_row[(size_t)c.nrows + row] = d0 * d0 + d1 * d1 + d2 * d2;
-            r0 = (float)d0;
-            r1 = (float)d1;
-            r2 = (float)d2;
-            msk = c.fine_mask[v];
-        }
-        if(s < c.M)
-        {
-            st4(c.R + 4 * (size_t)s, r0, r1, r2);
-        }
-        float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-#pragma unroll
-        for(int bb = 0; bb < B; bb++)
-        {
-            const float x0 = group_shfl<B>(r0, bb);
-            const float x1 = group_shfl<B>(r1, bb);
-            const float x2 = group_shfl<B>(r2, bb);
-            if(msk & (1u << bb))
-            {
-                a0 += x0;
-                a1 += x1;
-                a2 += x2;
-            }
-        }
-        const int lane = s % B;
-        if(v >= 0 && __popc(msk & lanemask_lt(lane)) == 0)
-        {
-            const int g = c.going_next[v];
-            st4(c.R + 4 * (size_t)g, a0, a1, a2);
-        }
+        acc += b_update<T, B>(c, first, s, alpha);
+        s += gn;
+    }
+    for(; s < span; s += gn)
+    {
+        BSlot<T> L;
+        b_load<T>(c, pn, q, s, L);
+        acc += b_update<T, B>(c, L, s, alpha);
     }
     for(int i = gt; i < c.abd_bodies * 4; i += gn)
     {
@@ -635,7 +686,14 @@ constexpr int D_PBYTES = 136 * 9 * 4;             // packed inverse of one bank
 constexpr int D_RBYTES = 16 * 16;                 // 16 float4 residual slots
 constexpr int D_BUF = D_PBYTES + D_RBYTES;        // one stage (16-byte multiple)
 constexpr int D_WARP_BYTES = 2 * D_BUF + 16;      // two stages + two mbarriers
-constexpr unsigned D_WAIT_LIMIT = 1u << 22;       // bounded mbarrier polling
+constexpr unsigned long long WAIT_NS = 1000000000ull;  // every bounded wait gives up after 1 s
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ unsigned smem_u32(const void* p)
 {
@@ -650,10 +708,31 @@ __device__ __forceinline__ void tma_load_1d(void* dst, const void* src, unsigned
                  : "memory");
 }
 
-// waits for phase `parity` of the mbarrier; false when the bounded wait gave up
+// waits for phase `parity` of the mbarrier; false when the bounded wait gave up (WAIT_NS of
+// the global timer, read every 256 polls)
+__device__ __noinline__ bool mbar_wait_slow(unsigned bar, unsigned parity);
+
+__device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok)
+                 : "r"(bar), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+// fast path inline (one poll); the timed loop out of line (inlining it into the pipelined
+// kernels makes ptxas 12.9 for sm_100a abort in register allocation)
 __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity)
 {
-    for(unsigned it = 0; it < D_WAIT_LIMIT; it++)
+    return mbar_try(bar, parity) || mbar_wait_slow(bar, parity);
+}
+
+__device__ __noinline__ bool mbar_wait_slow(unsigned bar, unsigned parity)
+{
+    unsigned long long t0 = 0;
+    for(unsigned it = 1; it != 0u; it++)  // the timer ends it; the count only bounds the loop
     {
         unsigned ok;
         asm volatile(
@@ -662,6 +741,14 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity)
             : "r"(bar), "r"(parity)
             : "memory");
         if(ok) return true;
+        if((it & 255u) == 0u)
+        {
+            const unsigned long long t = global_ns();
+            if(t0 == 0)
+                t0 = t;
+            else if(t - t0 > WAIT_NS)
+                return false;
+        }
     }
     return false;
 }
@@ -756,215 +843,10 @@ __global__ void __launch_bounds__(D_WARPS * 32) k_phase_d16(PcgDev c, int b0, in
     }
 }
 
-// ---------------------------------------------------------------------------------------
-// B + D0 (16-vertex banks; graph and host loops): phase B fused with the level-0 bank
-// solves.  One warp per level-0 bank (BD_WARPS per CTA, persistent over the banks), with a
-// two-stage ring per warp filled by bulk copies (cp.async.bulk, completion on an mbarrier):
-// a stage holds the bank's packed inverse and, when the bank's 16 slots are 16 consecutive
-// block rows (the Morton ordering), their p, q, x and r.  Nothing in a stage depends on the
-// p.q / r.z sums, so lane 0 starts the warp's first copy before the partials are summed, and
-// the next bank's copy before the current bank is computed.  Lanes 0..15 then update x and r
-// of the bank's slots (other slot maps, and a partial last bank, load their rows directly),
-// restrict the level-0 components into level 1 in lane order (as phase_b_mas), and the whole
-// warp solves the bank from the residual slots in shared memory in the order of
-// bank_dev.cuh.  The level-0 residual slots are not stored: nothing after this phase reads
-// them (a residual replacement restricts again and solves level 0 with k_phase_d16).
-// ---------------------------------------------------------------------------------------
-constexpr int BD_WARPS = 4;
-constexpr int BD_THREADS = BD_WARPS * 32;
-
-template <typename T>
-struct BdStage
+// 16-byte asynchronous copy global -> shared (L2 only)
+__device__ __forceinline__ void cp_async16(void* dst, const void* src)
 {
-    static constexpr int P = D_PBYTES;                         // packed inverse
-    static constexpr int PSLOT = P;                            // 16 zp slots {z, p} of the rows
-    static constexpr int Q = PSLOT + 16 * 8 * (int)sizeof(T);  // 16 q slots
-    static constexpr int X = Q + 16 * 4 * (int)sizeof(T);      // 16 x 3 FP64
-    static constexpr int R = X + 16 * 3 * 8;                   // 16 x 3 FP64
-    static constexpr int BYTES = R + 16 * 3 * 8;               // one stage (16-byte multiple)
-    static constexpr int AXPY = BYTES - P;
-    static constexpr int WARP = 2 * BYTES + D_RBYTES + 16;     // two stages, 16 slots, two mbarriers
-};
-
-// x_i += a p_i, r_i -= a q_i for the three dofs of one block row; adds |r_i|^2 to acc
-__device__ __forceinline__ void axpy_vals(double a, const double p[3], const double q[3], double x[3], double r[3],
-                                          double& acc)
-{
-#pragma unroll
-    for(int d = 0; d < 3; d++)
-    {
-        x[d] = fma(a, p[d], x[d]);
-        r[d] = fma(-a, q[d], r[d]);
-    }
-    acc = fma(r[2], r[2], fma(r[1], r[1], fma(r[0], r[0], acc)));
-}
-
-template <typename T>
-__device__ __forceinline__ void bd_issue(const PcgDev& c, const T* pn, const T* q, char* stage, unsigned bar, int bk,
-                                         int fem_row, bool staged_rows)
-{
-    using S = BdStage<T>;
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-                 "r"((unsigned)(staged_rows ? S::BYTES : S::P))
-                 : "memory");
-    tma_load_1d(stage, c.inv + (size_t)bk * 136 * 9, S::P, bar);
-    if(staged_rows)
-    {
-        const size_t row0 = (size_t)fem_row + 16 * (size_t)bk;
-        tma_load_1d(stage + S::PSLOT, pn + 8 * row0, 16 * 8 * sizeof(T), bar);
-        tma_load_1d(stage + S::Q, q + 4 * row0, 16 * 4 * sizeof(T), bar);
-        tma_load_1d(stage + S::X, c.x + 3 * row0, 16 * 3 * 8, bar);
-        tma_load_1d(stage + S::R, c.r + 3 * row0, 16 * 3 * 8, bar);
-    }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(BD_THREADS) k_phase_bd16(PcgDev c)
-{
-    using S = BdStage<T>;
-    if(c.flags[F_DONE]) return;
-    extern __shared__ __align__(128) char bsm[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    char* const base = bsm + (size_t)warp * S::WARP;
-    float4* const rs = reinterpret_cast<float4*>(base + 2 * S::BYTES);
-    const unsigned bar0 = smem_u32(base + 2 * S::BYTES + D_RBYTES), bar1 = bar0 + 8;
-    const int nb0 = c.M / 16;
-    const int gw = blockIdx.x * BD_WARPS + warp, nw = gridDim.x * BD_WARPS;
-    const T* pn = zpbuf<T>(c, iter_parity(c) ^ 1);
-    const T* q = reinterpret_cast<const T*>(c.q);
-    const int fem_row = c.fem_dof / 3;
-    // a bank's rows are staged when its 16 slots are 16 consecutive rows (and the caller's x
-    // is 16-byte aligned, as bulk copies need)
-    const bool aligned = ((reinterpret_cast<uintptr_t>(c.x) | reinterpret_cast<uintptr_t>(c.r)) & 15) == 0;
-    auto staged = [&](int bk) { return aligned && c.identity && 16 * bk + 16 <= c.V; };
-    if(lane == 0 && gw < nb0)
-    {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        bd_issue<T>(c, pn, q, base, bar0, gw, fem_row, staged(gw));
-    }
-    double pq, rz;
-    consume_sum2<BD_THREADS>(c, SITE_A, c.grid_a, SITE_E, c.grid_e, pq, rz);
-    const bool ok = pq > 0.0 && isfinite(pq);  // else breakdown: no update; the last CTA reports it
-    const double alpha = ok ? rz / pq : 0.0;
-    double acc = 0;
-    unsigned ph0 = 0u, ph1 = 0u;
-    int buf = 0;
-    bool failed = false;
-    for(int bk = gw; bk < nb0; bk += nw, buf ^= 1)
-    {
-        char* const cur = buf ? base + S::BYTES : base;
-        const unsigned bcur = buf ? bar1 : bar0, bnext = buf ? bar0 : bar1;
-        const int nxt = bk + nw;
-        if(lane == 0 && nxt < nb0)
-        {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            bd_issue<T>(c, pn, q, buf ? base : base + S::BYTES, bnext, nxt, fem_row, staged(nxt));
-        }
-        if(!__all_sync(0xffffffffu, mbar_wait(bcur, buf ? ph1 : ph0)))
-        {
-            failed = true;
-            // let the copy still in flight land before the CTA's shared memory is released
-            if(lane == 0 && nxt < nb0) mbar_wait(bnext, buf ? ph0 : ph1);
-            break;
-        }
-        if(buf)
-            ph1 ^= 1u;
-        else
-            ph0 ^= 1u;
-        // x / r update and the level-0 -> 1 restriction of the bank's slots (lanes 0..15)
-        const int s = 16 * bk + lane;
-        const int v = lane >= 16 ? -1 : (c.identity ? (s < c.V ? s : -1) : c.part_map[s]);
-        float r0 = 0.f, r1 = 0.f, r2 = 0.f;
-        unsigned msk = 0;
-        if(v >= 0 && ok)
-        {
-            const int row = fem_row + v;
-            double pv[3], qv[3], xv[3], rv[3];
-            if(staged(bk))
-            {
-                const T* ps = reinterpret_cast<const T*>(cur + S::PSLOT) + 8 * lane + 4;
-                const T* qs = reinterpret_cast<const T*>(cur + S::Q) + 4 * lane;
-                const double* xs = reinterpret_cast<const double*>(cur + S::X) + 3 * lane;
-                const double* rr = reinterpret_cast<const double*>(cur + S::R) + 3 * lane;
-#pragma unroll
-                for(int d = 0; d < 3; d++)
-                {
-                    pv[d] = (double)ps[d];
-                    qv[d] = (double)qs[d];
-                    xv[d] = xs[d];
-                    rv[d] = rr[d];
-                }
-            }
-            else
-            {
-                T p0, p1, p2, q0, q1, q2;
-                ld4(pn + 8 * (size_t)row + 4, p0, p1, p2);
-                ld4(q + 4 * (size_t)row, q0, q1, q2);
-                pv[0] = (double)p0; pv[1] = (double)p1; pv[2] = (double)p2;
-                qv[0] = (double)q0; qv[1] = (double)q1; qv[2] = (double)q2;
-#pragma unroll
-                for(int d = 0; d < 3; d++)
-                {
-                    xv[d] = c.x[3 * (size_t)row + d];
-                    rv[d] = c.r[3 * (size_t)row + d];
-                }
-            }
-            const double a = c.seg_of_row ? __ldcg(c.seg + SEG_N * c.seg_of_row[row] + SG_ALPHA) : alpha;
-            double rr2 = 0.0;
-            axpy_vals(a, pv, qv, xv, rv, rr2);
-            acc += rr2;
-#pragma unroll
-            for(int d = 0; d < 3; d++)
-            {
-                c.x[3 * (size_t)row + d] = xv[d];
-                c.r[3 * (size_t)row + d] = rv[d];
-            }
-            if(c.seg_of_row) c.seg_row[(size_t)c.nrows + row] = rr2;
-            r0 = (float)rv[0];
-            r1 = (float)rv[1];
-            r2 = (float)rv[2];
-            msk = c.fine_mask[v];
-        }
-        float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-#pragma unroll
-        for(int bb = 0; bb < 16; bb++)
-        {
-            const float x0 = group_shfl<16>(r0, bb);
-            const float x1 = group_shfl<16>(r1, bb);
-            const float x2 = group_shfl<16>(r2, bb);
-            if(msk & (1u << bb))
-            {
-                a0 += x0;
-                a1 += x1;
-                a2 += x2;
-            }
-        }
-        if(v >= 0 && ok && __popc(msk & lanemask_lt(lane)) == 0)
-            st4(c.R + 4 * (size_t)c.going_next[v], a0, a1, a2);
-        if(lane < 16) rs[lane] = make_float4(r0, r1, r2, 0.f);
-        __syncwarp();
-        // the bank solve: z = P r_0 from the staged inverse
-        float z0, z1, z2;
-        bank16_half(reinterpret_cast<const float*>(cur), rs, lane & 15, lane >> 4, z0, z1, z2);
-        bank16_join(z0, z1, z2);
-        if(lane < 16) st4(c.Z + ((size_t)bk * 16 + lane) * 4, z0, z1, z2);
-        __syncwarp();
-    }
-    if(failed && lane == 0)
-    {
-        atomicExch(c.flags + F_STATUS, 6);  // STG_ERR_TIMEOUT
-        atomicExch(c.flags + F_DONE, 1);
-    }
-    // the ABD range: plain axpy
-    if(ok)
-        for(int i = blockIdx.x * BD_THREADS + threadIdx.x; i < c.abd_bodies * 4; i += gridDim.x * BD_THREADS)
-        {
-            double d0, d1, d2;
-            axpy_row<T>(c, pn, q, alpha, i, d0, d1, d2, acc);
-        }
-    finish_reduction<BD_THREADS>(c, acc, SITE_B, POST_CHECK_PQ, 0, pq, rz);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 
 // ---------------------------------------------------------------------------------------
@@ -988,6 +870,43 @@ constexpr int A_THREADS = (A_CW + 1) * 32;
 // default for each precision is the first of its candidates; the autotuner may pick the
 // other (Solver::spmv_rt).
 template <typename T> constexpr int a_rt_default() { return sizeof(T) == 4 ? 64 : 32; }
+constexpr int SPMV_HALO = -2;  // stg_spmv_tiles value selecting the halo kernel
+
+// The autotuner's choices, one per shape class (precision, block rows, unique blocks) for
+// the whole process: the first handle that meets a class times the candidates, every later
+// solve of that class reuses the choice, so results stay reproducible within the process.
+struct TuneKey
+{
+    int prec, nrows, nnzb;
+    bool operator<(const TuneKey& o) const
+    {
+        return prec != o.prec ? prec < o.prec : (nrows != o.nrows ? nrows < o.nrows : nnzb < o.nnzb);
+    }
+};
+struct TuneVal
+{
+    int pick;
+    float us[3];
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, TuneVal> g_tune;
+
+static bool tuned_choice(int prec, int nrows, int nnzb, int* pick, float* us)
+{
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    const auto it = g_tune.find(TuneKey{prec, nrows, nnzb});
+    if(it == g_tune.end()) return false;
+    *pick = it->second.pick;
+    for(int i = 0; i < 3; i++) us[i] = it->second.us[i];
+    return true;
+}
+
+static void record_choice(int prec, int nrows, int nnzb, int pick, const float* us)
+{
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    TuneVal v{pick, {us[0], us[1], us[2]}};
+    g_tune[TuneKey{prec, nrows, nnzb}] = v;
+}
 template <typename T> constexpr int a_rt_alt() { return sizeof(T) == 4 ? 32 : 16; }
 
 template <typename T, int RT_ = a_rt_default<T>()>
@@ -1317,6 +1236,406 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T, RTT>::MIN_CTAS) k_phase_a_
     if(threadIdx.x == 0) c.partials[(size_t)SITE_A * c.slots + blockIdx.x] = bs;
 }
 
+// ---------------------------------------------------------------------------------------
+// A with a staged halo: the SpMV phase with every operand in shared memory.  Rows are cut
+// into fixed tiles of RT rows (tile t: [RT t, RT t + RT)), and CTA b takes the contiguous
+// tiles [b T / G, (b + 1) T / G).  Preparation (k_tile_halo) lists, per tile, the distinct
+// columns its entries read outside the tile (the halo: about a quarter of the entries on a
+// Morton-ordered mesh) and rewrites each entry's column as a slot of the tile's operand
+// window: col - r0 for a column inside the tile, RT + its rank in the halo list otherwise.
+// The producer warp fills a stage per tile: its lanes copy the halo's {z, p} slots with
+// cp.async (16-byte pieces; each lane ties its copies to the stage's mbarrier), then lane 0
+// starts the bulk copies of the tile's matrix planes, row bounds and own rows' {z, p}.  The
+// consumers read blocks and operands from shared memory only: no gather waits on L2.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+struct AHalo
+{
+    using FP = FullPlanes<T>;
+    static constexpr int RT = sizeof(T) == 4 ? 64 : 32;           // rows per tile
+    static constexpr int LPR = 32 * A_CW / RT;                     // consumer lanes per row
+    static constexpr int CAP = sizeof(T) == 4 ? 1024 : 512;        // entries per stage (even)
+    static constexpr int HCAP = sizeof(T) == 4 ? 320 : 192;        // halo slots per tile
+    static constexpr int SLOT = 8 * (int)sizeof(T);                // {z0 z1 z2 -, p0 p1 p2 -}
+    static constexpr int TAIL = FP::TAIL;
+    static constexpr int FROW = 4 * (RT + 4);                      // frow[r0 .. r0 + RT + 4)
+    static constexpr int HALO = (RT + HCAP) * SLOT;                // own rows, then the halo
+    static constexpr int PLANES = CAP * FP::ES;
+    static constexpr int STAGE = PLANES + FROW + HALO;             // 16-byte multiple
+    static constexpr int STAGES = 2;
+    static constexpr int META = 16 * STAGES;
+    static constexpr int SMEM = STAGES * STAGE + META + 16 * STAGES;
+    static constexpr int MAXE = 2048;                              // entries per tile the preparation sorts
+};
+
+// Preparation, one CTA per tile: the tile's sorted halo (hcnt[t], hlist[t * HCAP ..]) and
+// the slot-tail plane {h8, slot} that replaces {h8, col} for the halo kernel.  A tile with
+// more than CAP entries or HCAP halo columns counts in *bad (the solve keeps the plain tiled
+// kernel then).
+template <typename T>
+__global__ void __launch_bounds__(256) k_tile_halo(const int* __restrict__ frow, const unsigned char* __restrict__ fent,
+                                                   size_t S, int nrows, int* hcnt, int* hlist, unsigned char* htail,
+                                                   int* bad)
+{
+    using G = AHalo<T>;
+    constexpr int RT = G::RT, MAXE = G::MAXE, PER = MAXE / 256;
+    __shared__ int key[MAXE];
+    __shared__ int uniq[MAXE];
+    __shared__ int wsum[8];
+    __shared__ int total;
+    const int t = blockIdx.x, tid = threadIdx.x;
+    const int r0 = t * RT, r1 = min(r0 + RT, nrows);
+    const int F0 = frow[r0], n = frow[r1] - F0;
+    if(n + 2 > G::CAP || n > MAXE)  // a stage's copy starts at an even entry: up to n + 2
+    {
+        if(tid == 0)
+        {
+            atomicAdd(bad, 1);
+            hcnt[t] = 0;
+        }
+        return;
+    }
+    const unsigned char* tail = fent + (size_t)16 * FullPlanes<T>::NP * S;  // {h8, col} plane
+    auto col_of = [&](int f) -> int {
+        return sizeof(T) == 4 ? reinterpret_cast<const int*>(tail)[2 * (size_t)f + 1]
+                              : (int)reinterpret_cast<const long long*>(tail)[2 * (size_t)f + 1];
+    };
+    int P = 1;
+    while(P < n) P <<= 1;
+    for(int i = tid; i < MAXE; i += 256)
+    {
+        int k = 0x7fffffff;
+        if(i < n)
+        {
+            const int cc = col_of(F0 + i);
+            if(cc < r0 || cc >= r1) k = cc;
+        }
+        key[i] = k;
+    }
+    __syncthreads();
+    // bitonic sort of key[0, P)
+    for(int k = 2; k <= P; k <<= 1)
+        for(int j = k >> 1; j > 0; j >>= 1)
+        {
+            for(int i = tid; i < P; i += 256)
+            {
+                const int ixj = i ^ j;
+                if(ixj > i)
+                {
+                    const int a = key[i], b = key[ixj];
+                    if(((i & k) == 0) == (a > b))
+                    {
+                        key[i] = b;
+                        key[ixj] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    // distinct keys, in order: thread tid owns key[PER tid, PER tid + PER)
+    int cnt = 0;
+#pragma unroll
+    for(int u = 0; u < PER; u++)
+    {
+        const int i = PER * tid + u;
+        cnt += (i < P && key[i] != 0x7fffffff && (i == 0 || key[i] != key[i - 1])) ? 1 : 0;
+    }
+    const int lane = tid & 31, w = tid >> 5;
+    int incl = cnt;
+#pragma unroll
+    for(int o = 1; o < 32; o <<= 1)
+    {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if(lane >= o) incl += y;
+    }
+    if(lane == 31) wsum[w] = incl;
+    __syncthreads();
+    int before = 0;
+    for(int u = 0; u < w; u++) before += wsum[u];
+    if(tid == 255) total = before + incl;
+    int pos = before + incl - cnt;
+#pragma unroll
+    for(int u = 0; u < PER; u++)
+    {
+        const int i = PER * tid + u;
+        if(i < P && key[i] != 0x7fffffff && (i == 0 || key[i] != key[i - 1])) uniq[pos++] = key[i];
+    }
+    __syncthreads();
+    const int H = total;
+    if(H > G::HCAP)
+    {
+        if(tid == 0)
+        {
+            atomicAdd(bad, 1);
+            hcnt[t] = 0;
+        }
+        return;
+    }
+    if(tid == 0) hcnt[t] = H;
+    for(int i = tid; i < H; i += 256) hlist[(size_t)t * G::HCAP + i] = uniq[i];
+    for(int e = tid; e < n; e += 256)
+    {
+        const size_t f = (size_t)F0 + e;
+        const int cc = col_of((int)f);
+        int slot;
+        if(cc >= r0 && cc < r1)
+            slot = cc - r0;
+        else
+        {
+            int lo = 0, hi = H;  // first uniq >= cc
+            while(lo < hi)
+            {
+                const int mid = (lo + hi) >> 1;
+                if(uniq[mid] < cc)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            slot = RT + lo;
+        }
+        if(sizeof(T) == 4)
+        {
+            const float2 v = reinterpret_cast<const float2*>(tail)[f];
+            reinterpret_cast<float2*>(htail)[f] = make_float2(v.x, __int_as_float(slot));
+        }
+        else
+        {
+            const double2 v = reinterpret_cast<const double2*>(tail)[f];
+            reinterpret_cast<double2*>(htail)[f] = make_double2(v.x, __longlong_as_double((long long)slot));
+        }
+    }
+}
+
+// Producer of the halo kernel: fills stage k % STAGES with tile tb + k.  Lane 0 starts the
+// tile's bulk copies (planes, row bounds, own rows' {z, p}); every lane copies its share of
+// the halo with cp.async and arrives (.noinc) on the stage's barrier, which expects lane 0
+// plus the 32 lanes.  hc: the halo sizes of the 32 tiles from k & ~31 on, one per lane.
+template <typename T>
+__device__ __forceinline__ void halo_issue(const PcgDev& c, unsigned char* hsm_, int* meta, unsigned bar_full,
+                                           const T* zp, int tb, int k, int hc, int lane)
+{
+    using G = AHalo<T>;
+    using FP = FullPlanes<T>;
+    constexpr int RT = G::RT, CAP = G::CAP;
+    const int s = k % G::STAGES, t = tb + k;
+    const int r0 = t * RT, r1 = min(r0 + RT, c.nrows);
+    unsigned char* st = hsm_ + (size_t)s * G::STAGE;
+    const unsigned bf = bar_full + 8 * s;
+    if(lane == 0)
+    {
+        const int F0 = __ldg(c.frow + r0), F1 = __ldg(c.frow + r1);
+        const int F0a = F0 & ~1, n2 = ((F1 + 1) & ~1) - F0a;
+        meta[4 * s] = F0a;
+        const unsigned own = (unsigned)((r1 - r0) * G::SLOT);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(bf, (unsigned)(n2 * FP::ES + G::FROW) + own);
+#pragma unroll 1
+        for(int pl = 0; pl < FP::NP; pl++)
+            tma_load_1d(st + (size_t)16 * pl * CAP, c.fent + 16 * (pl * c.fstride + F0a), (unsigned)(16 * n2), bf);
+        tma_load_1d(st + (size_t)16 * FP::NP * CAP, c.htail + (size_t)FP::TAIL * F0a, (unsigned)(FP::TAIL * n2), bf);
+        tma_load_1d(st + G::PLANES, c.frow + r0, G::FROW, bf);
+        tma_load_1d(st + G::PLANES + G::FROW, zp + 8 * (size_t)r0, own, bf);
+    }
+    // the halo: {z, p} slots of the tile's outside columns; a lane's column ids are loaded
+    // together before its copies are issued
+    const int H = __shfl_sync(0xffffffffu, hc, k % 32);
+    const int* hl = c.hlist + (size_t)t * G::HCAP;
+    unsigned char* hs = st + G::PLANES + G::FROW + (size_t)RT * G::SLOT;
+    constexpr int PER = (G::HCAP + 31) / 32;
+    int cols[PER];
+#pragma unroll
+    for(int u = 0; u < PER; u++) cols[u] = lane + 32 * u < H ? __ldg(hl + lane + 32 * u) : -1;
+#pragma unroll
+    for(int u = 0; u < PER; u++)
+        if(cols[u] >= 0)
+        {
+            const unsigned char* src = reinterpret_cast<const unsigned char*>(zp + 8 * (size_t)cols[u]);
+            unsigned char* dst = hs + (size_t)(lane + 32 * u) * G::SLOT;
+#pragma unroll
+            for(int pc = 0; pc < G::SLOT / 16; pc++) cp_async16(dst + 16 * pc, src + 16 * pc);
+        }
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bf) : "memory");
+}
+
+template <typename T>
+__global__ void __launch_bounds__(A_THREADS, 2) k_phase_a_halo(PcgDev c)
+{
+    using G = AHalo<T>;
+    constexpr int RT = G::RT, LPR = G::LPR, CAP = G::CAP;
+    extern __shared__ __align__(128) unsigned char hsm_[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntiles = (c.nrows + RT - 1) / RT;
+    const int tb = (int)((long long)blockIdx.x * ntiles / gridDim.x);
+    const int te = (int)((long long)(blockIdx.x + 1) * ntiles / gridDim.x);
+    const int mine = te - tb;
+    const int done = __ldcg(c.flags + F_DONE);
+    const double s_iter = __ldcg(c.scal + SS_ITER), rz_old = __ldcg(c.scal + SS_RZ);
+    if(done) return;
+    int* meta = reinterpret_cast<int*>(hsm_ + G::STAGES * G::STAGE);
+    const unsigned sbase = smem_u32(hsm_);
+    const unsigned bar_full = smem_u32(hsm_ + G::STAGES * G::STAGE + G::META);
+    const unsigned bar_empty = bar_full + 8 * G::STAGES;
+    if(threadIdx.x == 0)
+    {
+        for(int s = 0; s < G::STAGES; s++)
+        {
+            mbar_init(bar_full + 8 * s, 33);  // lane 0's expect_tx arrival + one per producer lane
+            mbar_init(bar_empty + 8 * s, A_CW);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const int par = ((long)s_iter) & 1;
+    const T* zp = zpbuf<T>(c, par);
+    T* zpn = zpbuf<T>(c, par ^ 1);
+    T* q = reinterpret_cast<T*>(c.q);
+    // the first stages need nothing of beta: the producer starts them before the reduction
+    int hc = 0;
+    if(warp == A_CW)
+    {
+        hc = lane < mine ? __ldg(c.hcnt + tb + lane) : 0;
+        for(int k = 0; k < min(G::STAGES, mine); k++) halo_issue<T>(c, hsm_, meta, bar_full, zp, tb, k, hc, lane);
+    }
+    // beta = rz_k / rz_(k-1) (flexible PCG: r_k.(z_k - z_(k-1)) / r_(k-1).z_(k-1)); 0 at first
+    double rz_new, rz_mix = 0.0;
+    if(c.flex && (long)s_iter > 0)
+        consume_sum2<A_THREADS>(c, SITE_E, c.grid_e, SITE_F, c.grid_e, rz_new, rz_mix);
+    else
+        rz_new = consume_sum<A_THREADS>(c, SITE_E, c.grid_e);
+    const double s_beta = (long)s_iter == 0 ? 0.0 : (rz_new - rz_mix) / rz_old;
+    const T beta = (T)s_beta;
+    double acc = 0;
+    bool failed = false;
+
+    if(warp == A_CW)
+    {
+        // ---- producer warp: the remaining tiles, each once its stage is released ----
+        int issued = min(G::STAGES, mine);
+        for(int k = G::STAGES; k < mine && !failed; k++)
+        {
+            if(k % 32 == 0) hc = k + lane < mine ? __ldg(c.hcnt + tb + k + lane) : 0;
+            const int s = k % G::STAGES;
+            bool ok = true;
+            if(lane == 0) ok = mbar_wait(bar_empty + 8 * s, ((k / G::STAGES) - 1) & 1);
+            failed = __shfl_sync(0xffffffffu, ok ? 0 : 1, 0) != 0;
+            if(failed) break;
+            halo_issue<T>(c, hsm_, meta, bar_full, zp, tb, k, hc, lane);
+            issued = k + 1;
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        if(lane == 0)
+        {
+            if(failed)
+            {
+                atomicExch(c.flags + F_STATUS, 6);  // STG_ERR_TIMEOUT
+                atomicExch(c.flags + F_DONE, 1);
+            }
+            // drain: every issued stage's copies must have landed before the CTA exits
+            for(int k = max(0, issued - G::STAGES); k < issued; k++)
+                mbar_wait(bar_full + 8 * (k % G::STAGES), (k / G::STAGES) & 1);
+        }
+    }
+    else
+    {
+        // ---- consumer warps: LPR lanes per row, lane `sub` sums the row's entries sub,
+        //      sub + LPR, ... in order, four at a time; operands from the stage's window ----
+        const int sub = lane & (LPR - 1);
+        const int rloc = warp * (32 / LPR) + lane / LPR;
+        for(int k = 0; k < mine; k++)
+        {
+            const int s = k % G::STAGES, t = tb + k;
+            const int r0 = t * RT, r1 = min(r0 + RT, c.nrows);
+            const int i = r0 + rloc;
+            if(!__all_sync(0xffffffffu, mbar_wait(bar_full + 8 * s, (k / G::STAGES) & 1)))
+            {
+                failed = true;
+                break;
+            }
+            const unsigned sb = sbase + (unsigned)(s * G::STAGE);
+            const unsigned sfrow = sb + G::PLANES;
+            const T* win = reinterpret_cast<const T*>(hsm_ + (size_t)s * G::STAGE + G::PLANES + G::FROW);
+            const int F0a = meta[4 * s];
+            int f = 0, d = 0;
+            if(i < r1)
+            {
+                const int x0 = lds_s32(sfrow + 4 * rloc), x1 = lds_s32(sfrow + 4 * rloc + 4);
+                f = x0 - F0a;
+                d = x1 - x0;
+            }
+            const T bta = (c.seg_of_row && i < r1) ? (T)__ldcg(c.seg + SEG_N * c.seg_of_row[i] + SG_BETA) : beta;
+            T y0 = T(0), y1 = T(0), y2 = T(0);
+            for(int e0 = sub; e0 < d; e0 += 4 * LPR)
+            {
+                T h8[4];
+                int sl[4];
+#pragma unroll
+                for(int u = 0; u < 4; u++)
+                {
+                    h8[u] = T(0);
+                    sl[u] = 0;
+                    if(e0 + u * LPR < d) lds_tail<CAP>(sb, f + e0 + u * LPR, h8[u], sl[u]);
+                }
+#pragma unroll
+                for(int u = 0; u < 4; u++)
+                {
+                    const int e = e0 + u * LPR;
+                    if(e < d)
+                    {
+                        const T* w = win + 8 * sl[u];
+                        T x0, x1, x2, p0, p1, p2;
+                        ld4(w, x0, x1, x2);
+                        ld4(w + 4, p0, p1, p2);
+                        x0 += bta * p0;
+                        x1 += bta * p1;
+                        x2 += bta * p2;
+                        T h[9];
+                        lds_main<CAP>(sb, f + e, h);
+                        h[8] = h8[u];
+                        mv3<T>(h, false, x0, x1, x2, y0, y1, y2);
+                    }
+                }
+            }
+            T p0 = T(0), p1 = T(0), p2 = T(0);
+            if(sub == 0 && i < r1)
+            {
+                const T* w = win + 8 * rloc;
+                T z0, z1, z2, o0, o1, o2;
+                ld4(w, z0, z1, z2);
+                ld4(w + 4, o0, o1, o2);
+                p0 = z0 + bta * o0;
+                p1 = z1 + bta * o1;
+                p2 = z2 + bta * o2;
+            }
+            __syncwarp();
+            if(lane == 0) mbar_arrive(bar_empty + 8 * s);
+#pragma unroll
+            for(int o = LPR / 2; o > 0; o >>= 1)
+            {
+                y0 += __shfl_xor_sync(0xffffffffu, y0, o);
+                y1 += __shfl_xor_sync(0xffffffffu, y1, o);
+                y2 += __shfl_xor_sync(0xffffffffu, y2, o);
+            }
+            if(sub == 0 && i < r1)
+            {
+                st4(zpn + 8 * (size_t)i + 4, p0, p1, p2);
+                st4(q + 4 * (size_t)i, y0, y1, y2);
+                const double pq = (double)p0 * (double)y0 + (double)p1 * (double)y1 + (double)p2 * (double)y2;
+                acc += pq;
+                if(c.seg_of_row) c.seg_row[i] = pq;
+            }
+        }
+        if(failed && lane == 0)
+        {
+            atomicExch(c.flags + F_STATUS, 6);  // STG_ERR_TIMEOUT
+            atomicExch(c.flags + F_DONE, 1);
+        }
+    }
+    // p.q: this CTA's partial only; phase B finishes the sum (consume_sum)
+    __shared__ double red[A_THREADS / 32];
+    const double bs = block_sum<A_THREADS>(acc, red);
+    if(threadIdx.x == 0) c.partials[(size_t)SITE_A * c.slots + blockIdx.x] = bs;
+}
+
 // E (MAS): z = sum over levels (FP32) on the FEM range + ABD block-Jacobi; share of r.z
 // ABD 12x12 block-Jacobi (abd_preconditioner.cu:20-38): one thread per dof of the first
 // 12 * bodies dofs, z written into the zp slots; returns the share of r.z
@@ -1428,16 +1747,20 @@ __global__ void __launch_bounds__(PB) k_phase_a(PcgDev c)
 }
 
 template <typename T, int B>
-__global__ void __launch_bounds__(PB, 8) k_phase_b(PcgDev c)
+__global__ void __launch_bounds__(PB, 4) k_phase_b(PcgDev c)
 {
     if(c.flags[F_DONE]) return;
+    // the first slot's loads do not depend on alpha: issue them before the reductions
+    BSlot<T> first;
+    if(B > 0)
+        b_load<T>(c, zpbuf<T>(c, iter_parity(c) ^ 1), reinterpret_cast<const T*>(c.q), GT, first);
     double pq, rz;
     consume_sum2<PB>(c, SITE_A, c.grid_a, SITE_E, c.grid_e, pq, rz);
     double v = 0;
     if(pq > 0.0 && isfinite(pq))  // else breakdown: no update; the last CTA reports it
     {
         const double alpha = rz / pq;
-        v = B > 0 ? phase_b_mas<T, (B > 0 ? B : 16)>(c, GT, GN, alpha) : phase_b_plain<T>(c, GT, GN, alpha);
+        v = B > 0 ? phase_b_mas<T, (B > 0 ? B : 16)>(c, GT, GN, alpha, first, true) : phase_b_plain<T>(c, GT, GN, alpha);
     }
     finish_reduction(c, v, SITE_B, POST_CHECK_PQ, 0, pq, rz);
 }
@@ -1473,7 +1796,7 @@ template <int B>
 __global__ void __launch_bounds__(PB) k_phase_c1(PcgDev c)
 {
     if(c.flags[F_DONE]) return;
-    phase_c<B>(c, 1, 2, GT, GN, false);
+    if(c.L > 2) restrict_level<B>(c, c.ls[2], c.ls[3], GT, GN);  // level 1's (count, begin)
 }
 
 // C2: levels 2 -> 3 -> ... (small) by one CTA.  All nodes of the levels >= 2 (contiguous
@@ -1489,8 +1812,17 @@ template <int B>
 __global__ void __launch_bounds__(1024) k_phase_c2(PcgDev c)
 {
     if(c.flags[F_DONE]) return;
-    const int b2 = __ldg(c.ls_dev + 5);                   // first level-2 node
-    const int total = __ldg(c.ls_dev + 2 * (c.L - 1) + 1) + __ldg(c.ls_dev + 2 * (c.L - 1)) - b2;
+    // level sizes from the parameter block (unrolled constant indices: no dependent loads)
+    int last_n = 0, last_b = 0;
+#pragma unroll
+    for(int l = 0; l <= kMaxLevelsDev; l++)
+        if(l == c.L - 1)
+        {
+            last_n = c.ls[2 * l];
+            last_b = c.ls[2 * l + 1];
+        }
+    const int b2 = c.ls[5];  // first level-2 node
+    const int total = last_b + last_n - b2;
     if(total > C2_SMEM_NODES)
     {
         phase_c<B>(c, 2, c.L - 1, threadIdx.x, blockDim.x, true);
@@ -1500,7 +1832,7 @@ __global__ void __launch_bounds__(1024) k_phase_c2(PcgDev c)
     float4* rv = c2_smem;
     unsigned* cm = reinterpret_cast<unsigned*>(rv + C2_SMEM_NODES);
     int* par = reinterpret_cast<int*>(cm + C2_SMEM_NODES);
-    const int n2 = __ldg(c.ls_dev + 4);
+    const int n2 = c.ls[4];
     for(int i = threadIdx.x; i < total; i += 1024)
     {
         rv[i] = i < n2 ? *reinterpret_cast<const float4*>(c.R + 4 * (size_t)(b2 + i)) : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1510,7 +1842,14 @@ __global__ void __launch_bounds__(1024) k_phase_c2(PcgDev c)
     __syncthreads();
     for(int level = 2; level < c.L - 1; level++)
     {
-        const int number = __ldg(c.ls_dev + 2 * level), begin = __ldg(c.ls_dev + 2 * level + 1) - b2;
+        int number = 0, begin = 0;
+#pragma unroll
+        for(int l = 0; l < kMaxLevelsDev; l++)
+            if(l == level)
+            {
+                number = c.ls[2 * l];
+                begin = c.ls[2 * l + 1] - b2;
+            }
         const int span = (number + 31) / 32 * 32;
         for(int i = threadIdx.x; i < span; i += 1024)
         {
@@ -1758,7 +2097,8 @@ __global__ void __launch_bounds__(PB) k_pcg_persistent(PcgDev c)
         grid_barrier(c, phase_a<T>(c, gt, gn), SITE_A, POST_ALPHA, gen);
         if(is_done(c)) break;
         const double alpha = __ldcg(c.scal + SS_ALPHA);
-        const double vb = B > 0 ? phase_b_mas<T, BB>(c, gt, gn, alpha) : phase_b_plain<T>(c, gt, gn, alpha);
+        BSlot<T> none;
+        const double vb = B > 0 ? phase_b_mas<T, BB>(c, gt, gn, alpha, none, false) : phase_b_plain<T>(c, gt, gn, alpha);
         grid_barrier(c, vb, SITE_B, POST_CHECK, gen);
         if(is_done(c)) break;
         const long k = (long)__ldcg(c.scal + SS_ITER);
@@ -1904,6 +2244,32 @@ int pack_blocks(Solver& S)
     }
     STG_LAUNCH_CHECK();
     S.launches += 2;
+    // operand windows of the halo SpMV phase (one CTA per tile), when that kernel may run
+    A.halo_ok = false;
+    if(S.spmv_rt == SPMV_HALO || S.spmv_tune)
+    {
+        const int rt = fp32 ? AHalo<float>::RT : AHalo<double>::RT;
+        const int hcap = fp32 ? AHalo<float>::HCAP : AHalo<double>::HCAP;
+        const int tiles = div_up(A.nrows, rt);
+        STG_TRY(A.hcnt.resize(tiles));
+        STG_TRY(A.hlist.resize((size_t)tiles * hcap));
+        STG_TRY(A.htail.resize(A.fstride * (size_t)FullPlanes<double>::TAIL));
+        STG_TRY(S.cv.scratch.resize(4));
+        int* bad = S.cv.scratch.data() + 3;
+        STG_CUDA_TRY(cudaMemsetAsync(bad, 0, sizeof(int), S.stream));
+        if(fp32)
+            k_tile_halo<float><<<tiles, 256, 0, S.stream>>>(A.frow.data(), A.fent.data(), A.fstride, A.nrows,
+                                                            A.hcnt.data(), A.hlist.data(), A.htail.data(), bad);
+        else
+            k_tile_halo<double><<<tiles, 256, 0, S.stream>>>(A.frow.data(), A.fent.data(), A.fstride, A.nrows,
+                                                             A.hcnt.data(), A.hlist.data(), A.htail.data(), bad);
+        STG_LAUNCH_CHECK();
+        S.launches++;
+        int h = 0;
+        STG_CUDA_TRY(cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, S.stream));
+        STG_CUDA_TRY(cudaStreamSynchronize(S.stream));
+        A.halo_ok = h == 0;
+    }
     return 0;
 }
 
@@ -1966,31 +2332,9 @@ static int launch_d16(Solver& S, const PcgDev& c, int b0, int b1, int guarded)
     return 0;
 }
 
-// phase B fused with the level-0 bank solves (16-banks): one resident wave of CTAs
-template <typename T>
-static int launch_bd16(Solver& S, const PcgDev& c)
-{
-    const int smem = BD_WARPS * BdStage<T>::WARP;
-    static thread_local unsigned long long attr_done = 0;
-    if(first_on_device(attr_done))
-    {
-        STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_bd16<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_bd16<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                          cudaSharedmemCarveoutMaxShared));
-    }
-    int per_sm = 0;
-    STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase_bd16<T>, BD_THREADS, smem));
-    const int grid = std::max(1, std::min(div_up(c.M / 16, BD_WARPS), std::max(per_sm, 1) * kSMs));
-    k_phase_bd16<T><<<grid, BD_THREADS, smem, S.stream>>>(c);
-    STG_LAUNCH_CHECK();
-    S.launches++;
-    return 0;
-}
-
-// Restriction of the coarse levels and the bank solves of banks [d_from, nbanks) (d_from =
-// M / 16 when phase B has solved level 0 already).
+// Restriction of the coarse levels and the bank solves of every level.
 template <int B>
-static int launch_mas_cd(Solver& S, const PcgDev& c, int d_from = 0)
+static int launch_mas_cd(Solver& S, const PcgDev& c)
 {
     cudaStream_t s = S.stream;
     if(c.L > 2)
@@ -2006,7 +2350,7 @@ static int launch_mas_cd(Solver& S, const PcgDev& c, int d_from = 0)
         STG_LAUNCH_CHECK();
         S.launches++;
     }
-    if(B == 16) return launch_d16(S, c, d_from, c.nbanks, 0);
+    if(B == 16) return launch_d16(S, c, 0, c.nbanks, 0);
     k_phase_d<B><<<std::max(1, std::min(c.nbanks, kSMs * 8)), PB, 0, s>>>(c);
     STG_LAUNCH_CHECK();
     S.launches++;
@@ -2036,9 +2380,30 @@ static int phase_a_grid_rt(int nrows, int* grid)
     return 0;
 }
 
+// the halo SpMV phase: one resident wave of CTAs over the fixed tiles
 template <typename T>
-static int phase_a_grid(int nrows, int rt, int* grid)
+static int phase_a_grid_halo(int nrows, int* grid)
 {
+    static thread_local unsigned long long seen = 0;
+    static thread_local int per_sm_dev[64];
+    int dev = 0;
+    STG_CUDA_TRY(cudaGetDevice(&dev));
+    int& per_sm = per_sm_dev[dev & 63];
+    if(first_on_device(seen))
+    {
+        STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_a_halo<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, AHalo<T>::SMEM));
+        STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_a_halo<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          cudaSharedmemCarveoutMaxShared));
+        STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase_a_halo<T>, A_THREADS, AHalo<T>::SMEM));
+    }
+    *grid = std::max(1, std::min(div_up(nrows, AHalo<T>::RT), std::max(per_sm, 1) * kSMs));
+    return 0;
+}
+
+template <typename T>
+static int phase_a_grid(int nrows, int rt, int* grid, bool halo = false)
+{
+    if(halo) return phase_a_grid_halo<T>(nrows, grid);
     if(rt == a_rt_alt<T>()) return phase_a_grid_rt<T, a_rt_alt<T>()>(nrows, grid);
     return phase_a_grid_rt<T, a_rt_default<T>()>(nrows, grid);
 }
@@ -2047,13 +2412,15 @@ template <typename T>
 static int launch_phase_a(const PcgDev& c, cudaStream_t s)
 {
     int grid = 0;
-    STG_TRY(phase_a_grid<T>(c.nrows, c.a_rt, &grid));
+    STG_TRY(phase_a_grid<T>(c.nrows, c.a_rt, &grid, c.halo != 0));
     if(grid != c.grid_a)
     {
         set_error("SpMV phase grid differs from the one phase B sums over");
         return STG_ERR_INVALID;
     }
-    if(c.a_rt == a_rt_alt<T>())
+    if(c.halo)
+        k_phase_a_halo<T><<<grid, A_THREADS, AHalo<T>::SMEM, s>>>(c);
+    else if(c.a_rt == a_rt_alt<T>())
         k_phase_a_tiled<T, a_rt_alt<T>()><<<grid, A_THREADS, ATile<T, a_rt_alt<T>()>::SMEM, s>>>(c);
     else
         k_phase_a_tiled<T, a_rt_default<T>()><<<grid, A_THREADS, ATile<T>::SMEM, s>>>(c);
@@ -2061,18 +2428,23 @@ static int launch_phase_a(const PcgDev& c, cudaStream_t s)
     return 0;
 }
 
-// BCOO tile autotuner: every candidate tile shape of the SpMV phase launched on this system
-// (3 untimed, then `reps` timed with CUDA events); returns the fastest shape and each mean
+// BCOO tile autotuner: every candidate of the SpMV phase launched on this system (3 untimed,
+// then `reps` timed with CUDA events): the two tile shapes of the tiled kernel and, when its
+// operand windows fit (halo_ok), the halo kernel.  Returns the fastest (its rows per tile, or
+// SPMV_HALO) and each mean.
 template <typename T>
 static int tune_phase_a(Solver& S, PcgDev c, float* us, int* out)
 {
-    const int cand[2] = {a_rt_default<T>(), a_rt_alt<T>()};
+    const int cand[3] = {a_rt_default<T>(), a_rt_alt<T>(), SPMV_HALO};
+    const int ncand = S.bcoo.halo_ok ? 3 : 2;
+    us[2] = 0.f;
     float best = 0.f;
     int pick = cand[0];
-    for(int v = 0; v < 2; v++)
+    for(int v = 0; v < ncand; v++)
     {
-        c.a_rt = cand[v];
-        STG_TRY(phase_a_grid<T>(c.nrows, c.a_rt, &c.grid_a));
+        c.halo = cand[v] == SPMV_HALO ? 1 : 0;
+        c.a_rt = c.halo ? a_rt_default<T>() : cand[v];
+        STG_TRY(phase_a_grid<T>(c.nrows, c.a_rt, &c.grid_a, c.halo != 0));
         for(int i = 0; i < 3; i++) STG_TRY(launch_phase_a<T>(c, S.stream));
         const int reps = 10;
         STG_CUDA_TRY(cudaEventRecord(S.ev[4], S.stream));
@@ -2130,18 +2502,9 @@ static int launch_iteration(Solver& S, const PcgDev& c, int grid_vec, int grid_r
         STG_LAUNCH_CHECK();
         S.launches++;
     }
-    if(B == 16)
-    {
-        // B fused with the level-0 bank solves
-        STG_TRY(launch_bd16<T>(S, c));
-        S.launches++;
-    }
-    else
-    {
-        k_phase_b<T, B><<<B > 0 ? std::max(1, std::min(div_up(c.M, PB), kSMs * 4)) : grid_vec, PB, 0, s>>>(c);
-        STG_LAUNCH_CHECK();
-        S.launches += 2;
-    }
+    k_phase_b<T, B><<<B > 0 ? std::max(1, std::min(div_up(c.M, PB), kSMs * 4)) : grid_vec, PB, 0, s>>>(c);
+    STG_LAUNCH_CHECK();
+    S.launches += 2;
     if(c.seg_of_row)
     {
         k_seg<SEG_B><<<c.nseg, PB, 0, s>>>(c);
@@ -2180,11 +2543,9 @@ static int launch_iteration(Solver& S, const PcgDev& c, int grid_vec, int grid_r
                 STG_LAUNCH_CHECK();
                 S.launches++;
             }
-            // the fused B solved level 0 before the replacement: solve it again
-            if(B == 16) STG_TRY(launch_d16(S, c, 0, c.M / 16, 1));
         }
     }
-    if(B > 0) STG_TRY(launch_mas_cd<(B > 0 ? B : 16)>(S, c, B == 16 ? c.M / 16 : 0));
+    if(B > 0) STG_TRY(launch_mas_cd<(B > 0 ? B : 16)>(S, c));
     if(c.net_mode) STG_TRY(launch_learned(S, c));
     k_phase_e<T, B><<<grid_vec, PB, 0, s>>>(c, POST_BETA);
     STG_LAUNCH_CHECK();
@@ -2210,13 +2571,11 @@ static int record_if_body(Solver& S, const PcgDev& c, int grid_rows, cudaGraph_t
         k_restrict01<(B > 0 ? B : 16)><<<std::max(1, std::min(div_up(c.M, PB), kSMs * 4)), PB, 0, s>>>(c, 0);
         e1 = cudaGetLastError();
     }
-    int rc = 0;
-    if(B == 16 && e1 == cudaSuccess) rc = launch_d16(S, c, 0, c.M / 16, 0);
     cudaGraph_t out = body;
     cudaError_t e2 = cudaStreamEndCapture(s, &out);
     STG_CUDA_TRY(e1);
     STG_CUDA_TRY(e2);
-    return rc;
+    return 0;
 }
 
 // Every kernel of the iteration asks for the same shared-memory carveout (the largest), so
@@ -2246,7 +2605,7 @@ template <typename T, int B>
 static int pcg_run(Solver& S, PcgDev& c, int& h_done)
 {
     STG_TRY((set_carveouts<T, B>()));
-    STG_TRY(phase_a_grid<T>(c.nrows, c.a_rt, &c.grid_a));
+    STG_TRY(phase_a_grid<T>(c.nrows, c.a_rt, &c.grid_a, c.halo != 0));
     c.grid_e = std::max(1, std::min(div_up(c.n, PB), kSMs * 4));  // grid_vec below
     if(c.grid_a > c.slots || c.grid_e > c.slots)
     {
@@ -2548,6 +2907,10 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
     c.fent = bcoo.fent.data();
     c.frow = bcoo.frow.data();
     c.fstride = bcoo.fstride;
+    c.htail = bcoo.htail.data();
+    c.hcnt = bcoo.hcnt.data();
+    c.hlist = bcoo.hlist.data();
+    c.halo = 0;
     c.nrows = bcoo.nrows;
     c.n = n;
     char* vb = reinterpret_cast<char*>(P.vbuf.data());
@@ -2590,24 +2953,36 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
     c.prm.stop_rule = cfg.stop_rule;
     c.prm.refine = fp32 ? cfg.refine_interval : 0;
     c.bar = P.bar.data();
-    // SpMV tile shape: fixed, tuned once per system shape, or the precision's default
+    // SpMV kernel: a fixed tile shape (or the halo kernel), the autotuner's choice for this
+    // shape class (precision, block rows, unique blocks; one choice per class and process), or
+    // the precision's default shape
     c.a_rt = fp32 ? a_rt_default<float>() : a_rt_default<double>();
-    if(spmv_rt > 0)
+    c.halo = 0;
+    if(spmv_rt == SPMV_HALO)
+        c.halo = bcoo.halo_ok ? 1 : 0;
+    else if(spmv_rt > 0)
         c.a_rt = spmv_rt;
     else if(spmv_tune)
     {
         if(tuned_prec != (fp32 ? 1 : 0) || tuned_nrows != bcoo.nrows || tuned_nnzb != bcoo.nnzb)
         {
-            PcgDev t = c;
-            t.grid_e = std::max(1, std::min(div_up(n, PB), kSMs * 4));
             int r = 0;
-            STG_TRY(fp32 ? tune_phase_a<float>(*this, t, tune_us, &r) : tune_phase_a<double>(*this, t, tune_us, &r));
+            if(!tuned_choice(fp32 ? 1 : 0, bcoo.nrows, bcoo.nnzb, &r, tune_us))
+            {
+                PcgDev t = c;
+                t.grid_e = std::max(1, std::min(div_up(n, PB), kSMs * 4));
+                STG_TRY(fp32 ? tune_phase_a<float>(*this, t, tune_us, &r) : tune_phase_a<double>(*this, t, tune_us, &r));
+                record_choice(fp32 ? 1 : 0, bcoo.nrows, bcoo.nnzb, r, tune_us);
+            }
             tuned_rt = r;
             tuned_prec = fp32 ? 1 : 0;
             tuned_nrows = bcoo.nrows;
             tuned_nnzb = bcoo.nnzb;
         }
-        c.a_rt = tuned_rt;
+        if(tuned_rt == SPMV_HALO)
+            c.halo = bcoo.halo_ok ? 1 : 0;
+        else
+            c.a_rt = tuned_rt;
     }
     if(nseg > 0)
     {

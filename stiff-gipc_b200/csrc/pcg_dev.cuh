@@ -22,6 +22,10 @@ struct PcgDev
     const unsigned char* fent;  // full symmetric row-sliced copy in 16-byte planes (phase A)
     const int* frow;          // [nrows+1] first entry of each row in fent
     size_t fstride;           // entries per plane
+    const unsigned char* htail;  // halo SpMV: {h8, slot} plane, per-tile halo columns
+    const int* hcnt;
+    const int* hlist;
+    int halo;                 // the SpMV phase runs the halo kernel
     const double2* blk64;     // FP64 padded upper blocks (residual replacement)
     int nrows, n;
     // vectors in the iteration precision T, one 4-wide (16 B FP32 / 32 B FP64) slot per block

@@ -41,6 +41,10 @@ struct Bcoo
     DBuf<unsigned char> fent;
     DBuf<int> frow;              // [nrows+1] first entry of each row (row_ptr + t_ptr)
     size_t fstride = 0;          // entries per plane
+    // per-tile operand windows of the halo SpMV phase (k_tile_halo / k_phase_a_halo in pcg.cu)
+    DBuf<unsigned char> htail;   // {h8, slot} plane replacing {h8, col}
+    DBuf<int> hcnt, hlist;       // [tiles], [tiles * HCAP] halo columns, sorted
+    bool halo_ok = false;        // every tile fits a stage
     DBuf<double> diag_inv;       // 3x3 block-Jacobi inverses [nrows*9]
     int offdiag = 0;
 
@@ -169,7 +173,7 @@ struct Solver
     int spmv_rt = 0;
     bool spmv_tune = false;
     int tuned_rt = 0, tuned_prec = -1, tuned_nrows = -1, tuned_nnzb = -1;
-    float tune_us[2] = {0.f, 0.f};
+    float tune_us[3] = {0.f, 0.f, 0.f};
 
     ~Solver();
 

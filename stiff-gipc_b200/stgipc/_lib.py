@@ -98,6 +98,7 @@ def lib():
     L.stg_mas_export_matrices.argtypes = [vp, vp, vp, C.POINTER(ci)]
     L.stg_profile_spmv.argtypes = [vp, ci, C.POINTER(C.c_float), C.POINTER(cd)]
     L.stg_spmv_noalloc.argtypes = [cd, vp, vp, vp, ci, vp, cd, vp, ci, vp]
+    L.stg_morton_keys.argtypes = [ci, vp, vp, vp]
     L.stg_selftest_wait_timeout.argtypes = [C.POINTER(ci), C.POINTER(cd)]
     L.stg_spmv_tiles.argtypes = [vp, ci]
     L.stg_set_segments.argtypes = [vp, vp, ci]
@@ -107,7 +108,8 @@ def lib():
                                         C.c_size_t, vp]
     L.stg_fem_energy.argtypes = [ci, vp, vp, vp, ci, vp, vp, cd, cd, cd, ci, vp, vp, C.c_size_t, C.POINTER(cd),
                                  C.POINTER(ci), vp]
-    L.stg_spmv_tiles_info.argtypes = [vp, C.POINTER(ci), C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    L.stg_spmv_tiles_info.argtypes = [vp, C.POINTER(ci), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                      C.POINTER(C.c_float)]
     L.stg_net_configure.argtypes = [vp, ci]
     L.stg_net_graph_info.argtypes = [vp, C.POINTER(ci), C.POINTER(ci)]
     L.stg_net_export_graph.argtypes = [vp, vp, vp, vp, vp, vp, vp]

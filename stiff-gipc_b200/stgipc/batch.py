@@ -203,13 +203,16 @@ class ConcatenatedBatch:
     a bank, but with no edges between them they are never merged and their bank matrix is
     block-diagonal, so the preconditioner never couples scenes.
 
+    spmv_tiles: the SpMV kernel (Solver.spmv_tiles); 0, the default, lets the autotuner time
+    the candidates on the batch's first solve and keep the choice for its shape class.
+
     per_scene=True (stg_set_segments): every scene runs its own recurrence (alpha, beta,
     stop test ||r_s|| <= tol ||b_s||) inside the one loop.  per_scene=False: one recurrence
     with global scalars and the stop test tightened to tol min_s ||b_s|| / ||b||, so that
     ||r_s|| <= ||r|| <= tol min_s ||b_s|| <= tol ||b_s|| for every scene s."""
 
     def __init__(self, systems, config: Optional[PCGSolverConfig] = None, device="cuda", bank: int = 16,
-                 per_scene: bool = True):
+                 per_scene: bool = True, spmv_tiles: int = 0):
         import torch
         self.systems = list(systems)
         self.device = torch.device(device)
@@ -231,6 +234,9 @@ class ConcatenatedBatch:
                              np.concatenate(lists).astype(np.uint32), part_map, real_map)
         if per_scene:
             self.solver.set_segments(self.voff.astype(np.int32))
+        # the SpMV kernel of this batch's shape class: autotuned once per process by default
+        # (stg_spmv_tiles: 0), or fixed
+        self.solver.spmv_tiles(spmv_tiles)
         t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
         self.rows, self.cols, self.blocks, self.b = t(rows), t(cols), t(blocks.reshape(-1)), t(b)
         self.x = torch.zeros_like(self.b)

@@ -96,6 +96,24 @@ def spmv_noalloc(a, blocks, rows, cols, nnzb, x, b, y, stream=None):
                                         _ptr(y), int(y.numel()), s), "stg_spmv_noalloc")
 
 
+def morton_keys(pos, stream=None):
+    """Per-vertex 64-bit Morton keys (code << 32) | index of device positions (stg_morton_keys,
+    _calcVertMChash at GIPC.cu:453-502); pos: CUDA float64 tensor [V, 3] or [3V].  Returns an
+    int64 tensor [V] on the same device holding the keys' uint64 bit patterns (view it as
+    uint64 on the host: keys.cpu().numpy().view(np.uint64))."""
+    import torch
+    _require_cuda(pos)
+    if pos.dtype != torch.float64 or pos.numel() % 3 != 0:
+        raise ValueError("morton_keys: pos must be float64 with 3 values per vertex")
+    pos = pos.contiguous()
+    n = pos.numel() // 3
+    keys = torch.empty(n, dtype=torch.int64, device=pos.device)
+    s = None if stream is None else stream.cuda_stream
+    with torch.cuda.device(pos.device):
+        check(_L.lib().stg_morton_keys(n, _ptr(pos), _ptr(keys), s), "stg_morton_keys")
+    return keys
+
+
 class Solver:
     """One handle: GlobalLinearSystem + PCGSolver + MAS preconditioner on one stream."""
 
@@ -226,14 +244,17 @@ class Solver:
 
     # -- BCOO tile autotuner -------------------------------------------------------------------
     def spmv_tiles(self, rows_per_tile: int):
-        """0: autotune at the next solve of a new shape; -1: default; else a fixed shape."""
+        """0: autotune at the next solve of a new shape class; -1: default; -2: the halo
+        kernel; else a fixed tile shape."""
         check(_L.lib().stg_spmv_tiles(self.h, int(rows_per_tile)), "stg_spmv_tiles")
 
     def spmv_tiles_info(self):
-        """(rows per tile of the last solve, tuner us per launch: default, alternative)."""
-        rt, a, b = C.c_int(), C.c_float(), C.c_float()
-        check(_L.lib().stg_spmv_tiles_info(self.h, C.byref(rt), C.byref(a), C.byref(b)), "stg_spmv_tiles_info")
-        return rt.value, a.value, b.value
+        """(rows per tile of the last solve (-2: halo kernel), tuner us per launch: default
+        shape, alternative shape, halo kernel)."""
+        rt, a, b, h = C.c_int(), C.c_float(), C.c_float(), C.c_float()
+        check(_L.lib().stg_spmv_tiles_info(self.h, C.byref(rt), C.byref(a), C.byref(b), C.byref(h)),
+              "stg_spmv_tiles_info")
+        return rt.value, a.value, b.value, h.value
 
     # -- learned coarse correction (stg_net_*) ---------------------------------------------
     def net_configure(self, level: int):

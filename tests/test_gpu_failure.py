@@ -18,7 +18,8 @@ def test_bounded_wait_gives_up_and_context_stays_usable(dev):
     status, seconds = C.c_int(-1), C.c_double(-1.0)
     assert L.stg_selftest_wait_timeout(C.byref(status), C.byref(seconds)) == _lib.STG_OK
     assert status.value == _lib.STG_ERR_TIMEOUT
-    assert 0.0 < seconds.value < 60.0
+    # every bounded wait gives up after 1 s of the device's global timer
+    assert 0.9 < seconds.value < 3.0, seconds.value
     # the device still works: a normal solve afterwards
     gls = GlobalLinearSystem(cube_system(8), PCGSolverConfig(), device=dev)
     st = gls.solve_linear_system()

@@ -72,6 +72,51 @@ def test_morton_code_known_answers():
     assert int(scenes.expand_bits(np.array([1023], np.uint32))[0]) == 0x09249249
 
 
+def _scalar_morton_keys(pos):
+    """_calcVertMChash + hash_code(type -1) + expand_bits (GIPC.cu:183-208, 453-502) written
+    out per vertex with Python floats and 32-bit integer arithmetic."""
+    def spread(v):
+        for mul, mask in ((0x00010001, 0xFF0000FF), (0x00000101, 0x0F00F00F), (0x00000011, 0xC30C30C3),
+                          (0x00000005, 0x49249249)):
+            v = ((v * mul) & 0xFFFFFFFF) & mask
+        return v
+    lo = [min(float(p[a]) for p in pos) for a in range(3)]
+    hi = [max(float(p[a]) for p in pos) for a in range(3)]
+    keys = []
+    for i, p in enumerate(pos):
+        cells = []
+        for a in range(3):
+            v = (float(p[a]) - lo[a]) / (hi[a] - lo[a]) * 1024.0
+            v = 0.0 if v < 0.0 else v
+            v = 1023.0 if 1023.0 < v else v
+            cells.append(int(v))
+        code = ((spread(cells[0]) << 2) + (spread(cells[1]) << 1) + spread(cells[2])) & 0xFFFFFFFF
+        keys.append((code << 32) | i)
+    return np.array(keys, dtype=np.uint64)
+
+
+def test_morton_whole_keys_and_order():
+    """Whole 64-bit keys of scenes.morton_hash against the per-vertex restatement, on a
+    jittered cube and on a random cloud; morton_renumber's order against an independent sort
+    by (code, index)."""
+    from stgipc import scenes
+    s = cube_system(8)
+    rng = np.random.default_rng(3)
+    for pos in (s.pos, rng.uniform(-2.0, 3.0, size=(700, 3))):
+        want = _scalar_morton_keys(pos)
+        assert np.array_equal(scenes.morton_hash(pos), want)
+    pos, tets = scenes.cube_mesh(6)
+    pos = pos + rng.uniform(-1e-3, 1e-3, size=pos.shape)
+    keys = _scalar_morton_keys(pos)
+    order_want = np.array(sorted(range(pos.shape[0]), key=lambda i: (int(keys[i]) >> 32, i)))
+    pos2, tets2, order = scenes.morton_renumber(pos, tets)
+    assert np.array_equal(order, order_want)
+    assert np.array_equal(pos2, pos[order_want])
+    new_of_old = np.empty_like(order)
+    new_of_old[order] = np.arange(order.size)
+    assert np.array_equal(tets2, new_of_old[tets])
+
+
 def test_neighbor_lists_symmetric_and_complete():
     s = cube_system(8)
     V = s.num_verts
