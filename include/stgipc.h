@@ -246,6 +246,26 @@ int stg_fem_energy(int verts, const double* rest, const double* pos, const doubl
                    int nplanes, const double* planes, void* scratch, size_t scratch_bytes, double* energy,
                    int* violations, void* stream);
 
+/* ---- contact barriers ------------------------------------------------------------------- */
+/* Replaces _calBarrierGradientAndHessian (StiffGIPC/GIPC.cu:3149-4988, built with NEWF and
+ * RANK 2) for the unmollified encodings of the int4 pairs (GIPC.cuh:49-66): edge-edge
+ * (x, y | z, w), point-point (-x-1, y; z < 0), point-edge (-x-1 | y, z; w < 0) and
+ * point-triangle (-x-1 | y, z, w).  With s = d / sqrt(dhat) (d the pair's distance, dhat the
+ * squared activation distance) the barrier is kappa dhat^2 (s^2 - 1)^2 ln^2(s^2) for s < 1;
+ * per pair: gradient E'(s) ds/dx (12 doubles, 3 per local vertex, zero for unused vertices)
+ * and the 10 upper 3x3 blocks (column-major, row <= col, plus block_offset) of the rank-one
+ * Hessian E''(s) ds/dx ds/dx^T, with E'' frozen at s^2 = 1e-6 below it (GIPC.cu:3171,
+ * 3310-3327).  Slot k of pair p is triplet 10 p + k in the order (0,0) (0,1) (0,2) (0,3)
+ * (1,1) (1,2) (1,3) (2,2) (2,3) (3,3) of local vertices; a slot past the pair's vertex count
+ * holds a zero block on its first vertex.  A mollified, out-of-range or degenerate pair gets
+ * zero blocks and a zero gradient and is counted in *skipped (device int, may be NULL; added
+ * to, not reset).  pairs: device int32[4 ncp]; x: device double[3 num_verts]; rows / cols:
+ * device int32[10 ncp]; blocks: device double[90 ncp]; grad: device double[12 ncp].
+ * Asynchronous on `stream` (a cudaStream_t; NULL: the legacy default stream). */
+int stg_contact_barrier(int ncp, const int32_t* pairs, const double* x, int num_verts, int block_offset,
+                        double dhat, double kappa, int32_t* rows, int32_t* cols, double* blocks,
+                        double* grad, int* skipped, void* stream);
+
 /* ---- independent scenes in one solve ---------------------------------------------------- */
 /* No counterpart in the reference.  The system of the following solves is a block-diagonal
  * batch of independent scenes on contiguous block-row ranges [row_offsets[s],

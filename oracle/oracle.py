@@ -69,6 +69,11 @@ def lib():
         L.orc_pcg.argtypes = [_i32p, _i32p, _f64p, C.c_int, C.c_int, _f64p, _f64p, C.c_void_p, C.c_int, C.c_int,
                               C.c_int, C.c_void_p, C.c_double, C.c_double, C.POINTER(PcgStats)]
         L.orc_pcg.restype = C.c_int
+        L.orc_contact_barrier.argtypes = [C.c_int, _i32p, _f64p, C.c_int, C.c_int, C.c_double, C.c_double, _i32p,
+                                          _i32p, _f64p, _f64p]
+        L.orc_contact_barrier.restype = C.c_int
+        L.orc_contact_d2.argtypes = [C.c_int, _f64p, _f64p]
+        L.orc_contact_d2.restype = C.c_double
         L.orc_pcg_ex.argtypes = [_i32p, _i32p, _f64p, C.c_int, C.c_int, _f64p, _f64p, C.c_void_p, C.c_int, C.c_int,
                                  C.c_int, C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_double,
                                  C.POINTER(PcgStats), C.POINTER(C.c_double), C.POINTER(C.c_int)]
@@ -249,3 +254,26 @@ def extrapolated_iterations(stats, target=1e-4):
         return it
     rate = rel ** (1.0 / it)
     return int(np.ceil(np.log(target) / np.log(rate)))
+
+
+def contact_barrier(pairs, x, dhat, kappa, block_offset=0):
+    """(rows, cols, blocks [10 P, 9] column-major, grad [P, 12], skipped) of the contact
+    barrier of the sign-encoded pairs [P, 4] at positions x [V, 3] (the restatement of
+    GIPC.cu:3149-4988 in stg_oracle.c)."""
+    pairs = np.ascontiguousarray(pairs, np.int32).reshape(-1, 4)
+    x = np.ascontiguousarray(x, np.float64).reshape(-1, 3)
+    P = pairs.shape[0]
+    rows, cols = np.empty(10 * P, np.int32), np.empty(10 * P, np.int32)
+    blocks, grad = np.empty((10 * P, 9)), np.empty((P, 12))
+    sk = lib().orc_contact_barrier(P, pairs.reshape(-1), x.reshape(-1), x.shape[0], block_offset, float(dhat),
+                                   float(kappa), rows, cols, blocks.reshape(-1), grad.reshape(-1))
+    return rows, cols, blocks, grad, int(sk)
+
+
+def contact_d2(kind, v):
+    """(d^2, d(d^2)/dx [12]) of one pair of kind 0 PP, 1 PE, 2 PT, 3 EE; v: [k, 3] vertices."""
+    w = np.zeros(12)
+    v = np.asarray(v, np.float64).reshape(-1)
+    w[:v.size] = v
+    g = np.zeros(12)
+    return float(lib().orc_contact_d2(int(kind), w, g)), g

@@ -1456,3 +1456,150 @@ int orc_cg_bj_mt(const int* rows, const int* cols, const double* blocks, int nnz
     free(A.ptr); free(A.col); free(A.val);
     return (int)k;
 }
+
+/* ---- contact barrier Hessians ----------------------------------------------------------
+ * Restates _calBarrierGradientAndHessian (StiffGIPC/GIPC.cu:3149-4988, NEWF and RANK 2) for
+ * the unmollified pair encodings: E(s) = kappa dHat^2 (s^2 - 1)^2 ln^2(s^2), s = d / sqrt(dHat),
+ * gradient E'(s) ds/dx (flatten_pk1, GIPC.cu:3258-3262), Hessian lambda0 ds/dx ds/dx^T with
+ * lambda0 = E''(s) (GIPC.cu:3310-3327), frozen at s^2 = 1e-6 below it.  ds/dx is written here
+ * in closed form from the squared distances of mlbvh.cu:229-257 (the reference's PFPx last
+ * column, GIPC_PDerivative.cuh, is the same derivative generated symbolically).  The output
+ * layout is 10 upper 3x3 blocks per pair (SymGH order, GIPC.cu:117-175) plus 12 gradient
+ * entries; unused slots hold a zero block on the first vertex's diagonal.  Returns the number
+ * of pairs skipped (mollified encodings, out-of-range or repeated vertices). */
+static void v3sub(const double* a, const double* b, double* r) { r[0] = a[0] - b[0], r[1] = a[1] - b[1], r[2] = a[2] - b[2]; }
+static double v3dot(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+static void v3cross(const double* a, const double* b, double* r)
+{
+    r[0] = a[1] * b[2] - a[2] * b[1];
+    r[1] = a[2] * b[0] - a[0] * b[2];
+    r[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* d^2 and its gradient (12 entries, 3 per local vertex) for type 0 PP, 1 PE, 2 PT, 3 EE */
+static double contact_d2(int type, const double* v, double* g)
+{
+    const double *p0 = v, *p1 = v + 3, *p2 = v + 6, *p3 = v + 9;
+    memset(g, 0, 12 * sizeof(double));
+    if(type == 0)
+    {
+        double r[3];
+        v3sub(p0, p1, r);
+        for(int k = 0; k < 3; k++) g[k] = 2 * r[k], g[3 + k] = -2 * r[k];
+        return v3dot(r, r);
+    }
+    if(type == 1)
+    {
+        /* d^2 = |c|^2 / |e|^2, c = (p1 - p0) x (p2 - p0), e = p2 - p1 */
+        double a[3], b[3], c[3], e[3], bc[3], ca[3];
+        v3sub(p1, p0, a), v3sub(p2, p0, b), v3sub(p2, p1, e), v3cross(a, b, c);
+        v3cross(b, c, bc), v3cross(c, a, ca);
+        const double C2 = v3dot(c, c), E2 = v3dot(e, e), d2 = C2 / E2;
+        for(int k = 0; k < 3; k++)
+        {
+            const double ga = 2 * bc[k], gb = 2 * ca[k]; /* d|c|^2 / da, d|c|^2 / db */
+            g[3 + k] = (ga + d2 * 2 * e[k]) / E2;
+            g[6 + k] = (gb - d2 * 2 * e[k]) / E2;
+            g[k] = -(ga + gb) / E2;
+        }
+        return d2;
+    }
+    /* PT: b = (p2 - p1) x (p3 - p1), r = p0 - p1, u = p2 - p1, w = p3 - p1, moving (r, u, w);
+     * EE: b = (p1 - p0) x (p3 - p2), r = p2 - p0, u = p1 - p0, w = p3 - p2.
+     * d^2 = A^2 / |b|^2 with A = r . b */
+    double r[3], u[3], w[3], b[3], wr[3], ru[3], wb[3], bu[3];
+    if(type == 2)
+        v3sub(p0, p1, r), v3sub(p2, p1, u), v3sub(p3, p1, w);
+    else
+        v3sub(p2, p0, r), v3sub(p1, p0, u), v3sub(p3, p2, w);
+    v3cross(u, w, b), v3cross(w, r, wr), v3cross(r, u, ru), v3cross(w, b, wb), v3cross(b, u, bu);
+    const double A = v3dot(r, b), B2 = v3dot(b, b), d2 = A * A / B2;
+    for(int k = 0; k < 3; k++)
+    {
+        /* d(d^2) = (2 A dA - d^2 d|b|^2) / |b|^2; dA/dr = b, dA/du = w x r, dA/dw = r x u;
+         * d|b|^2/du = 2 w x b, d|b|^2/dw = 2 b x u */
+        const double gr = 2 * A * b[k] / B2;
+        const double gu = (2 * A * wr[k] - d2 * 2 * wb[k]) / B2;
+        const double gw = (2 * A * ru[k] - d2 * 2 * bu[k]) / B2;
+        if(type == 2)
+            g[k] = gr, g[6 + k] = gu, g[9 + k] = gw, g[3 + k] = -(gr + gu + gw);
+        else
+            g[k] = -(gr + gu), g[3 + k] = gu, g[6 + k] = gr - gw, g[9 + k] = gw;
+    }
+    return d2;
+}
+
+int orc_contact_barrier(int ncp, const int32_t* pairs, const double* x, int nv, int block_offset, double dhat,
+                        double kappa, int32_t* rows, int32_t* cols, double* blocks, double* grad)
+{
+    int skipped = 0;
+    for(int p = 0; p < ncp; p++)
+    {
+        const int32_t* q = pairs + 4 * (size_t)p;
+        int vid[4] = {0, 0, 0, 0}, cnt = 0, type = -1;
+        if(q[0] >= 0)
+        {
+            if(q[3] >= 0) type = 3, vid[0] = q[0], vid[1] = q[1], vid[2] = q[2], vid[3] = q[3], cnt = 4;
+        }
+        else if(q[1] >= 0)
+        {
+            vid[0] = -q[0] - 1, vid[1] = q[1];
+            if(q[2] < 0)
+                type = 0, cnt = 2;
+            else if(q[3] < 0)
+                type = 1, vid[2] = q[2], cnt = 3;
+            else
+                type = 2, vid[2] = q[2], vid[3] = q[3], cnt = 4;
+        }
+        int ok = type >= 0;
+        for(int i = 0; i < cnt; i++) ok = ok && vid[i] >= 0 && vid[i] < nv;
+        for(int i = 0; i < cnt; i++)
+            for(int j = i + 1; j < cnt; j++) ok = ok && vid[i] != vid[j];
+        double h[12] = {0}, lam = 0, e1 = 0;
+        if(ok)
+        {
+            double v[12] = {0}, g2[12];
+            for(int i = 0; i < cnt; i++) memcpy(v + 3 * i, x + 3 * (size_t)vid[i], 3 * sizeof(double));
+            const double d2 = contact_d2(type, v, g2), d = sqrt(d2), s = d / sqrt(dhat);
+            if(s > 0 && s < 1)
+            {
+                const double I = s * s, lI = log(I), D2 = dhat * dhat;
+                e1 = s * 2 * (2 * kappa * D2 * lI * (I - 1) * (I + I * lI - 1)) / I;
+                const double Ic = I < 1e-6 ? 1e-6 : I, l = log(Ic);
+                lam = -(4 * kappa * D2 *
+                        (4 * Ic + l - 3 * Ic * Ic * l * l + 6 * Ic * l - 2 * Ic * Ic + Ic * l * l - 7 * Ic * Ic * l - 2)) /
+                      Ic;
+                for(int k = 0; k < 12; k++) h[k] = g2[k] / (2 * d) / sqrt(dhat);
+            }
+        }
+        else
+            skipped++;
+        for(int k = 0; k < 12; k++) grad[12 * (size_t)p + k] = e1 * h[k];
+        int slot = 0;
+        for(int i = 0; i < 4; i++)
+            for(int j = i; j < 4; j++, slot++)
+            {
+                const size_t o = 10 * (size_t)p + slot;
+                double* B = blocks + 9 * o;
+                if(!ok || i >= cnt || j >= cnt)
+                {
+                    rows[o] = cols[o] = block_offset + (ok ? vid[0] : 0);
+                    memset(B, 0, 9 * sizeof(double));
+                    continue;
+                }
+                const int gi = vid[i], gj = vid[j], sw = gi > gj;
+                rows[o] = block_offset + (sw ? gj : gi);
+                cols[o] = block_offset + (sw ? gi : gj);
+                for(int a = 0; a < 3; a++)
+                    for(int b = 0; b < 3; b++)
+                    {
+                        const double val = lam * h[3 * i + a] * h[3 * j + b];
+                        B[sw ? a * 3 + b : b * 3 + a] = val;
+                    }
+            }
+    }
+    return skipped;
+}
+
+/* d^2 of one pair of type 0 PP, 1 PE, 2 PT, 3 EE and its gradient g[12] (test access) */
+double orc_contact_d2(int type, const double* v, double* g) { return contact_d2(type, v, g); }

@@ -108,6 +108,7 @@ def lib():
                                         C.c_size_t, vp]
     L.stg_fem_energy.argtypes = [ci, vp, vp, vp, ci, vp, vp, cd, cd, cd, ci, vp, vp, C.c_size_t, C.POINTER(cd),
                                  C.POINTER(ci), vp]
+    L.stg_contact_barrier.argtypes = [ci, vp, vp, ci, ci, cd, cd, vp, vp, vp, vp, vp, vp]
     L.stg_spmv_tiles_info.argtypes = [vp, C.POINTER(ci), C.POINTER(C.c_float), C.POINTER(C.c_float),
                                       C.POINTER(C.c_float)]
     L.stg_net_configure.argtypes = [vp, ci]

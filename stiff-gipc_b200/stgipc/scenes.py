@@ -457,3 +457,172 @@ def cached(builder, key: str, **kw) -> NewtonSystem:
              pos=s.pos, tets=s.tets, neighbor_start=s.neighbor_start, neighbor_num=s.neighbor_num,
              neighbor_list=s.neighbor_list, contacts=s.contacts)
     return s
+
+
+# ----------------------------------------------------------------------------------------
+# Contact pairs between bodies (the input of stgipc.contact.barrier)
+# ----------------------------------------------------------------------------------------
+
+
+def boundary_faces(tets: np.ndarray) -> np.ndarray:
+    """The triangles of a tet mesh that belong to exactly one tet."""
+    f = np.concatenate([tets[:, [0, 1, 2]], tets[:, [0, 1, 3]], tets[:, [0, 2, 3]], tets[:, [1, 2, 3]]])
+    key = np.sort(f, axis=1)
+    _, idx, cnt = np.unique(key, axis=0, return_index=True, return_counts=True)
+    return f[idx[cnt == 1]].astype(np.int64)
+
+
+def face_edges(tris: np.ndarray) -> np.ndarray:
+    e = np.concatenate([tris[:, [0, 1]], tris[:, [1, 2]], tris[:, [2, 0]]])
+    return np.unique(np.sort(e, axis=1), axis=0)
+
+
+def _pt_type(p, t0, t1, t2):
+    """Closest feature of triangle (t0, t1, t2) to p, per pair (the regions of _dType_PT,
+    mlbvh.cu:288-446): 0..2 vertex t_k, 3..5 edge (t0 t1), (t1 t2), (t2 t0), 6 interior."""
+    n = np.cross(t1 - t0, t2 - t0)
+    out = np.full(p.shape[0], 6, np.int64)
+    pars = []
+    for (a, b) in ((t0, t1), (t1, t2), (t2, t0)):
+        e = b - a
+        side = np.cross(e, n)                       # in-plane, pointing out of the triangle
+        w = p - a
+        s = np.einsum("ij,ij->i", w, e) / np.einsum("ij,ij->i", e, e)
+        h = np.einsum("ij,ij->i", w, side)
+        pars.append((s, h))
+    done = np.zeros(p.shape[0], bool)
+    for k, (s, h) in enumerate(pars):
+        m = ~done & (s > 0) & (s < 1) & (h >= 0)
+        out[m], done = 3 + k, done | m
+    for k in range(3):   # vertex t_k: beyond the start of edge k and the end of edge k-1
+        s_out, s_in = pars[k][0], pars[k - 1][0]
+        m = ~done & (s_out <= 0) & (s_in >= 1)
+        out[m], done = k, done | m
+    return out
+
+
+def contact_pairs(pos: np.ndarray, tris: np.ndarray, body: np.ndarray, dhat: float, mollify_eps: float = 1e-3):
+    """Sign-encoded int4 pairs (GIPC.cuh:49-66) between the surfaces of different bodies
+    within distance sqrt(dhat): every (surface vertex, triangle) pair classified by its
+    closest feature into PT, PE or PP, and every (edge, edge) pair whose closest points are
+    interior to both edges as EE.  Near-parallel edge pairs (|ea x eb|^2 < mollify_eps
+    |ea|^2 |eb|^2, the reference's mollifier zone, mlbvh.cu:278-285) and edge pairs whose closest
+    points sit at an endpoint are left out.  Duplicates are merged.  Brute force over a
+    uniform grid of cell size max(longest edge, sqrt(dhat)); meant for scene synthesis."""
+    r = np.sqrt(dhat)
+    edges = face_edges(tris)
+    verts = np.unique(tris)
+    h = max(float(np.linalg.norm(pos[edges[:, 0]] - pos[edges[:, 1]], axis=1).max()), r) * 1.0001
+
+    def cand(prim_a, prim_b):
+        """Pairs (i, j) of primitives (vertex lists) whose cells are within one of each other."""
+        ca = np.floor(pos[prim_a].min(axis=1) / h).astype(np.int64)
+        cb_lo = np.floor((pos[prim_b].min(axis=1) - r) / h).astype(np.int64)
+        cb_hi = np.floor((pos[prim_b].max(axis=1) + r) / h).astype(np.int64)
+        ka = ca @ np.array([1 << 42, 1 << 21, 1])
+        order = np.argsort(ka, kind="stable")
+        ks = ka[order]
+        out_i, out_j = [], []
+        span = cb_hi - cb_lo
+        for dx in range(int(span[:, 0].max()) + 2):
+            for dy in range(int(span[:, 1].max()) + 2):
+                for dz in range(int(span[:, 2].max()) + 2):
+                    c = cb_lo + np.array([dx, dy, dz]) - 1
+                    ok = np.all(c <= cb_hi, axis=1)
+                    kb = c @ np.array([1 << 42, 1 << 21, 1])
+                    lo = np.searchsorted(ks, kb, "left")
+                    hi = np.searchsorted(ks, kb, "right")
+                    for j in np.nonzero(ok & (hi > lo))[0]:
+                        out_i.append(order[lo[j]:hi[j]])
+                        out_j.append(np.full(hi[j] - lo[j], j))
+        if not out_i:
+            return np.zeros(0, np.int64), np.zeros(0, np.int64)
+        pi, pj = np.concatenate(out_i), np.concatenate(out_j)
+        key = np.unique(pi * (prim_b.shape[0] + 1) + pj)
+        return key // (prim_b.shape[0] + 1), key % (prim_b.shape[0] + 1)
+
+    out = []
+    # point - triangle
+    i, j = cand(verts[:, None], tris)
+    p = verts[i]
+    t = tris[j]
+    keep = body[p] != body[t[:, 0]]
+    p, t = p[keep], t[keep]
+    if p.size:
+        P, T0, T1, T2 = pos[p], pos[t[:, 0]], pos[t[:, 1]], pos[t[:, 2]]
+        ty = _pt_type(P, T0, T1, T2)
+        n = np.cross(T1 - T0, T2 - T0)
+        d2 = np.full(p.size, np.inf)
+        m = ty == 6
+        d2[m] = np.einsum("ij,ij->i", P[m] - T0[m], n[m]) ** 2 / np.einsum("ij,ij->i", n[m], n[m])
+        ea = [(0, 1), (1, 2), (2, 0)]
+        tv = [T0, T1, T2]
+        enc = np.zeros((p.size, 4), np.int64)
+        enc[m] = np.stack([-p[m] - 1, t[m, 0], t[m, 1], t[m, 2]], 1)
+        for k, (a, b) in enumerate(ea):
+            mk = ty == 3 + k
+            e = tv[b][mk] - tv[a][mk]
+            c = np.cross(tv[a][mk] - P[mk], tv[b][mk] - P[mk])
+            d2[mk] = np.einsum("ij,ij->i", c, c) / np.einsum("ij,ij->i", e, e)
+            enc[mk] = np.stack([-p[mk] - 1, t[mk, a], t[mk, b], -np.ones(mk.sum(), np.int64)], 1)
+        for k in range(3):
+            mk = ty == k
+            dv = P[mk] - tv[k][mk]
+            d2[mk] = np.einsum("ij,ij->i", dv, dv)
+            enc[mk] = np.stack([-p[mk] - 1, t[mk, k], -np.ones(mk.sum(), np.int64), -np.ones(mk.sum(), np.int64)], 1)
+        out.append(enc[d2 < dhat])
+    # edge - edge
+    i, j = cand(edges, edges)
+    keep = (i < j) & (body[edges[i, 0]] != body[edges[j, 0]])
+    ea_, eb_ = edges[i[keep]], edges[j[keep]]
+    if ea_.size:
+        A0, A1, B0, B1 = pos[ea_[:, 0]], pos[ea_[:, 1]], pos[eb_[:, 0]], pos[eb_[:, 1]]
+        u, v, w = A1 - A0, B1 - B0, A0 - B0
+        a = np.einsum("ij,ij->i", u, u)
+        b = np.einsum("ij,ij->i", u, v)
+        c = np.einsum("ij,ij->i", v, v)
+        d = np.einsum("ij,ij->i", u, w)
+        e = np.einsum("ij,ij->i", v, w)
+        D = a * c - b * b
+        cr = np.cross(u, v)
+        cr2 = np.einsum("ij,ij->i", cr, cr)
+        ok = cr2 >= mollify_eps * a * c
+        Ds = np.where(ok, D, 1.0)
+        s = (b * e - c * d) / Ds
+        tt = (a * e - b * d) / Ds
+        ok &= (s > 0) & (s < 1) & (tt > 0) & (tt < 1)
+        d2 = np.einsum("ij,ij->i", w, cr) ** 2 / np.where(ok, cr2, 1.0)
+        ok &= d2 < dhat
+        out.append(np.stack([ea_[ok, 0], ea_[ok, 1], eb_[ok, 0], eb_[ok, 1]], 1))
+    if not out:
+        return np.zeros((0, 4), np.int32)
+    allp = np.concatenate(out)
+    return np.unique(allp, axis=0).astype(np.int32)
+
+
+def make_stacked_cubes(n: int = 8, seed: int = 1006, E: float = 1e5, nu: float = 0.45, rho: float = 1000.0,
+                       dt: float = 1.0 / 60.0, size: float = 0.5, gap: float = 4e-4, dhat: float = 1e-6,
+                       kappa: float = 1e5, jitter: float = 1e-5):
+    """Two soft cubes, one resting on the other, with the upper one shifted by half a cell in
+    x and z so its bottom vertices lie over the lower one's top triangles, ``gap`` m apart
+    (inside the barrier's sqrt(dhat)); the lower cube rests ``gap`` above a ground barrier.
+    Returns (NewtonSystem of the elastic + inertia + ground terms, contact pairs [C, 4],
+    body id per vertex); the contact barrier terms come from stgipc.contact.barrier."""
+    rng = np.random.default_rng(seed)
+    pa, ta = cube_mesh(n, size, origin=(0.0, gap, 0.0))
+    h = size / n
+    pb, tb = cube_mesh(n, size, origin=(0.5 * h, gap + size + gap, 0.5 * h))
+    pos = np.concatenate([pa, pb])
+    tets = np.concatenate([ta, tb + pa.shape[0]])
+    body = np.concatenate([np.zeros(pa.shape[0], np.int64), np.ones(pb.shape[0], np.int64)])
+    pos = pos + rng.uniform(-jitter, jitter, size=pos.shape)
+    pos, tets, old_of_new = morton_renumber(pos, tets)
+    body = body[old_of_new]
+    E_t = np.full(tets.shape[0], E)
+    vel = np.zeros_like(pos)
+    vel[:, 1] = -0.5
+    sysm = _assemble(f"stacked{n}", pos, pos, tets, E_t, nu, rho, dt, vel,
+                     barriers=[((0.0, 1.0, 0.0), 0.0, np.sqrt(dhat), kappa)])
+    pairs = contact_pairs(pos, boundary_faces(tets), body, dhat)
+    sysm.contacts = pairs
+    return sysm, pairs, body
