@@ -168,7 +168,10 @@ typedef struct stg_system
     int fem_block_offset;       /* 4 * abd_bodies                                      */
     const int32_t* contacts;    /* int4 collision pairs or NULL                        */
     int ncp;
-    /* ABD 12x12 block-Jacobi (abd_preconditioner.cu:20-38): row-major inverses or NULL */
+    /* ABD 12x12 block-Jacobi (abd_preconditioner.cu:20-38): row-major inverses, or NULL to
+     * invert the bodies' diagonal 12x12 tiles of the converted BCOO on the device, as
+     * ABDSystem::_cal_abd_system_preconditioner does (setup_abd_system_gradient_and_hessian.cu:
+     * 612-655; FP64 Gauss-Jordan with partial pivoting) */
     int abd_bodies;
     const double* abd_inv;
 } stg_system;
@@ -265,6 +268,45 @@ int stg_fem_energy(int verts, const double* rest, const double* pos, const doubl
 int stg_contact_barrier(int ncp, const int32_t* pairs, const double* x, int num_verts, int block_offset,
                         double dhat, double kappa, int32_t* rows, int32_t* cols, double* blocks,
                         double* grad, int* skipped, void* stream);
+
+/* ---- affine bodies (ABD) ---------------------------------------------------------------- */
+/* Body b owns block rows 4 b .. 4 b + 3; q[12 b ..] = (t, a1, a2, a3) with a_i the rows of A
+ * (x = A xbar + t, abd_jacobi_matrix.inl); FEM vertices follow at block row 4 bodies + v.
+ *
+ * Replaces ABDSystem::_cal_abd_body_gradient_and_hessian + write_abd_body_hessian
+ * (abd_system/abd_system_function/setup_abd_system_gradient_and_hessian.cu:129-139, 200-262)
+ * for free and fixed bodies: per body, the 10 upper 3x3 blocks (column-major, triplets
+ * 10 b .. 10 b + 9 in (0,0) (0,1) .. (3,3) order) of H = M + kappa vol dt^2 PSD(d2S/da2) and
+ * the gradient g = M (q - q_tilde) + kappa vol dt^2 dS/da, S = sum (a_i.a_i - 1)^2 +
+ * sum_{i != j} (a_i.a_j)^2 (abd_energy.inl:9-140), PSD by clamping negative eigenvalues of the
+ * 9x9 a-block (FP64 Jacobi).  mass: 13 doubles per body, the dyadic mass m, m xbar (3),
+ * m xbar xbar^T (9, row-major) summed over the body's points (ABDJacobiDyadicMass).  fixed
+ * (may be NULL): nonzero marks a fixed body (H = M, g = 0).  Device arrays; asynchronous. */
+int stg_abd_body_system(int bodies, const double* q, const double* q_tilde, const double* mass,
+                        const double* volume, const int32_t* fixed, double kappa, double dt,
+                        int32_t* rows, int32_t* cols, double* blocks, double* grad, void* stream);
+/* Replaces write_barrier_hessian and the ABD-FEM coupling kernel
+ * (setup_abd_system_gradient_and_hessian.cu:89-126, 510-551) and the FEM contact shift
+ * (GIPC.cu:10328-10362): maps `count` point-level 3x3 triplets (i, j) of a symmetric matrix
+ * given by its upper blocks (a block with i > j is read as the transpose at (j, i)) onto the
+ * global block index space, 16 output triplets per input at 16 t .. 16 t + 15.  Points
+ * [0, abd_points) belong to bodies point_body[i] with rest coordinates xbar[3 i ..]; points
+ * from abd_points on are FEM vertex i - abd_points.  Two FEM vertices: the block at
+ * (4 bodies + i - P, 4 bodies + j - P).  Body point and FEM vertex: the 4 blocks of J_i^T B.
+ * Two body points of different bodies: the 16 blocks of J_i^T B J_j (JT_H_J).  Of one body:
+ * the 10 upper blocks of J_i^T B J_i (i == j) or of J_i^T B J_j + (J_i^T B J_j)^T (i != j).
+ * Unused slots hold zero blocks on the first row written.  *bad (device, may be NULL) counts
+ * inputs with a negative index or a body id outside [0, bodies); they get zero blocks. */
+int stg_abd_map_triplets(int count, const int32_t* rows, const int32_t* cols, const double* blocks,
+                         int abd_points, const int32_t* point_body, const double* xbar, int bodies,
+                         int32_t* out_rows, int32_t* out_cols, double* out_blocks, int* bad, void* stream);
+/* x[3 i ..] = A xbar_i + t of point i's body (cal_x_from_q); device arrays. */
+int stg_abd_points(int abd_points, const int32_t* point_body, const double* xbar, const double* q,
+                   double* x, void* stream);
+/* body_grad[12 b ..] += sum over the body's points i in [start[b], start[b + 1]) of J_i^T g_i,
+ * in point order (_cal_abd_system_barrier_gradient, :362-396); device arrays. */
+int stg_abd_gather_gradient(int bodies, const int32_t* body_point_start, const double* xbar,
+                            const double* point_grad, double* body_grad, void* stream);
 
 /* ---- independent scenes in one solve ---------------------------------------------------- */
 /* No counterpart in the reference.  The system of the following solves is a block-diagonal

@@ -199,18 +199,20 @@ def pcg(rows, cols, blocks, b, mas: Mas | None = None, fem_offset=0, use_diag=Fa
 
 
 def pcg_timed(rows, cols, blocks, b, mas: Mas | None = None, fem_offset=0, use_diag=False, tol=1e-4,
-              max_iter_ratio=0.3, stop_rule="reference", budget_s=0.0):
+              max_iter_ratio=0.3, stop_rule="reference", budget_s=0.0, abd_bodies=0, abd_inv=None):
     """PCG with a wall-time budget (CPU baseline sampling).  Returns (x, stats, seconds per
     iteration, finished)."""
     n = b.size
     x = np.zeros(n)
     st = PcgStats()
+    ai = None if abd_inv is None else np.ascontiguousarray(abd_inv, np.float64).reshape(-1)
     t_iter = C.c_double()
     done = C.c_int()
     L = lib()
     L.orc_pcg_ex(np.ascontiguousarray(rows, np.int32), np.ascontiguousarray(cols, np.int32),
                  np.ascontiguousarray(blocks, np.float64).reshape(-1), rows.size, n, np.ascontiguousarray(b, np.float64),
-                 x, mas.h if mas is not None else None, fem_offset, 1 if use_diag else 0, 0, None, tol, max_iter_ratio,
+                 x, mas.h if mas is not None else None, fem_offset, 1 if use_diag else 0, abd_bodies, _p(ai), tol,
+                 max_iter_ratio,
                  0 if stop_rule == "reference" else 1, float(budget_s), C.byref(st), C.byref(t_iter), C.byref(done))
     stats = dict(iterations=st.iterations, rz0=st.rz0, rz_final=st.rz_final, rel_residual=st.rel_residual)
     return x, stats, t_iter.value, bool(done.value)

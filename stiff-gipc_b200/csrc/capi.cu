@@ -323,7 +323,7 @@ int stg_solve_linear_system(stg_handle h, const stg_system* sys, double* x, stg_
     GUARD({
         Solver& S = *h;
         if(!sys || !x || sys->triplet_count < 1 || !sys->rows || !sys->cols || !sys->blocks || !sys->b || sys->n < 3 ||
-           sys->n % 3 != 0 || sys->abd_bodies < 0 || (sys->abd_bodies > 0 && !sys->abd_inv) || sys->ncp < 0 ||
+           sys->n % 3 != 0 || sys->abd_bodies < 0 || sys->ncp < 0 ||
            (sys->ncp > 0 && !sys->contacts))
         {
             stg::set_error("stg_solve_linear_system: invalid arguments");

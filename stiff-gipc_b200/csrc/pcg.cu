@@ -2878,7 +2878,20 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
         set_error("stg_pcg_solve: MAS range exceeds the system");
         return STG_ERR_INVALID;
     }
+    if(abd_bodies > 0 && 4 * abd_bodies > bcoo.nrows)
+    {
+        set_error("stg_pcg_solve: ABD bodies exceed the system");
+        return STG_ERR_INVALID;
+    }
     PcgState& P = pcg;
+    if(abd_bodies > 0 && !abd_inv)
+    {
+        // ABDPreconditioner::assemble: inverses of the bodies' diagonal tiles of this BCOO
+        STG_TRY(P.abd_inv.resize((size_t)abd_bodies * 144));
+        STG_TRY(abd_block_jacobi(bcoo.nnzb, bcoo.R(), bcoo.C(), bcoo.B(), abd_bodies, P.abd_inv.data(), nullptr, s));
+        launches += 3;
+        abd_inv = P.abd_inv.data();
+    }
     const size_t es = fp32 ? sizeof(float) : sizeof(double);
     STG_TRY(P.r.resize(n));
     const size_t nr = (size_t)bcoo.nrows;

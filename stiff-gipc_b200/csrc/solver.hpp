@@ -97,6 +97,7 @@ struct PcgState
     DBuf<int> flags;               // [0] done, [1] status, [2] replacements
     DBuf<unsigned> bar;            // persistent grid barrier
     DBuf<unsigned char> flush;     // 256 MiB written between timed SpMV launches (L2 flush)
+    DBuf<double> abd_inv;          // ABD 12x12 block-Jacobi built from the BCOO [bodies * 144]
     cudaGraphExec_t graph = nullptr;
     PcgDev graph_key{};            // parameter block of the captured graph (handles zeroed)
     PcgDev graph_dev{};            // the same with the graph's conditional handles
@@ -189,6 +190,10 @@ struct Solver
     int mas_apply(const double* r, double* z);
     int pcg_solve(const double* b, double* x, int n, int abd_bodies, const double* abd_inv, stg_stats* st);
 };
+
+// ABD block-Jacobi (abd.cu): inverses of the bodies' diagonal 12x12 tiles of a sorted BCOO
+int abd_block_jacobi(int nnzb, const int* rows, const int* cols, const double* blocks, int N, double* P,
+                     int* singular, cudaStream_t s);
 
 // Hessian producer (fem.cu): 10 T + V triplets and the gradient of one Newton iteration
 size_t fem_scratch_bytes(int V, int T);

@@ -108,6 +108,10 @@ def lib():
                                         C.c_size_t, vp]
     L.stg_fem_energy.argtypes = [ci, vp, vp, vp, ci, vp, vp, cd, cd, cd, ci, vp, vp, C.c_size_t, C.POINTER(cd),
                                  C.POINTER(ci), vp]
+    L.stg_abd_body_system.argtypes = [ci, vp, vp, vp, vp, vp, cd, cd, vp, vp, vp, vp, vp]
+    L.stg_abd_map_triplets.argtypes = [ci, vp, vp, vp, ci, vp, vp, ci, vp, vp, vp, vp, vp]
+    L.stg_abd_points.argtypes = [ci, vp, vp, vp, vp, vp]
+    L.stg_abd_gather_gradient.argtypes = [ci, vp, vp, vp, vp, vp]
     L.stg_contact_barrier.argtypes = [ci, vp, vp, ci, ci, cd, cd, vp, vp, vp, vp, vp, vp]
     L.stg_spmv_tiles_info.argtypes = [vp, C.POINTER(ci), C.POINTER(C.c_float), C.POINTER(C.c_float),
                                       C.POINTER(C.c_float)]

@@ -71,15 +71,19 @@ def morton_hash(pos: np.ndarray, resolution: float = 1024.0) -> np.ndarray:
 
 def cube_mesh(n: int, size: float = 1.0, origin=(0.0, 0.0, 0.0)):
     """(n+1)^3 grid vertices and 6 n^3 Kuhn tets (all sharing each hex's main diagonal)."""
-    m = n + 1
-    g = np.arange(m, dtype=np.float64) * (size / n)
-    z, y, x = np.meshgrid(g, g, g, indexing="ij")
+    return box_mesh(n, n, n, size / n, origin)
+
+
+def box_mesh(nx: int, ny: int, nz: int, h: float, origin=(0.0, 0.0, 0.0)):
+    """(nx+1)(ny+1)(nz+1) grid vertices of spacing h (x fastest) and 6 nx ny nz Kuhn tets."""
+    mx, my, mz = nx + 1, ny + 1, nz + 1
+    z, y, x = np.meshgrid(np.arange(mz) * h, np.arange(my) * h, np.arange(mx) * h, indexing="ij")
     pos = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1) + np.asarray(origin, dtype=np.float64)
 
     def vid(i, j, k):
-        return i + m * (j + m * k)
+        return i + mx * (j + my * k)
 
-    ii, jj, kk = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
     ii, jj, kk = ii.ravel(), jj.ravel(), kk.ravel()
     e = [(1, 0, 0), (0, 1, 0), (0, 0, 1)]
     perms = [(0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)]
@@ -519,22 +523,26 @@ def contact_pairs(pos: np.ndarray, tris: np.ndarray, body: np.ndarray, dhat: flo
         ca = np.floor(pos[prim_a].min(axis=1) / h).astype(np.int64)
         cb_lo = np.floor((pos[prim_b].min(axis=1) - r) / h).astype(np.int64)
         cb_hi = np.floor((pos[prim_b].max(axis=1) + r) / h).astype(np.int64)
-        ka = ca @ np.array([1 << 42, 1 << 21, 1])
+        ka = (ca + (1 << 20)) @ np.array([1 << 42, 1 << 21, 1])
         order = np.argsort(ka, kind="stable")
         ks = ka[order]
         out_i, out_j = [], []
         span = cb_hi - cb_lo
-        for dx in range(int(span[:, 0].max()) + 2):
-            for dy in range(int(span[:, 1].max()) + 2):
-                for dz in range(int(span[:, 2].max()) + 2):
+        for dx in range(int(span[:, 0].max()) + 3):
+            for dy in range(int(span[:, 1].max()) + 3):
+                for dz in range(int(span[:, 2].max()) + 3):
                     c = cb_lo + np.array([dx, dy, dz]) - 1
-                    ok = np.all(c <= cb_hi, axis=1)
-                    kb = c @ np.array([1 << 42, 1 << 21, 1])
+                    ok = np.all(c <= cb_hi + 1, axis=1)
+                    kb = (c + (1 << 20)) @ np.array([1 << 42, 1 << 21, 1])
                     lo = np.searchsorted(ks, kb, "left")
                     hi = np.searchsorted(ks, kb, "right")
-                    for j in np.nonzero(ok & (hi > lo))[0]:
-                        out_i.append(order[lo[j]:hi[j]])
-                        out_j.append(np.full(hi[j] - lo[j], j))
+                    cnt = np.where(ok, hi - lo, 0)
+                    tot = int(cnt.sum())
+                    if tot == 0:
+                        continue
+                    first = np.cumsum(cnt) - cnt
+                    out_i.append(order[np.repeat(lo, cnt) + np.arange(tot) - np.repeat(first, cnt)])
+                    out_j.append(np.repeat(np.arange(cnt.size), cnt))
         if not out_i:
             return np.zeros(0, np.int64), np.zeros(0, np.int64)
         pi, pj = np.concatenate(out_i), np.concatenate(out_j)
@@ -626,3 +634,115 @@ def make_stacked_cubes(n: int = 8, seed: int = 1006, E: float = 1e5, nu: float =
     pairs = contact_pairs(pos, boundary_faces(tets), body, dhat)
     sysm.contacts = pairs
     return sysm, pairs, body
+
+
+def random_rotation(rng) -> np.ndarray:
+    """A uniformly random rotation (QR of a Gaussian matrix with the sign fixed)."""
+    Q, R = np.linalg.qr(rng.normal(size=(3, 3)))
+    Q = Q * np.sign(np.diag(R))
+    if np.linalg.det(Q) < 0:
+        Q[:, 0] = -Q[:, 0]
+    return Q
+
+
+@dataclasses.dataclass
+class AbdScene:
+    """Affine bodies over a FEM mesh at one Newton iteration: bodies own block rows
+    [0, 4 N), FEM vertex v block row 4 N + v.  Points [0, P) are the bodies' mesh points
+    (point_body, rest coordinates xbar), FEM vertices follow as points P + v."""
+    name: str
+    q: np.ndarray             # [N, 12] current (t, a1, a2, a3)
+    q_tilde: np.ndarray       # [N, 12] inertial target
+    mass: np.ndarray          # [N, 13] dyadic mass (m, m xbar, m xbar xbar^T)
+    volume: np.ndarray        # [N]
+    kappa: float
+    dt: float
+    point_body: np.ndarray    # int32 [P]
+    xbar: np.ndarray          # [P, 3]
+    body_point_start: np.ndarray  # int32 [N + 1]
+    fem: NewtonSystem         # FEM elastic + inertia + ground terms (vertex numbering)
+    contacts: np.ndarray      # int32 [C, 4] pairs over the point numbering
+    dhat: float               # squared activation distance of the contacts
+    kappa_contact: float
+
+    @property
+    def bodies(self) -> int:
+        return self.q.shape[0]
+
+    @property
+    def abd_points(self) -> int:
+        return self.point_body.shape[0]
+
+    @property
+    def n(self) -> int:
+        return 3 * (4 * self.bodies + self.fem.num_verts)
+
+
+def make_abd_slab(lattice: int = 8, body_size: float = 0.1, body_n: int = 2, kappa_abd: float = 1e8,
+                  rho: float = 1000.0, slab_n: int = 64, slab_layers: int = 8, slab_size: float = 1.5,
+                  E: float = 1e5, nu: float = 0.45, dt: float = 1.0 / 100.0, body_gap: float = 2e-3,
+                  dhat: float = 1e-6, kappa: float = 1e5, seed: int = 1003, warp: float = 1e-3) -> AbdScene:
+    """lattice^3 affine cubes (body_n^3 hexes, 6 tets each, uniform-random rotations baked
+    into their rest shape) on a lattice of pitch (diagonal + body_gap), falling onto a slab of
+    slab_n x slab_n x slab_layers hexes; the Newton iteration of the step at which the lowest
+    corner of every bottom-layer body sits 2e-4 .. 8e-4 m above the slab (inside sqrt(dhat)).
+    A is I plus a U(+-warp) perturbation, so the orthogonality terms are active; q_tilde is
+    q minus the step's gravity drop.  The slab rests 5e-4 m above a ground barrier.  Defaults:
+    512 bodies, 65 x 65 x 9 = 38,025 slab vertices, 196,608 tets; 6,144 + 114,075 DOF."""
+    rng = np.random.default_rng(seed)
+    h = slab_size / slab_n
+    srest, stets = box_mesh(slab_n, slab_layers, slab_n, h, origin=(0.0, 5e-4, 0.0))
+    srest, stets, _ = morton_renumber(srest, stets)
+    top = float(srest[:, 1].max())
+    bpos, btets = cube_mesh(body_n, body_size, origin=(-0.5 * body_size,) * 3)
+    nb = lattice ** 3
+    pitch = body_size * np.sqrt(3.0) + body_gap
+    x0 = 0.5 * slab_size - 0.5 * pitch * (lattice - 1)
+    xbar, point_body, tris, start, q, masses_all, vols = [], [], [], [0], [], [], []
+    tet_vol = np.abs(np.linalg.det(np.transpose(bpos[btets[:, 1:]] - bpos[btets[:, :1]], (0, 2, 1)))) / 6.0
+    btris = boundary_faces(btets)
+    P = 0
+    for b in range(nb):
+        i, j, k = b % lattice, (b // lattice) % lattice, b // (lattice * lattice)
+        Rm = random_rotation(rng)
+        rest = bpos @ Rm.T
+        c = np.array([x0 + pitch * i, 0.0, x0 + pitch * k])
+        c[1] = top + rng.uniform(2e-4, 8e-4) - rest[:, 1].min() + pitch * j
+        rest = rest + c  # rest shape in world coordinates (x = A xbar + t, q = (0, I) at rest)
+        m = np.zeros(rest.shape[0])
+        np.add.at(m, btets.reshape(-1), np.repeat(rho * tet_vol / 4.0, 4))
+        A = np.eye(3) + rng.uniform(-warp, warp, size=(3, 3))
+        low = rest[np.argmin(rest[:, 1])]
+        t = low - A @ low  # the lowest point stays where it is
+        xbar.append(rest)
+        point_body.append(np.full(rest.shape[0], b, np.int32))
+        tris.append(btris + P)
+        masses_all.append(m)
+        vols.append(float(tet_vol.sum()))
+        q.append(np.concatenate([t, A.reshape(-1)]))
+        P += rest.shape[0]
+        start.append(P)
+    xbar = np.concatenate(xbar)
+    point_body = np.concatenate(point_body)
+    q = np.stack(q)
+    mass = np.zeros((nb, 13))
+    for b in range(nb):
+        xb, m = xbar[start[b]:start[b + 1]], masses_all[b]
+        mass[b, 0] = m.sum()
+        mass[b, 1:4] = (m[:, None] * xb).sum(0)
+        mass[b, 4:] = (m[:, None, None] * xb[:, :, None] * xb[:, None, :]).sum(0).reshape(-1)
+    q_tilde = q.copy()
+    q_tilde[:, 1] += -9.8 * dt * dt
+    fem = _assemble(f"slab{slab_n}x{slab_layers}", srest, srest.copy(), stets, np.full(stets.shape[0], E), nu, rho,
+                    dt, np.zeros_like(srest), barriers=[((0.0, 1.0, 0.0), 0.0, np.sqrt(dhat), kappa)])
+    # contacts between the bodies and the slab's top, over the point numbering
+    xa = np.einsum("pij,pj->pi", q[point_body, 3:].reshape(-1, 3, 3), xbar) + q[point_body, :3]
+    allpos = np.concatenate([xa, srest])
+    body_of = np.concatenate([point_body.astype(np.int64), np.full(srest.shape[0], nb, np.int64)])
+    alltris = np.concatenate([np.concatenate(tris), boundary_faces(stets) + P])
+    band = allpos[alltris].min(axis=1)[:, 1] < top + 0.02
+    pairs = contact_pairs(allpos, alltris[band], body_of, dhat)
+    return AbdScene(name=f"abd{nb}_slab{slab_n}", q=q, q_tilde=q_tilde, mass=mass, volume=np.array(vols),
+                    kappa=kappa_abd, dt=dt, point_body=point_body, xbar=xbar,
+                    body_point_start=np.array(start, np.int32), fem=fem, contacts=pairs, dhat=dhat,
+                    kappa_contact=kappa)
