@@ -7,7 +7,9 @@ oracle/abd_oracle.py (rows / cols bit-exact, values to 1e-12 of their block's sc
 projection's eigen-solvers differ, 1e-9 there); the coupled FP64 MAS-PCG solve, with the ABD
 block-Jacobi built on the device from the BCOO, at the oracle's iteration count and within
 1e-8 of its x; the FP32-storage solve (relative-residual stop at 1e-4) to an FP64 true residual
-<= 1.5e-4 and within 1e-3 of the oracle's converged x.
+<= 1.5e-4, with an error against the converged x no more than 3x that of the oracle's FP64 solve
+stopped at the same relative residual (the error at a 1e-4 residual is set by the system's
+conditioning, not by the storage precision), and an iteration count within 20 % of it.
 """
 import functools
 
@@ -99,5 +101,11 @@ def test_abd512_slab_coupled_solve(dev, precision):
     else:
         # FP32 storage, FP64 dots and residual replacement: the FP64 true residual
         assert st["rel_residual"] <= 1.5e-4
+        # as accurate as the oracle's FP64 solve stopped at the same relative residual
         xt, _ = orc.pcg(r, c, bl, bh, mas=om, fem_offset=4 * N, abd_bodies=N, abd_inv=ai, tol=1e-12)
-        assert np.linalg.norm(xg - xt) <= 1e-3 * np.linalg.norm(xt)
+        x64, st64, _, done = orc.pcg_timed(r, c, bl, bh, mas=om, fem_offset=4 * N, tol=1e-4, stop_rule="relative",
+                                           abd_bodies=N, abd_inv=ai)
+        assert done
+        e64 = np.linalg.norm(x64 - xt)
+        assert np.linalg.norm(xg - xt) <= 3.0 * e64 + 1e-6 * np.linalg.norm(xt)
+        assert abs(st["iterations"] - st64["iterations"]) <= max(4, st64["iterations"] // 5)
