@@ -308,6 +308,22 @@ int stg_abd_points(int abd_points, const int32_t* point_body, const double* xbar
 int stg_abd_gather_gradient(int bodies, const int32_t* body_point_start, const double* xbar,
                             const double* point_grad, double* body_grad, void* stream);
 
+/* ---- continuous collision detection (line-search step bound) ------------------------------ */
+/* Replaces GIPC::self_largestFeasibleStepSize and _reduct_min_selfTimeStep_to_double
+ * (StiffGIPC/GIPC.cu:7095-7180, 9010-9047) with the reference's additive CCD per pair
+ * (point_triangle_ccd, edge_edge_ccd and their distance classification, ACCD.cu:15-534).
+ * pairs: device int32[4 npairs], point-triangle as (-p-1, t0, t1, t2), edge-edge as
+ * (a0, a1, b0, b1); x, dx: device double[3 num_verts], positions and the step's displacement
+ * (the reference passes -moveDir).  Each pair's time of impact toc in [0, 1] uses
+ * eta = 1 - slackness (the reference calls it with slackness 0.8) and `thickness` (0 there);
+ * *alpha (device double) = 1 / max over pairs of 1 / toc, 1 with no pairs.  toc (device
+ * double[npairs], may be NULL) receives every pair's value; *bad (device int, may be NULL;
+ * added to) counts pairs with a vertex outside [0, num_verts), which impose no bound.
+ * scratch: one device unsigned long long the call owns until it completes.  Asynchronous. */
+int stg_ccd_step_size(int npairs, const int32_t* pairs, const double* x, const double* dx, int num_verts,
+                      double slackness, double thickness, double* alpha, double* toc, int* bad,
+                      unsigned long long* scratch, void* stream);
+
 /* ---- independent scenes in one solve ---------------------------------------------------- */
 /* No counterpart in the reference.  The system of the following solves is a block-diagonal
  * batch of independent scenes on contiguous block-row ranges [row_offsets[s],

@@ -72,6 +72,10 @@ def lib():
         L.orc_contact_barrier.argtypes = [C.c_int, _i32p, _f64p, C.c_int, C.c_int, C.c_double, C.c_double, _i32p,
                                           _i32p, _f64p, _f64p]
         L.orc_contact_barrier.restype = C.c_int
+        L.orc_accd.argtypes = [C.c_int, _f64p, _f64p, C.c_double, C.c_double]
+        L.orc_accd.restype = C.c_double
+        L.orc_ccd_step_size.argtypes = [C.c_int, _i32p, _f64p, _f64p, C.c_double]
+        L.orc_ccd_step_size.restype = C.c_double
         L.orc_contact_d2.argtypes = [C.c_int, _f64p, _f64p]
         L.orc_contact_d2.restype = C.c_double
         L.orc_pcg_ex.argtypes = [_i32p, _i32p, _f64p, C.c_int, C.c_int, _f64p, _f64p, C.c_void_p, C.c_int, C.c_int,
@@ -279,3 +283,16 @@ def contact_d2(kind, v):
     w[:v.size] = v
     g = np.zeros(12)
     return float(lib().orc_contact_d2(int(kind), w, g)), g
+
+
+def accd(kind, x, dx, eta, thickness=0.0):
+    """Time of impact of one pair (kind 0 point-triangle, 1 edge-edge); x, dx: [4, 3]."""
+    return float(lib().orc_accd(int(kind), np.ascontiguousarray(x, np.float64).reshape(-1),
+                                np.ascontiguousarray(dx, np.float64).reshape(-1), float(eta), float(thickness)))
+
+
+def ccd_step_size(pairs, x, dx, slackness=0.8):
+    """The line search's step bound over CCD pairs (GIPC::self_largestFeasibleStepSize)."""
+    pairs = np.ascontiguousarray(pairs, np.int32).reshape(-1, 4)
+    return float(lib().orc_ccd_step_size(pairs.shape[0], pairs.reshape(-1), np.ascontiguousarray(x, np.float64).reshape(-1),
+                                         np.ascontiguousarray(dx, np.float64).reshape(-1), float(slackness)))

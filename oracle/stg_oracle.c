@@ -1603,3 +1603,218 @@ int orc_contact_barrier(int ncp, const int32_t* pairs, const double* x, int nv, 
 
 /* d^2 of one pair of type 0 PP, 1 PE, 2 PT, 3 EE and its gradient g[12] (test access) */
 double orc_contact_d2(int type, const double* v, double* g) { return contact_d2(type, v, g); }
+
+/* ---- additive CCD (line-search step bound) ----------------------------------------------
+ * Restates the reference's conservative-advancement CCD (StiffGIPC/ACCD.cu:15-262 distance
+ * classification, :264-371 unclassified squared distances, :373-534 edge_edge_ccd /
+ * point_triangle_ccd) and the step bound of GIPC::self_largestFeasibleStepSize
+ * (GIPC.cu:7095-7180, 9010-9047): per pair the time of impact toc along the displacement,
+ * eta = 1 - slackness, thickness 0 in the reference's call; alpha = 1 / max(1 / toc).
+ * Every expression keeps the operand order of the reference's vector helpers
+ * (gpu_eigen_libs.cu: dot and squared norm summed x, y, z; the 3x3 determinant as a sum of six
+ * triple products), so that the device restatement (ccd.cu, compiled without FMA contraction)
+ * can be compared bit for bit. */
+typedef struct { double x, y, z; } cv3;
+static cv3 c3(double x, double y, double z) { cv3 r = {x, y, z}; return r; }
+static cv3 c3sub(cv3 a, cv3 b) { return c3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static cv3 c3add(cv3 a, cv3 b) { return c3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static cv3 c3mul(cv3 a, double s) { return c3(a.x * s, a.y * s, a.z * s); }
+static double c3dot(cv3 a, cv3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static double c3sq(cv3 a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+static cv3 c3cross(cv3 a, cv3 b) { return c3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+/* det of the matrix with columns (c0, c1, c2) given row-wise as m[r][k] = ck.r */
+static double cdet(const double m[3][3])
+{
+    return m[0][0] * m[1][1] * m[2][2] + m[1][0] * m[2][1] * m[0][2] + m[2][0] * m[0][1] * m[1][2] -
+           m[2][0] * m[1][1] * m[0][2] - m[0][0] * m[1][2] * m[2][1] - m[0][1] * m[1][0] * m[2][2];
+}
+static void cset(double m[3][3], cv3 a, cv3 b, cv3 c)
+{
+    m[0][0] = a.x, m[0][1] = b.x, m[0][2] = c.x;
+    m[1][0] = a.y, m[1][1] = b.y, m[1][2] = c.y;
+    m[2][0] = a.z, m[2][1] = b.z, m[2][2] = c.z;
+}
+/* barycentric-like parameters of p against edge (a, b) of a triangle with normal n */
+static void pt_param(cv3 p, cv3 a, cv3 b, cv3 n, double* px, double* py)
+{
+    const cv3 b0 = c3sub(b, a), b1 = c3cross(b0, n), b2 = c3sub(p, a);
+    double D[3][3], D1[3][3], D2[3][3];
+    cset(D, b0, b1, n), cset(D1, b2, b1, n), cset(D2, b0, b2, n);
+    *px = cdet(D1) / cdet(D);
+    *py = cdet(D2) / cdet(D);
+}
+/* 0..2 vertex t_k, 3..5 edges (t0 t1), (t1 t2), (t2 t0), 6 interior */
+static int pt_type(cv3 p, cv3 t0, cv3 t1, cv3 t2)
+{
+    const cv3 n = c3cross(c3sub(t1, t0), c3sub(t2, t0));
+    double x0, y0, x1, y1, x2, y2;
+    pt_param(p, t0, t1, n, &x0, &y0);
+    if(x0 > 0 && x0 < 1 && y0 >= 0) return 3;
+    pt_param(p, t1, t2, n, &x1, &y1);
+    if(x1 > 0.0 && x1 < 1.0 && y1 >= 0.0) return 4;
+    pt_param(p, t2, t0, n, &x2, &y2);
+    if(x2 > 0.0 && x2 < 1.0 && y2 >= 0.0) return 5;
+    if(x0 <= 0.0 && x2 >= 1.0) return 0;
+    if(x1 <= 0.0 && x0 >= 1.0) return 1;
+    if(x2 <= 0.0 && x1 >= 1.0) return 2;
+    return 6;
+}
+/* 0..8: (a0 b0) (a0 b1) (a0 | b) (a1 b0) (a1 b1) (a1 | b) (b0 | a) (b1 | a) (a | b) */
+static int ee_type(cv3 v0, cv3 v1, cv3 v2, cv3 v3)
+{
+    const cv3 u = c3sub(v1, v0), v = c3sub(v3, v2), w = c3sub(v0, v2);
+    const double a = c3sq(u), b = c3dot(u, v), c = c3sq(v), d = c3dot(u, w), e = c3dot(v, w);
+    const double D = a * c - b * b;
+    double tD = D, tN;
+    int dflt = 8;
+    const double sN = (b * e - c * d);
+    if(sN <= 0.0)
+        tN = e, tD = c, dflt = 2;
+    else if(sN >= D)
+        tN = e + b, tD = c, dflt = 5;
+    else
+    {
+        tN = (a * e - b * d);
+        if(tN > 0.0 && tN < tD && (c3dot(w, c3cross(u, v)) == 0.0 || c3sq(c3cross(u, v)) < 1.0e-20 * a * c))
+        {
+            if(sN < D / 2)
+                tN = e, tD = c, dflt = 2;
+            else
+                tN = e + b, tD = c, dflt = 5;
+        }
+    }
+    if(tN <= 0.0) return -d <= 0.0 ? 0 : (-d >= a ? 3 : 6);
+    if(tN >= tD) return (-d + b) <= 0.0 ? 1 : ((-d + b) >= a ? 4 : 7);
+    return dflt;
+}
+static double d_pp(cv3 a, cv3 b) { return c3sq(c3sub(a, b)); }
+static double d_pe(cv3 p, cv3 e0, cv3 e1) { return c3sq(c3cross(c3sub(e0, p), c3sub(e1, p))) / c3sq(c3sub(e1, e0)); }
+static double d_pt(cv3 p, cv3 t0, cv3 t1, cv3 t2)
+{
+    const cv3 b = c3cross(c3sub(t1, t0), c3sub(t2, t0));
+    const double aTb = c3dot(c3sub(p, t0), b);
+    return aTb * aTb / c3sq(b);
+}
+static double d_ee(cv3 a0, cv3 a1, cv3 b0, cv3 b1)
+{
+    const cv3 b = c3cross(c3sub(a1, a0), c3sub(b1, b0));
+    const double aTb = c3dot(c3sub(b0, a0), b);
+    return aTb * aTb / c3sq(b);
+}
+static double ee_dist2(cv3 a0, cv3 a1, cv3 b0, cv3 b1)
+{
+    switch(ee_type(a0, a1, b0, b1))
+    {
+        case 0: return d_pp(a0, b0);
+        case 1: return d_pp(a0, b1);
+        case 2: return d_pe(a0, b0, b1);
+        case 3: return d_pp(a1, b0);
+        case 4: return d_pp(a1, b1);
+        case 5: return d_pe(a1, b0, b1);
+        case 6: return d_pe(b0, a0, a1);
+        case 7: return d_pe(b1, a0, a1);
+        default: return d_ee(a0, a1, b0, b1);
+    }
+}
+static double pt_dist2(cv3 p, cv3 t0, cv3 t1, cv3 t2)
+{
+    switch(pt_type(p, t0, t1, t2))
+    {
+        case 0: return d_pp(p, t0);
+        case 1: return d_pp(p, t1);
+        case 2: return d_pp(p, t2);
+        case 3: return d_pe(p, t0, t1);
+        case 4: return d_pe(p, t1, t2);
+        case 5: return d_pe(p, t2, t0);
+        default: return d_pt(p, t0, t1, t2);
+    }
+}
+static double ee_floor(cv3 a0, cv3 a1, cv3 b0, cv3 b1)
+{
+    const double s0 = c3sq(c3sub(a0, b0)), s1 = c3sq(c3sub(a0, b1)), s2 = c3sq(c3sub(a1, b0)),
+                 s3 = c3sq(c3sub(a1, b1));
+    return fmin(fmin(s0, s1), fmin(s2, s3));
+}
+
+/* time of impact of points x[0..3] moving by dx[0..3]: type 0 point-triangle (p, t0, t1, t2),
+ * 1 edge-edge (a0, a1, b0, b1) */
+double orc_accd(int type, const double* x, const double* dx, double eta, double thickness)
+{
+    cv3 v[4], d[4];
+    for(int i = 0; i < 4; i++) v[i] = c3(x[3 * i], x[3 * i + 1], x[3 * i + 2]), d[i] = c3(dx[3 * i], dx[3 * i + 1], dx[3 * i + 2]);
+    const double th2 = thickness * thickness;
+    if(type == 1)
+    {
+        const cv3 mov = c3mul(c3add(c3add(d[0], d[1]), c3add(d[2], d[3])), -0.25);
+        for(int i = 0; i < 4; i++) d[i] = c3add(d[i], mov);
+        const double mdm = sqrt(fmax(c3sq(d[0]), c3sq(d[1]))) + sqrt(fmax(c3sq(d[2]), c3sq(d[3])));
+        if(mdm == 0) return 1.0;
+        double dist2 = ee_dist2(v[0], v[1], v[2], v[3]);
+        double dF = dist2 - th2;
+        if(dF <= 0)
+        {
+            dist2 = ee_floor(v[0], v[1], v[2], v[3]);
+            dF = dist2 - th2;
+        }
+        double dist = sqrt(dist2);
+        const double gap = eta * dF / (dist + thickness);
+        double toc = 0.0;
+        for(int count = 1;; count++)
+        {
+            if(count > 50000) return toc;
+            const double lb = (1 - eta) * dF / ((dist + thickness) * mdm);
+            for(int i = 0; i < 4; i++) v[i] = c3add(v[i], c3mul(d[i], lb));
+            dist2 = ee_dist2(v[0], v[1], v[2], v[3]);
+            dF = dist2 - th2;
+            if(dF <= 0)
+            {
+                dist2 = ee_floor(v[0], v[1], v[2], v[3]);
+                dF = dist2 - th2;
+            }
+            dist = sqrt(dist2);
+            if(toc != 0.0 && (dF / (dist + thickness) < gap)) break;
+            toc += lb;
+            if(toc > 1.0) return 1.0;
+        }
+        return toc;
+    }
+    const cv3 mov = c3mul(c3add(c3add(d[1], d[2]), c3add(d[3], d[0])), -0.25);
+    for(int i = 0; i < 4; i++) d[i] = c3add(d[i], mov);
+    const double mdm = sqrt(c3sq(d[0])) + sqrt(fmax(c3sq(d[1]), fmax(c3sq(d[2]), c3sq(d[3]))));
+    if(mdm == 0) return 1.0;
+    double dist2 = pt_dist2(v[0], v[1], v[2], v[3]);
+    double dist = sqrt(dist2);
+    const double gap = eta * (dist2 - th2) / (dist + thickness);
+    double toc = 0.0;
+    for(int count = 1;; count++)
+    {
+        if(count > 50000) return toc;
+        const double lb = (1 - eta) * (dist2 - th2) / ((dist + thickness) * mdm);
+        for(int i = 0; i < 4; i++) v[i] = c3add(v[i], c3mul(d[i], lb));
+        dist2 = pt_dist2(v[0], v[1], v[2], v[3]);
+        dist = sqrt(dist2);
+        if(toc != 0.0 && ((dist2 - th2) / (dist + thickness) < gap)) break;
+        toc += lb;
+        if(toc > 1.0) return 1.0;
+    }
+    return toc;
+}
+
+/* the largest feasible step of displacement dx for the CCD pairs (x < 0: point -x-1 and
+ * triangle (y, z, w); else edges (x, y), (z, w)): 1 / max over pairs of 1 / toc, or 1 */
+double orc_ccd_step_size(int npairs, const int32_t* pairs, const double* x, const double* dx, double slackness)
+{
+    if(npairs < 1) return 1.0;
+    double mx = 0.0;
+    for(int p = 0; p < npairs; p++)
+    {
+        const int32_t* q = pairs + 4 * (size_t)p;
+        const int id[4] = {q[0] < 0 ? -q[0] - 1 : q[0], q[1], q[2], q[3]};
+        double xs[12], ds[12];
+        for(int i = 0; i < 4; i++)
+            for(int k = 0; k < 3; k++) xs[3 * i + k] = x[3 * (size_t)id[i] + k], ds[3 * i + k] = dx[3 * (size_t)id[i] + k];
+        const double t = 1.0 / orc_accd(q[0] < 0 ? 0 : 1, xs, ds, 1.0 - slackness, 0.0);
+        if(!(t <= mx)) mx = t;
+    }
+    return 1.0 / mx;
+}

@@ -22,13 +22,18 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", 
          "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 
 
+# per-file flags: the CCD step bound is compared bit for bit with the oracle, so its kernels
+# keep every multiply and add separately rounded
+EXTRA = {"ccd.cu": ["-fmad=false"]}
+
+
 def sources():
     return sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
 
 
 def _compile(src: str, verbose: bool) -> str:
     obj = os.path.join(OUT, src[:-3] + ".o")
-    cmd = [NVCC, *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+    cmd = [NVCC, *ARCH, *FLAGS, *EXTRA.get(src, []), "-c", os.path.join(CSRC, src), "-o", obj]
     if verbose:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)
