@@ -268,6 +268,12 @@ int stg_fem_energy(int verts, const double* rest, const double* pos, const doubl
 int stg_contact_barrier(int ncp, const int32_t* pairs, const double* x, int num_verts, int block_offset,
                         double dhat, double kappa, int32_t* rows, int32_t* cols, double* blocks,
                         double* grad, int* skipped, void* stream);
+/* The energies of the same pairs: energy[p] = kappa dhat^2 (s^2 - 1)^2 ln^2(s^2) for s < 1,
+ * else 0 (also 0 for the pairs stg_contact_barrier skips) -- the barrier term of the
+ * incremental potential the line search evaluates (GIPC::computeEnergy, the RANK 2 barrier).
+ * energy: device double[ncp]; asynchronous. */
+int stg_contact_energy(int ncp, const int32_t* pairs, const double* x, int num_verts, double dhat,
+                       double kappa, double* energy, void* stream);
 
 /* ---- affine bodies (ABD) ---------------------------------------------------------------- */
 /* Body b owns block rows 4 b .. 4 b + 3; q[12 b ..] = (t, a1, a2, a3) with a_i the rows of A

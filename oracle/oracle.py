@@ -76,6 +76,8 @@ def lib():
         L.orc_accd.restype = C.c_double
         L.orc_ccd_step_size.argtypes = [C.c_int, _i32p, _f64p, _f64p, C.c_double]
         L.orc_ccd_step_size.restype = C.c_double
+        L.orc_contact_energy.argtypes = [C.c_int, _i32p, _f64p, C.c_int, C.c_double, C.c_double, _f64p]
+        L.orc_contact_energy.restype = None
         L.orc_contact_d2.argtypes = [C.c_int, _f64p, _f64p]
         L.orc_contact_d2.restype = C.c_double
         L.orc_pcg_ex.argtypes = [_i32p, _i32p, _f64p, C.c_int, C.c_int, _f64p, _f64p, C.c_void_p, C.c_int, C.c_int,
@@ -296,3 +298,12 @@ def ccd_step_size(pairs, x, dx, slackness=0.8):
     pairs = np.ascontiguousarray(pairs, np.int32).reshape(-1, 4)
     return float(lib().orc_ccd_step_size(pairs.shape[0], pairs.reshape(-1), np.ascontiguousarray(x, np.float64).reshape(-1),
                                          np.ascontiguousarray(dx, np.float64).reshape(-1), float(slackness)))
+
+
+def contact_energy(pairs, x, dhat, kappa):
+    """Per-pair barrier energies of the sign-encoded pairs at positions x [V, 3]."""
+    pairs = np.ascontiguousarray(pairs, np.int32).reshape(-1, 4)
+    x = np.ascontiguousarray(x, np.float64).reshape(-1, 3)
+    e = np.zeros(pairs.shape[0])
+    lib().orc_contact_energy(pairs.shape[0], pairs.reshape(-1), x.reshape(-1), x.shape[0], float(dhat), float(kappa), e)
+    return e

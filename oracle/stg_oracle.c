@@ -1818,3 +1818,45 @@ double orc_ccd_step_size(int npairs, const int32_t* pairs, const double* x, cons
     }
     return 1.0 / mx;
 }
+
+/* the barrier energy of each pair (kappa dhat^2 (s^2 - 1)^2 ln^2(s^2), s^2 = d^2 / dhat < 1) */
+void orc_contact_energy(int ncp, const int32_t* pairs, const double* x, int nv, double dhat, double kappa,
+                        double* energy)
+{
+    for(int p = 0; p < ncp; p++)
+    {
+        const int32_t* q = pairs + 4 * (size_t)p;
+        int vid[4] = {0, 0, 0, 0}, cnt = 0, type = -1;
+        if(q[0] >= 0)
+        {
+            if(q[3] >= 0) type = 3, vid[0] = q[0], vid[1] = q[1], vid[2] = q[2], vid[3] = q[3], cnt = 4;
+        }
+        else if(q[1] >= 0)
+        {
+            vid[0] = -q[0] - 1, vid[1] = q[1];
+            if(q[2] < 0)
+                type = 0, cnt = 2;
+            else if(q[3] < 0)
+                type = 1, vid[2] = q[2], cnt = 3;
+            else
+                type = 2, vid[2] = q[2], vid[3] = q[3], cnt = 4;
+        }
+        int ok = type >= 0;
+        for(int i = 0; i < cnt; i++) ok = ok && vid[i] >= 0 && vid[i] < nv;
+        for(int i = 0; i < cnt; i++)
+            for(int j = i + 1; j < cnt; j++) ok = ok && vid[i] != vid[j];
+        double e = 0.0;
+        if(ok)
+        {
+            double v[12] = {0}, g[12];
+            for(int i = 0; i < cnt; i++) memcpy(v + 3 * i, x + 3 * (size_t)vid[i], 3 * sizeof(double));
+            const double I = contact_d2(type, v, g) / dhat;
+            if(I < 1.0)
+            {
+                const double l = log(I);
+                e = kappa * dhat * dhat * (I - 1.0) * (I - 1.0) * l * l;
+            }
+        }
+        energy[p] = e;
+    }
+}

@@ -218,7 +218,68 @@ __global__ void k_contact_barrier(int ncp, const int4* __restrict__ pairs, const
         }
 }
 
+// per-pair barrier energy kappa dHat^2 (s^2 - 1)^2 ln^2(s^2) for s < 1 (the reference's
+// barrier at RANK 2, GIPC.cu:3226-3230 integrated); unsupported or invalid pairs give 0
+__global__ void k_contact_energy(int ncp, const int4* __restrict__ pairs, const double* __restrict__ x, int nv,
+                                 double dhat, double kappa, double* energy)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= ncp) return;
+    const int4 q = pairs[p];
+    int vid[4] = {0, 0, 0, 0}, cnt = 0, type = -1;
+    if(q.x >= 0)
+    {
+        if(q.w >= 0) type = 3, vid[0] = q.x, vid[1] = q.y, vid[2] = q.z, vid[3] = q.w, cnt = 4;
+    }
+    else if(q.y >= 0)
+    {
+        vid[0] = -q.x - 1, vid[1] = q.y;
+        if(q.z < 0)
+            type = 0, cnt = 2;
+        else if(q.w < 0)
+            type = 1, vid[2] = q.z, cnt = 3;
+        else
+            type = 2, vid[2] = q.z, vid[3] = q.w, cnt = 4;
+    }
+    bool ok = type >= 0;
+    for(int i = 0; i < cnt; i++) ok = ok && vid[i] >= 0 && vid[i] < nv;
+    for(int i = 0; i < cnt; i++)
+        for(int j = i + 1; j < cnt; j++) ok = ok && vid[i] != vid[j];
+    double e = 0.0;
+    if(ok)
+    {
+        DVec v[4];
+        for(int i = 0; i < 4; i++)
+        {
+            const int g = vid[i < cnt ? i : 0];
+            v[i] = {dconst(x[3 * (size_t)g]), dconst(x[3 * (size_t)g + 1]), dconst(x[3 * (size_t)g + 2])};
+        }
+        const double I = squared_distance(type, v).v / dhat;
+        if(I < 1.0)
+        {
+            const double l = log(I);
+            e = kappa * dhat * dhat * (I - 1.0) * (I - 1.0) * l * l;
+        }
+    }
+    energy[p] = e;
+}
+
 }  // namespace stg
+
+extern "C" int stg_contact_energy(int ncp, const int32_t* pairs, const double* x, int num_verts, double dhat,
+                                  double kappa, double* energy, void* stream)
+{
+    if(ncp < 0 || num_verts < 0 || !(dhat > 0.0) || !(kappa >= 0.0) || (ncp > 0 && (!pairs || !x || !energy)))
+    {
+        stg::set_error("stg_contact_energy: invalid arguments");
+        return STG_ERR_INVALID;
+    }
+    if(ncp == 0) return STG_OK;
+    stg::k_contact_energy<<<(ncp + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        ncp, reinterpret_cast<const int4*>(pairs), x, num_verts, dhat, kappa, energy);
+    STG_CUDA_TRY(cudaGetLastError());
+    return STG_OK;
+}
 
 extern "C" int stg_contact_barrier(int ncp, const int32_t* pairs, const double* x, int num_verts, int block_offset,
                                    double dhat, double kappa, int32_t* rows, int32_t* cols, double* blocks,

@@ -61,3 +61,14 @@ def scatter_gradient(pairs, grad, num_verts: int):
     out = torch.zeros(num_verts, 3, dtype=grad.dtype, device=grad.device)
     out.index_add_(0, vid[valid], g[valid])
     return out
+
+
+def energy(pairs, x, dhat: float, kappa: float, stream=None):
+    """Per-pair barrier energies [P] (device float64) of the pairs at positions x."""
+    import torch
+    pairs, x = pairs.contiguous().view(-1, 4), x.contiguous().view(-1, 3)
+    e = torch.empty(pairs.shape[0], dtype=torch.float64, device=x.device)
+    s = None if stream is None else stream.cuda_stream
+    check(_L.lib().stg_contact_energy(pairs.shape[0], pairs.data_ptr(), x.data_ptr(), x.shape[0], float(dhat),
+                                      float(kappa), e.data_ptr(), s), "stg_contact_energy")
+    return e

@@ -7,7 +7,11 @@ Each Newton iteration builds the incremental potential's triplets and gradient o
 barrier planes (vertex-plane time of impact, scaled by 0.8 as IPC's CCD does), and
 backtracks until the potential decreases and no vertex reaches a plane.  A step ends when
 the direction's largest entry, divided by dt, falls below tol (IPC's Newton criterion).
-Only plane barriers are modelled: the synthetic scenes have no triangle contacts.
+With a ContactModel the potential also carries the IPC barrier of the point-triangle /
+edge-edge / point-edge / point-point pairs between the surfaces (stgipc.contact: its
+triplets join the system, its pairs the MAS connectivity), and the step is also bounded by
+the additive CCD of the swept surface pairs (stgipc.ccd, GIPC::self_largestFeasibleStepSize
+with slackness 0.8).  The pair sets come from the host-side search of stgipc.scenes.
 """
 from __future__ import annotations
 
@@ -25,6 +29,34 @@ class StepStats:
     pcg_iterations: List[int]
     line_search_halvings: int
     min_plane_distance: float
+    min_contact_distance: float = float("inf")
+    contacts: int = 0
+    ccd_alpha: float = 1.0
+
+
+@dataclasses.dataclass
+class ContactModel:
+    """Surface contact between bodies: surface triangles (vertex ids), a body id per vertex
+    (pairs within one body are ignored; None: every pair sharing no vertex), the squared
+    activation distance dhat and the barrier stiffness kappa."""
+    tris: np.ndarray
+    body: Optional[np.ndarray]
+    dhat: float
+    kappa: float
+
+    def pairs(self, x_host):
+        from . import scenes
+        body = self.body if self.body is not None else np.arange(x_host.shape[0])
+        return scenes.contact_pairs(x_host, self.tris, body, self.dhat, return_d2=True)
+
+    def energy(self, x):
+        """The barrier energy at device positions x [V, 3] (pairs searched at x)."""
+        import torch
+        from . import contact
+        p, _ = self.pairs(x.cpu().numpy())
+        if p.shape[0] == 0:
+            return 0.0
+        return float(contact.energy(torch.from_numpy(p).to(x.device), x, self.dhat, self.kappa).sum())
 
 
 def plane_step_bound(scene: FemScene, x, p) -> float:
@@ -49,30 +81,57 @@ def min_plane_distance(scene: FemScene, x) -> float:
     return float(d.min())
 
 
-def step(scene: FemScene, solver, tol: float = 1e-6, max_newton: int = 30) -> StepStats:
+def step(scene: FemScene, solver, tol: float = 1e-6, max_newton: int = 30,
+         contact: Optional[ContactModel] = None) -> StepStats:
     """One implicit-Euler step of `scene` (positions and velocities updated in place) with
     the linear solves of `solver` (stgipc.Solver, MAS initialised for the mesh)."""
     import torch
+    from . import ccd
+    from . import contact as cmod
+    from . import scenes
     dt = scene.dt
-    g = torch.tensor([0.0, scene.gy, 0.0], dtype=torch.float64, device=scene.device)
+    dev = scene.device
+    g = torch.tensor([0.0, scene.gy, 0.0], dtype=torch.float64, device=dev)
     x_n = scene.pos.clone()
     xtilde = (x_n + dt * scene.vel + dt * dt * g).contiguous()
     x = x_n.clone()
-    dx = torch.zeros(3 * scene.V, dtype=torch.float64, device=scene.device)
-    pcg, halvings, it = [], 0, 0
+    dx = torch.zeros(3 * scene.V, dtype=torch.float64, device=dev)
+    pcg, halvings, it, ncont, amin = [], 0, 0, 0, 1.0
+
+    def potential(xx):
+        e, viol = scene.energy(xx, xtilde)
+        return (e + (contact.energy(xx) if contact is not None else 0.0)), viol
+
     for it in range(1, max_newton + 1):
         scene.assemble(x, xtilde)
+        rows, cols, blocks, b, P = scene.rows, scene.cols, scene.blocks, scene.b, None
+        if contact is not None:
+            pairs, _ = contact.pairs(x.cpu().numpy())
+            ncont = max(ncont, pairs.shape[0])
+            if pairs.shape[0]:
+                P = torch.from_numpy(pairs).to(dev)
+                cr, cc, cb, cg, sk = cmod.barrier(P, x, contact.dhat, contact.kappa)
+                rows, cols = torch.cat([rows, cr]), torch.cat([cols, cc])
+                blocks = torch.cat([blocks, cb.reshape(-1)])
+                b = b + cmod.scatter_gradient(P, cg, scene.V).reshape(-1)
         dx.zero_()
-        st = solver.solve_linear_system(scene.rows, scene.cols, scene.blocks, scene.b, dx)
+        st = solver.solve_linear_system(rows, cols, blocks, b, dx, contacts=P)
         pcg.append(st["iterations"])
         p = (-dx).view(scene.V, 3)
         if float(p.abs().max()) / dt < tol:
             break
         alpha = plane_step_bound(scene, x, p)
-        e0, _ = scene.energy(x, xtilde)
+        if contact is not None:
+            cp = scenes.ccd_candidates(x.cpu().numpy(), p.cpu().numpy(), contact.tris, contact.body,
+                                       pad=float(np.sqrt(contact.dhat)))
+            if cp.shape[0]:
+                a_ccd = float(ccd.step_size(torch.from_numpy(cp).to(dev), x, p.contiguous(), slackness=0.8).item())
+                amin = min(amin, a_ccd)
+                alpha = min(alpha, a_ccd)
+        e0, _ = potential(x)
         for _ in range(40):
             xn = (x + alpha * p).contiguous()
-            e1, viol = scene.energy(xn, xtilde)
+            e1, viol = potential(xn)
             if viol == 0 and e1 <= e0:
                 break
             alpha *= 0.5
@@ -80,7 +139,12 @@ def step(scene: FemScene, solver, tol: float = 1e-6, max_newton: int = 30) -> St
         x = xn
     scene.vel = ((x - x_n) / dt).contiguous()
     scene.pos = x.contiguous()
-    return StepStats(it, pcg, halvings, min_plane_distance(scene, x))
+    dmin = float("inf")
+    if contact is not None:
+        _, d2 = contact.pairs(x.cpu().numpy())
+        if d2.size:
+            dmin = float(np.sqrt(d2.min()))
+    return StepStats(it, pcg, halvings, min_plane_distance(scene, x), dmin, ncont, amin)
 
 
 def save_checkpoint(path: str, positions, velocities, step: int):
@@ -101,11 +165,11 @@ def resume_state(state: dict, path: str, step: Optional[int] = None) -> dict:
 
 
 def trajectory(state: dict, steps: int, config=None, tol: float = 1e-6, device="cuda", bank: int = 16,
-               solver_hook=None, checkpoint: Optional[str] = None):
+               solver_hook=None, checkpoint: Optional[str] = None, contact: Optional[ContactModel] = None):
     """Run `steps` implicit-Euler steps from a scene state (stgipc.scenes ..., state_only=True);
     returns (positions after each step as host arrays, step statistics).  With
     `checkpoint`, positions and velocities of every step are written there after each step
-    (resume with resume_state)."""
+    (resume with resume_state).  contact: surface contact (ContactModel)."""
     from . import scenes
     from .linear_system import PCGSolverConfig, Solver
     scene = FemScene(state, device=device)
@@ -118,7 +182,7 @@ def trajectory(state: dict, steps: int, config=None, tol: float = 1e-6, device="
         solver_hook(solver)
     out, vels, stats = [], [], []
     for k in range(steps):
-        stats.append(step(scene, solver, tol))
+        stats.append(step(scene, solver, tol, contact=contact))
         out.append(scene.pos.cpu().numpy().copy())
         vels.append(scene.vel.cpu().numpy().copy())
         if checkpoint:

@@ -505,15 +505,18 @@ def _pt_type(p, t0, t1, t2):
     return out
 
 
-def contact_pairs(pos: np.ndarray, tris: np.ndarray, body: np.ndarray, dhat: float, mollify_eps: float = 1e-3):
+def contact_pairs(pos: np.ndarray, tris: np.ndarray, body: np.ndarray, dhat: float, mollify_eps: float = 1e-3,
+                  return_d2: bool = False):
     """Sign-encoded int4 pairs (GIPC.cuh:49-66) between the surfaces of different bodies
     within distance sqrt(dhat): every (surface vertex, triangle) pair classified by its
     closest feature into PT, PE or PP, and every (edge, edge) pair whose closest points are
     interior to both edges as EE.  Near-parallel edge pairs (|ea x eb|^2 < mollify_eps
     |ea|^2 |eb|^2, the reference's mollifier zone, mlbvh.cu:278-285) and edge pairs whose closest
     points sit at an endpoint are left out.  Duplicates are merged.  Brute force over a
-    uniform grid of cell size max(longest edge, sqrt(dhat)); meant for scene synthesis."""
+    uniform grid of cell size max(longest edge, sqrt(dhat)); meant for scene synthesis and the
+    host side of the Newton driver.  return_d2: also the squared distance of every pair."""
     r = np.sqrt(dhat)
+    dout = []
     edges = face_edges(tris)
     verts = np.unique(tris)
     h = max(float(np.linalg.norm(pos[edges[:, 0]] - pos[edges[:, 1]], axis=1).max()), r) * 1.0001
@@ -579,6 +582,7 @@ def contact_pairs(pos: np.ndarray, tris: np.ndarray, body: np.ndarray, dhat: flo
             d2[mk] = np.einsum("ij,ij->i", dv, dv)
             enc[mk] = np.stack([-p[mk] - 1, t[mk, k], -np.ones(mk.sum(), np.int64), -np.ones(mk.sum(), np.int64)], 1)
         out.append(enc[d2 < dhat])
+        dout.append(d2[d2 < dhat])
     # edge - edge
     i, j = cand(edges, edges)
     keep = (i < j) & (body[edges[i, 0]] != body[edges[j, 0]])
@@ -602,20 +606,26 @@ def contact_pairs(pos: np.ndarray, tris: np.ndarray, body: np.ndarray, dhat: flo
         d2 = np.einsum("ij,ij->i", w, cr) ** 2 / np.where(ok, cr2, 1.0)
         ok &= d2 < dhat
         out.append(np.stack([ea_[ok, 0], ea_[ok, 1], eb_[ok, 0], eb_[ok, 1]], 1))
+        dout.append(d2[ok])
     if not out:
-        return np.zeros((0, 4), np.int32)
-    allp = np.concatenate(out)
-    return np.unique(allp, axis=0).astype(np.int32)
+        return (np.zeros((0, 4), np.int32), np.zeros(0)) if return_d2 else np.zeros((0, 4), np.int32)
+    allp, idx = np.unique(np.concatenate(out), axis=0, return_index=True)
+    if return_d2:
+        return allp.astype(np.int32), np.concatenate(dout)[idx]
+    return allp.astype(np.int32)
 
 
 def make_stacked_cubes(n: int = 8, seed: int = 1006, E: float = 1e5, nu: float = 0.45, rho: float = 1000.0,
                        dt: float = 1.0 / 60.0, size: float = 0.5, gap: float = 4e-4, dhat: float = 1e-6,
-                       kappa: float = 1e5, jitter: float = 1e-5):
+                       kappa: float = 1e5, jitter: float = 1e-5, v0: float = -0.5, v_top: Optional[float] = None,
+                       state_only: bool = False):
     """Two soft cubes, one resting on the other, with the upper one shifted by half a cell in
     x and z so its bottom vertices lie over the lower one's top triangles, ``gap`` m apart
     (inside the barrier's sqrt(dhat)); the lower cube rests ``gap`` above a ground barrier.
     Returns (NewtonSystem of the elastic + inertia + ground terms, contact pairs [C, 4],
-    body id per vertex); the contact barrier terms come from stgipc.contact.barrier."""
+    body id per vertex); the contact barrier terms come from stgipc.contact.barrier.  Both
+    cubes move at v0 in y (the upper one at v_top when given).  state_only: (scene state for stgipc.newton, surface triangles,
+    body id per vertex) instead."""
     rng = np.random.default_rng(seed)
     pa, ta = cube_mesh(n, size, origin=(0.0, gap, 0.0))
     h = size / n
@@ -628,9 +638,15 @@ def make_stacked_cubes(n: int = 8, seed: int = 1006, E: float = 1e5, nu: float =
     body = body[old_of_new]
     E_t = np.full(tets.shape[0], E)
     vel = np.zeros_like(pos)
-    vel[:, 1] = -0.5
-    sysm = _assemble(f"stacked{n}", pos, pos, tets, E_t, nu, rho, dt, vel,
-                     barriers=[((0.0, 1.0, 0.0), 0.0, np.sqrt(dhat), kappa)])
+    vel[:, 1] = v0
+    if v_top is not None:
+        vel[body == 1, 1] = v_top
+    barriers = [((0.0, 1.0, 0.0), 0.0, np.sqrt(dhat), kappa)]
+    if state_only:
+        state = dict(name=f"stacked{n}", pos_rest=pos, pos=pos.copy(), tets=tets, E=E_t, nu=nu, rho=rho, dt=dt,
+                     vel=vel, barriers=barriers)
+        return state, boundary_faces(tets), body
+    sysm = _assemble(f"stacked{n}", pos, pos, tets, E_t, nu, rho, dt, vel, barriers=barriers)
     pairs = contact_pairs(pos, boundary_faces(tets), body, dhat)
     sysm.contacts = pairs
     return sysm, pairs, body
@@ -746,3 +762,61 @@ def make_abd_slab(lattice: int = 8, body_size: float = 0.1, body_n: int = 2, kap
                     kappa=kappa_abd, dt=dt, point_body=point_body, xbar=xbar,
                     body_point_start=np.array(start, np.int32), fem=fem, contacts=pairs, dhat=dhat,
                     kappa_contact=kappa)
+
+
+def _box_pairs(lo_a, hi_a, lo_b, hi_b, pad):
+    """Index pairs (i, j) whose boxes [lo_a, hi_a] and [lo_b - pad, hi_b + pad] overlap, found
+    on a uniform grid whose cell is at least every box's extent."""
+    if lo_a.shape[0] == 0 or lo_b.shape[0] == 0:
+        return np.zeros(0, np.int64), np.zeros(0, np.int64)
+    h = max(float((hi_a - lo_a).max()), float((hi_b - lo_b).max()) + 2 * pad, 1e-12) * 1.0001
+    w = np.array([1 << 42, 1 << 21, 1])
+    ka = (np.floor(lo_a / h).astype(np.int64) + (1 << 20)) @ w
+    order = np.argsort(ka, kind="stable")
+    ks = ka[order]
+    clo = np.floor((lo_b - pad) / h).astype(np.int64) - 1
+    out_i, out_j = [], []
+    for dx in range(3):
+        for dy in range(3):
+            for dz in range(3):
+                kb = (clo + np.array([dx, dy, dz]) + (1 << 20)) @ w
+                lo = np.searchsorted(ks, kb, "left")
+                cnt = np.searchsorted(ks, kb, "right") - lo
+                tot = int(cnt.sum())
+                if tot == 0:
+                    continue
+                first = np.cumsum(cnt) - cnt
+                out_i.append(order[np.repeat(lo, cnt) + np.arange(tot) - np.repeat(first, cnt)])
+                out_j.append(np.repeat(np.arange(cnt.size), cnt))
+    if not out_i:
+        return np.zeros(0, np.int64), np.zeros(0, np.int64)
+    i, j = np.concatenate(out_i), np.concatenate(out_j)
+    ok = np.all(lo_a[i] <= hi_b[j] + pad, axis=1) & np.all(hi_a[i] >= lo_b[j] - pad, axis=1)
+    return i[ok], j[ok]
+
+
+def ccd_candidates(pos: np.ndarray, disp: np.ndarray, tris: np.ndarray, body: Optional[np.ndarray] = None,
+                   pad: float = 0.0) -> np.ndarray:
+    """The CCD pairs of a step (the reference's _ccd_collisonPairs): every (surface vertex,
+    triangle) and (edge, edge) pair whose boxes swept over pos -> pos + disp overlap (within
+    pad), sharing no vertex and, with `body`, of different bodies; point-triangle encoded
+    (-p-1, t0, t1, t2), edge-edge (a0, a1, b0, b1)."""
+    end = pos + disp
+    lo_v, hi_v = np.minimum(pos, end), np.maximum(pos, end)
+    verts = np.unique(tris)
+    edges = face_edges(tris)
+    out = []
+    i, j = _box_pairs(lo_v[verts], hi_v[verts], lo_v[tris].min(axis=1), hi_v[tris].max(axis=1), pad)
+    p, t = verts[i], tris[j]
+    keep = (p != t[:, 0]) & (p != t[:, 1]) & (p != t[:, 2])
+    if body is not None:
+        keep &= body[p] != body[t[:, 0]]
+    out.append(np.stack([-p[keep] - 1, t[keep, 0], t[keep, 1], t[keep, 2]], 1))
+    i, j = _box_pairs(lo_v[edges].min(axis=1), hi_v[edges].max(axis=1), lo_v[edges].min(axis=1),
+                      hi_v[edges].max(axis=1), pad)
+    a, b = edges[i], edges[j]
+    keep = (i < j) & (a[:, 0] != b[:, 0]) & (a[:, 0] != b[:, 1]) & (a[:, 1] != b[:, 0]) & (a[:, 1] != b[:, 1])
+    if body is not None:
+        keep &= body[a[:, 0]] != body[b[:, 0]]
+    out.append(np.concatenate([a[keep], b[keep]], axis=1))
+    return np.concatenate(out).astype(np.int32)

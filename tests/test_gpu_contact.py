@@ -96,3 +96,24 @@ def test_stacked_cubes_solve_with_contacts(dev):
     assert st["total_clusters"] == om.total
     assert st["iterations"] == st_e["iterations"]
     assert np.linalg.norm(X.cpu().numpy() - xe) <= 1e-8 * np.linalg.norm(xe)
+
+
+def test_energy_matches_oracle(dev):
+    """Per-pair barrier energies (stg_contact_energy) against the oracle, within 1e-12 of the
+    largest."""
+    from oracle import oracle as orc
+    from stgipc.contact import energy
+    rng = np.random.default_rng(31)
+    V = 2000
+    x = rng.uniform(0, 1, size=(V, 3))
+    pairs = random_contacts(V, 5000, seed=32, local=8)
+    for q in pairs[:3000]:
+        ids = [(-i - 1) if i < 0 else i for i in q]
+        x[ids[1:]] = x[ids[0]] + rng.normal(scale=0.01, size=(3, 3))
+    want = orc.contact_energy(pairs, x, 4e-4, 1e5)
+    got = energy(_t(pairs, dev), _t(x, dev), 4e-4, 1e5).cpu().numpy()
+    assert (want > 0).sum() > 500
+    assert np.array_equal(want == 0, got == 0)
+    # near s = 1 the energy goes as (1 - s^2)^4, so a pair's relative error grows there: the
+    # bound is relative to the largest energy of the set
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
