@@ -7,8 +7,9 @@
 // unique count to the host.
 //
 // Here the same result is produced by a counting sort on the row (histogram -> scan ->
-// scatter), a per-row warp sort on (col, original index), and a per-row emit that sums
-// duplicate blocks in original triplet order.  No atomics touch the values, so the output
+// scatter), a per-row sort on (col, original index) (a warp per row of up to 128 entries, a
+// CTA per longer row), and a per-row emit that sums duplicate blocks in original triplet
+// order.  No atomics touch the values, so the output
 // is bitwise deterministic; the summation order (input order) equals that of a stable
 // sort followed by a sequential sum.
 #include "solver.hpp"
@@ -60,9 +61,9 @@ __global__ void k_conv_scatter(const int* rows, const int* cols, int count, int 
 
 // One warp per row: order every entry by (col, original index), write the sorted permutation
 // and sorted cols, and count distinct cols.  Rows of up to 128 entries are sorted by a
-// bitonic network on 64-bit keys (col << 32 | index; 4 keys per lane, position 4 * lane + h),
-// longer rows by ranking (each lane counts the entries before its own).  The keys are
-// unique, so both give the same permutation.
+// bitonic network on 64-bit keys (col << 32 | index; 4 keys per lane, position 4 * lane + h);
+// longer rows are listed for k_conv_sort_long, which sorts each with a whole CTA.  The keys
+// are unique, so every path gives the same permutation.
 constexpr int CONV_WARPS = 8;
 
 __device__ __forceinline__ unsigned long long shfl_xor_u64(unsigned long long v, int m)
@@ -74,7 +75,8 @@ __device__ __forceinline__ unsigned long long shfl_xor_u64(unsigned long long v,
 
 __global__ void __launch_bounds__(32 * CONV_WARPS) k_conv_sort_rows(const int* pcol, const int* row_start,
                                                                     const int* perm_in, int* perm_out, int* scol,
-                                                                    int* uniq, int nrows)
+                                                                    int* uniq, int nrows, int* long_rows,
+                                                                    int* long_cnt)
 {
     const int warps = (gridDim.x * blockDim.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -137,20 +139,8 @@ __global__ void __launch_bounds__(32 * CONV_WARPS) k_conv_sort_rows(const int* p
         }
         else
         {
-            for(int a = lane; a < n; a += 32)
-            {
-                const int ia = perm_in[s + a];
-                const int ca = pcol[s + a];
-                int rank = 0;
-                for(int b = 0; b < n; b++)
-                {
-                    const int ib = perm_in[s + b];
-                    const int cb = pcol[s + b];
-                    rank += (cb < ca) || (cb == ca && ib < ia);
-                }
-                perm_out[s + rank] = ia;
-                scol[s + rank] = ca;
-            }
+            if(lane == 0) long_rows[atomicAdd(long_cnt, 1)] = r;
+            continue;
         }
         __syncwarp();
         int heads = 0;
@@ -159,6 +149,80 @@ __global__ void __launch_bounds__(32 * CONV_WARPS) k_conv_sort_rows(const int* p
         for(int o = 16; o > 0; o >>= 1) heads += __shfl_xor_sync(0xffffffffu, heads, o);
         if(lane == 0) uniq[r] = heads;
         __syncwarp();
+    }
+}
+
+// Rows of more than 128 entries, one CTA each: a bitonic sort of the 64-bit keys in shared
+// memory (up to CONV_LONG_CAP entries), else ranking against the row in global memory;
+// then the distinct cols are counted.
+constexpr int CONV_LONG_THREADS = 256;
+constexpr int CONV_LONG_CAP = 4096;
+
+__global__ void __launch_bounds__(CONV_LONG_THREADS) k_conv_sort_long(const int* pcol, const int* row_start,
+                                                                      const int* perm_in, int* perm_out, int* scol,
+                                                                      int* uniq, const int* long_rows,
+                                                                      const int* long_cnt)
+{
+    __shared__ unsigned long long key[CONV_LONG_CAP];
+    __shared__ int heads;
+    const int nl = *long_cnt, t = threadIdx.x;
+    for(int i = blockIdx.x; i < nl; i += gridDim.x)
+    {
+        const int r = long_rows[i];
+        const int s = row_start[r], n = row_start[r + 1] - s;
+        if(t == 0) heads = 0;
+        if(n <= CONV_LONG_CAP)
+        {
+            int P = 1;
+            while(P < n) P <<= 1;
+            for(int a = t; a < P; a += CONV_LONG_THREADS)
+                key[a] = a < n ? ((unsigned long long)(unsigned)pcol[s + a] << 32) | (unsigned)perm_in[s + a] : ~0ull;
+            __syncthreads();
+            for(int k = 2; k <= P; k <<= 1)
+                for(int j = k >> 1; j > 0; j >>= 1)
+                {
+                    for(int a = t; a < P; a += CONV_LONG_THREADS)
+                    {
+                        const int b = a ^ j;
+                        if(b > a)
+                        {
+                            const unsigned long long x = key[a], y = key[b];
+                            if((x > y) == ((a & k) == 0)) key[a] = y, key[b] = x;
+                        }
+                    }
+                    __syncthreads();
+                }
+            int h = 0;
+            for(int a = t; a < n; a += CONV_LONG_THREADS)
+            {
+                perm_out[s + a] = (int)(unsigned)key[a];
+                scol[s + a] = (int)(key[a] >> 32);
+                h += a == 0 || (key[a] >> 32) != (key[a - 1] >> 32);
+            }
+            atomicAdd(&heads, h);
+        }
+        else
+        {
+            for(int a = t; a < n; a += CONV_LONG_THREADS)
+            {
+                const int ia = perm_in[s + a], ca = pcol[s + a];
+                int rank = 0;
+                for(int b = 0; b < n; b++)
+                {
+                    const int ib = perm_in[s + b], cb = pcol[s + b];
+                    rank += (cb < ca) || (cb == ca && ib < ia);
+                }
+                perm_out[s + rank] = ia;
+                scol[s + rank] = ca;
+            }
+            __syncthreads();
+            int h = 0;
+            for(int a = t; a < n; a += CONV_LONG_THREADS) h += a == 0 || scol[s + a] != scol[s + a - 1];
+            atomicAdd(&heads, h);
+        }
+        __syncthreads();
+        if(t == 0) uniq[r] = heads;
+        __syncthreads();
     }
 }
 
@@ -192,6 +256,62 @@ __global__ void __launch_bounds__(32 * CONV_EMIT_WARPS) k_conv_emit(const double
             }
             __syncwarp();
         }
+        if(!staged)
+        {
+            // a long row: the warp loads 32 entries at a time and every lane accumulates the
+            // runs in sorted order from the shuffled values (the same sums as one lane walking
+            // the run); lane 0 writes each finished run
+            double acc[9];
+            int cur = -1, o = ustart[r] - 1;
+            for(int a0 = 0; a0 < n; a0 += 32)
+            {
+                const int a = a0 + lane;
+                int col = -1;
+                double v[9];
+#pragma unroll
+                for(int t = 0; t < 9; t++) v[t] = 0.0;
+                if(a < n)
+                {
+                    col = scol[s + a];
+                    const double* b0 = blocks + 9 * (size_t)perm[s + a];
+#pragma unroll
+                    for(int t = 0; t < 9; t++) v[t] = b0[t];
+                }
+                const int m = min(32, n - a0);
+                for(int j = 0; j < m; j++)
+                {
+                    const int cj = __shfl_sync(0xffffffffu, col, j);
+                    if(cj != cur)
+                    {
+                        if(cur >= 0 && lane == 0)
+                        {
+                            out_rows[o] = r;
+                            out_cols[o] = cur;
+#pragma unroll
+                            for(int t = 0; t < 9; t++) out_blocks[9 * (size_t)o + t] = acc[t];
+                        }
+                        o++;
+                        cur = cj;
+#pragma unroll
+                        for(int t = 0; t < 9; t++) acc[t] = __shfl_sync(0xffffffffu, v[t], j);
+                    }
+                    else
+                    {
+#pragma unroll
+                        for(int t = 0; t < 9; t++) acc[t] += __shfl_sync(0xffffffffu, v[t], j);
+                    }
+                }
+            }
+            if(cur >= 0 && lane == 0)
+            {
+                out_rows[o] = r;
+                out_cols[o] = cur;
+#pragma unroll
+                for(int t = 0; t < 9; t++) out_blocks[9 * (size_t)o + t] = acc[t];
+            }
+            __syncwarp();
+            continue;
+        }
         int base = 0;
         for(int a0 = 0; a0 < n; a0 += 32)
         {
@@ -202,27 +322,12 @@ __global__ void __launch_bounds__(32 * CONV_EMIT_WARPS) k_conv_emit(const double
             {
                 const int o = ustart[r] + base + __popc(hm & lanemask_lt(lane));
                 double acc[9];
-                if(staged)
+#pragma unroll
+                for(int t = 0; t < 9; t++) acc[t] = sb[9 * a + t];
+                for(int c = a + 1; c < n && scol[s + c] == scol[s + a]; c++)
                 {
 #pragma unroll
-                    for(int t = 0; t < 9; t++) acc[t] = sb[9 * a + t];
-                    for(int c = a + 1; c < n && scol[s + c] == scol[s + a]; c++)
-                    {
-#pragma unroll
-                        for(int t = 0; t < 9; t++) acc[t] += sb[9 * c + t];
-                    }
-                }
-                else
-                {
-                    const double* b0 = blocks + 9 * (size_t)perm[s + a];
-#pragma unroll
-                    for(int t = 0; t < 9; t++) acc[t] = b0[t];
-                    for(int c = a + 1; c < n && scol[s + c] == scol[s + a]; c++)
-                    {
-                        const double* bc = blocks + 9 * (size_t)perm[s + c];
-#pragma unroll
-                        for(int t = 0; t < 9; t++) acc[t] += bc[t];
-                    }
+                    for(int t = 0; t < 9; t++) acc[t] += sb[9 * c + t];
                 }
                 out_rows[o] = r;
                 out_cols[o] = scol[s + a];
@@ -260,13 +365,14 @@ int convert_into(Solver& S, ConvertScratch& cv, int count, const int* rows, cons
     STG_TRY(cv.scol.resize(count));
     STG_TRY(cv.pcol.resize(count));
     STG_TRY(cv.uniq.resize(nrows + 1));
+    STG_TRY(cv.long_rows.resize(nrows + 1));
     STG_TRY(out_rows.resize(count));
     STG_TRY(out_cols.resize(count));
     STG_TRY(out_blocks.resize((size_t)count * 9));
 
     STG_CUDA_TRY(cudaMemsetAsync(cv.row_cnt.data(), 0, sizeof(int) * (nrows + 1), s));
     STG_CUDA_TRY(cudaMemsetAsync(cv.cursor.data(), 0, sizeof(int) * (nrows + 1), s));
-    STG_CUDA_TRY(cudaMemsetAsync(cv.scratch.data() + 2, 0, sizeof(int), s));
+    STG_CUDA_TRY(cudaMemsetAsync(cv.scratch.data() + 2, 0, 2 * sizeof(int), s));
     const int g = std::min(div_up(count, 256), kSMs * 16);
     k_conv_hist<<<g, 256, 0, s>>>(rows, cols, count, nrows, skip_negative, cv.row_cnt.data(), cv.scratch.data() + 2);
     STG_LAUNCH_CHECK();
@@ -277,7 +383,12 @@ int convert_into(Solver& S, ConvertScratch& cv, int count, const int* rows, cons
     STG_LAUNCH_CHECK();
     const int gw = std::min(div_up((long)nrows * 32, 32 * CONV_WARPS), kSMs * 16);
     k_conv_sort_rows<<<gw, 32 * CONV_WARPS, 0, s>>>(cv.pcol.data(), cv.row_start.data(), cv.perm.data(), cv.perm2.data(),
-                                                    cv.scol.data(), cv.uniq.data(), nrows);
+                                                    cv.scol.data(), cv.uniq.data(), nrows, cv.long_rows.data(),
+                                                    cv.scratch.data() + 3);
+    STG_LAUNCH_CHECK();
+    k_conv_sort_long<<<kSMs, CONV_LONG_THREADS, 0, s>>>(cv.pcol.data(), cv.row_start.data(), cv.perm.data(),
+                                                        cv.perm2.data(), cv.scol.data(), cv.uniq.data(),
+                                                        cv.long_rows.data(), cv.scratch.data() + 3);
     STG_LAUNCH_CHECK();
     STG_CUDA_TRY(cudaMemsetAsync(cv.uniq.data() + nrows, 0, sizeof(int), s));
     k_scan_exclusive<<<1, 1024, 0, s>>>(cv.uniq.data(), row_ptr.data(), nullptr, nrows + 1, cv.scratch.data() + 1);
@@ -287,7 +398,7 @@ int convert_into(Solver& S, ConvertScratch& cv, int count, const int* rows, cons
         blocks, cv.row_start.data(), cv.perm2.data(), cv.scol.data(), row_ptr.data(), out_rows.data(), out_cols.data(),
         out_blocks.data(), nrows);
     STG_LAUNCH_CHECK();
-    S.launches += 6;
+    S.launches += 7;
     int h[2] = {0, 0};
     STG_CUDA_TRY(cudaMemcpyAsync(h, cv.scratch.data() + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     STG_CUDA_TRY(cudaStreamSynchronize(s));

@@ -55,7 +55,7 @@ struct Bcoo
 
 struct ConvertScratch
 {
-    DBuf<int> row_cnt, row_start, cursor, perm, perm2, pcol, scol, uniq, scratch;
+    DBuf<int> row_cnt, row_start, cursor, perm, perm2, pcol, scol, uniq, scratch, long_rows;
 };
 
 struct MasState

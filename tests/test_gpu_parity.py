@@ -71,6 +71,36 @@ def test_convert_edge_cases(dev):
     assert np.array_equal(Bk[:9 * u].cpu().numpy().reshape(-1, 9), eb)
 
 
+def test_convert_long_rows_bit_exact(dev):
+    """Rows far longer than the warp sort's 128 entries (sorted by a CTA each) and runs of
+    more than a thousand duplicates of one block (summed warp-cooperatively in input order):
+    a 1,500-entry row with a 1,200-entry run, a 5,000-entry row (beyond the CTA's
+    shared-memory sort, ranked), and rows of exactly 129 entries, mixed with short rows."""
+    from oracle import oracle as orc
+    rng = np.random.default_rng(23)
+    rows, cols = [], []
+    rows += [7] * 1500
+    cols += [7] * 1200 + list(rng.integers(7, 200, size=300))
+    rows += [11] * 5000
+    cols += list(rng.integers(11, 400, size=5000))
+    rows += [13] * 129
+    cols += list(rng.integers(13, 60, size=129))
+    for r in range(400):
+        k = int(rng.integers(1, 20))
+        rows += [r] * k
+        cols += list(rng.integers(r, 400, size=k))
+    rows, cols = np.array(rows, np.int32), np.array(cols, np.int32)
+    perm = rng.permutation(rows.size)
+    rows, cols = rows[perm], cols[perm]
+    blocks = rng.standard_normal((rows.size, 9))
+    er, ec, eb = orc.convert(rows, cols, blocks)
+    R, Cc, Bk = _t(rows, dev), _t(cols, dev), _t(blocks.reshape(-1), dev)
+    u = _solver().convert(R, Cc, Bk)
+    assert u == er.size
+    assert np.array_equal(R[:u].cpu().numpy(), er) and np.array_equal(Cc[:u].cpu().numpy(), ec)
+    assert np.array_equal(Bk[:9 * u].cpu().numpy().reshape(-1, 9), eb)
+
+
 # ------------------------------------------------------------------------------------------
 @pytest.mark.parametrize("a,b", [(1.0, 0.0), (-0.5, 2.0)])
 def test_spmv(dev, a, b):
