@@ -275,6 +275,30 @@ int stg_contact_barrier(int ncp, const int32_t* pairs, const double* x, int num_
 int stg_contact_energy(int ncp, const int32_t* pairs, const double* x, int num_verts, double dhat,
                        double kappa, double* energy, void* stream);
 
+/* ---- cloth ------------------------------------------------------------------------------ */
+/* Replaces _calculate_triangle_fem_gradient_hessian (StiffGIPC/femEnergy.cu:2146-2216): per
+ * triangle, the Baraff-Witkin membrane energy area dt^2 [stretch ((su - 1)^2 + (sv - 1)^2 +
+ * strain_rate ((su - 1)^3_+ + (sv - 1)^3_+)) + shear I6^2], su = |F u|, sv = |F v|,
+ * I6 = F u . F v, F = Ds Dm^-1; gradient (9 doubles per triangle, 3 per vertex) and the 6 upper
+ * 3x3 blocks (column-major, row <= col, plus block_offset) of its Hessian, whose stretch part is
+ * projected per direction and shear part to PSD as the reference does (:535-706).
+ * tri_verts: int32[3 tris]; dminv: double[4 tris] row-major 2x2 inverse of the rest edges in
+ * the reference's triangle frame (__calculateDm2D_double); area: double[tris], rest area times
+ * thickness.  *bad (device, may be NULL) counts triangles with an index out of range or a
+ * repeated vertex (zero terms).  Device arrays; asynchronous. */
+int stg_cloth_membrane(int tris, const int32_t* tri_verts, const double* dminv, const double* area,
+                       const double* x, int num_verts, double stretch, double shear, double strain_rate,
+                       double dt, int block_offset, int32_t* rows, int32_t* cols, double* blocks,
+                       double* grad, int* bad, void* stream);
+/* Replaces _calculate_quad_bending_gradient_hessian (femEnergy.cu:2620-2755,
+ * USE_QUADRATIC_BENDING): per edge stencil (v0, v1, opposite vertex of each triangle;
+ * int32[4 edges], the last -1 for a boundary edge, which gets zero terms), c = rest_length
+ * bend_stiff dt^2, gradient c Q x (12 doubles) and the 10 upper blocks of c Q (x) I3.  Q:
+ * double[16 edges], row-major 4x4 (PrepareQuadBendingQ).  Device arrays; asynchronous. */
+int stg_cloth_bending(int edges, const int32_t* stencil, const double* Q, const double* rest_length,
+                      const double* x, int num_verts, double bend_stiff, double dt, int block_offset,
+                      int32_t* rows, int32_t* cols, double* blocks, double* grad, int* bad, void* stream);
+
 /* ---- affine bodies (ABD) ---------------------------------------------------------------- */
 /* Body b owns block rows 4 b .. 4 b + 3; q[12 b ..] = (t, a1, a2, a3) with a_i the rows of A
  * (x = A xbar + t, abd_jacobi_matrix.inl); FEM vertices follow at block row 4 bodies + v.

@@ -114,6 +114,8 @@ def lib():
     L.stg_abd_gather_gradient.argtypes = [ci, vp, vp, vp, vp, vp]
     L.stg_ccd_step_size.argtypes = [ci, vp, vp, vp, ci, cd, cd, vp, vp, vp, vp, vp]
     L.stg_contact_energy.argtypes = [ci, vp, vp, ci, cd, cd, vp, vp]
+    L.stg_cloth_membrane.argtypes = [ci, vp, vp, vp, vp, ci, cd, cd, cd, cd, ci, vp, vp, vp, vp, vp, vp]
+    L.stg_cloth_bending.argtypes = [ci, vp, vp, vp, vp, ci, cd, cd, ci, vp, vp, vp, vp, vp, vp]
     L.stg_contact_barrier.argtypes = [ci, vp, vp, ci, ci, cd, cd, vp, vp, vp, vp, vp, vp]
     L.stg_spmv_tiles_info.argtypes = [vp, C.POINTER(ci), C.POINTER(C.c_float), C.POINTER(C.c_float),
                                       C.POINTER(C.c_float)]

@@ -115,6 +115,30 @@ def morton_renumber(pos: np.ndarray, tets: np.ndarray):
     return pos[order], new_of_old[tets], order
 
 
+def edge_neighbors(num_verts: int, pairs: np.ndarray):
+    """CSR vertex neighbour lists from oriented vertex pairs, with the ordering rule of
+    vert_neighbors (first orientation met kept, set walked in lexicographic order)."""
+    pairs = np.asarray(pairs, dtype=np.int64).reshape(-1, 2)
+    lo = np.minimum(pairs[:, 0], pairs[:, 1])
+    hi = np.maximum(pairs[:, 0], pairs[:, 1])
+    ukey = lo * num_verts + hi
+    _, first = np.unique(ukey, return_index=True)
+    edges = pairs[np.sort(first)]
+    order = np.lexsort((edges[:, 1], edges[:, 0]))
+    edges = edges[order]
+    a, b = edges[:, 0], edges[:, 1]
+    src = np.empty(2 * a.size, dtype=np.int64)
+    dst = np.empty(2 * a.size, dtype=np.int64)
+    src[0::2], dst[0::2] = a, b
+    src[1::2], dst[1::2] = b, a
+    order = np.argsort(src, kind="stable")
+    nlist = dst[order].astype(np.uint32)
+    num = np.bincount(src, minlength=num_verts).astype(np.uint32)
+    start = np.zeros(num_verts, dtype=np.uint32)
+    start[1:] = np.cumsum(num[:-1], dtype=np.int64).astype(np.uint32)
+    return start, num, nlist
+
+
 def vert_neighbors(num_verts: int, tets: np.ndarray):
     """CSR vertex neighbour lists with the ordering of ``getVertNeighbors``.
 
@@ -820,3 +844,183 @@ def ccd_candidates(pos: np.ndarray, disp: np.ndarray, tris: np.ndarray, body: Op
         keep &= body[a[:, 0]] != body[b[:, 0]]
     out.append(np.concatenate([a[keep], b[keep]], axis=1))
     return np.concatenate(out).astype(np.int32)
+
+
+# ----------------------------------------------------------------------------------------
+# Cloth on a soft ball (the cloth-on-solid configuration)
+# ----------------------------------------------------------------------------------------
+
+
+def cloth_rest_frame(rest: np.ndarray, tris: np.ndarray):
+    """(Dm^-1 [T, 4] row-major 2x2, rest area [T]) of each triangle in the reference's 2D frame
+    (__calculateDm2D_double, femEnergy.cu:256-303: the triangle rotated so that its normal is
+    +z, then its x, y coordinates)."""
+    x0, x1, x2 = rest[tris[:, 0]], rest[tris[:, 1]], rest[tris[:, 2]]
+    n = np.cross(x1 - x0, x2 - x0)
+    area = 0.5 * np.linalg.norm(n, axis=1)
+    n = n / np.linalg.norm(n, axis=1, keepdims=True)
+    z = np.array([0.0, 0.0, 1.0])
+    vec = np.cross(n, z)
+    cos = n @ z
+    T = tris.shape[0]
+    R = np.tile(np.eye(3), (T, 1, 1))
+    flip = cos + 1 == 0
+    R[flip, 0, 0] = R[flip, 1, 1] = -1
+    k = ~flip
+    C = np.zeros((T, 3, 3))
+    C[:, 0, 1], C[:, 0, 2] = -vec[:, 2], vec[:, 1]
+    C[:, 1, 0], C[:, 1, 2] = vec[:, 2], -vec[:, 0]
+    C[:, 2, 0], C[:, 2, 1] = -vec[:, 1], vec[:, 0]
+    R[k] = R[k] + C[k] + (C[k] @ C[k]) / (1 + cos[k])[:, None, None]
+    u0 = np.einsum("tij,tj->ti", R, x1)[:, :2] - np.einsum("tij,tj->ti", R, x0)[:, :2]
+    u1 = np.einsum("tij,tj->ti", R, x2)[:, :2] - np.einsum("tij,tj->ti", R, x0)[:, :2]
+    Dm = np.stack([u0, u1], axis=2)  # columns u0, u1
+    return np.linalg.inv(Dm).reshape(T, 4), area
+
+
+def bending_stencils(rest: np.ndarray, tris: np.ndarray):
+    """Interior edges (v0, v1, opposite of the first triangle, opposite of the second), their
+    rest lengths and the quadratic bending matrices Q (PrepareQuadBendingQ,
+    femEnergy.cu:2490-2618: Q = 3 / (A0 + A1) K K^T from the cotangent weights K)."""
+    e = np.concatenate([tris[:, [0, 1, 2]], tris[:, [1, 2, 0]], tris[:, [2, 0, 1]]])  # edge a b, opposite c
+    key = np.minimum(e[:, 0], e[:, 1]) * (rest.shape[0] + 1) + np.maximum(e[:, 0], e[:, 1])
+    order = np.argsort(key, kind="stable")
+    ks = key[order]
+    pair = np.nonzero(ks[1:] == ks[:-1])[0]
+    a, b = e[order[pair]], e[order[pair + 1]]
+    st = np.stack([a[:, 0], a[:, 1], a[:, 2], b[:, 2]], axis=1)
+    v0, v1, v2, v3 = (rest[st[:, i]] for i in range(4))
+    e0, e1, e2, e3, e4 = v1 - v0, v2 - v0, v3 - v0, v2 - v1, v3 - v1
+
+    def cot(p, q):
+        cr = np.linalg.norm(np.cross(p, q), axis=1)
+        return np.where(cr < 1e-12, 0.0, np.einsum("ij,ij->i", p, q) / np.where(cr < 1e-12, 1.0, cr))
+
+    c01, c02, c03, c04 = cot(e0, e1), cot(e0, e2), cot(-e0, e3), cot(-e0, e4)
+    K = np.stack([c03 + c04, c01 + c02, -c01 - c03, -c02 - c04], axis=1)
+    a0 = 0.5 * np.linalg.norm(np.cross(e0, e1), axis=1)
+    a1 = 0.5 * np.linalg.norm(np.cross(e0, e2), axis=1)
+    Q = 3.0 / (a0 + a1)[:, None, None] * K[:, :, None] * K[:, None, :]
+    return st.astype(np.int32), np.linalg.norm(e0, axis=1), Q.reshape(-1, 16)
+
+
+def ball_mesh(n: int, radius: float, center):
+    """A tet ball: the n^3-hex cube grid over [-1, 1]^3 mapped onto the ball (each point of the
+    cube moved along the map x' = x sqrt(1 - y^2/2 - z^2/2 + y^2 z^2/3), cyclically)."""
+    p, tets = box_mesh(n, n, n, 2.0 / n, origin=(-1.0, -1.0, -1.0))
+    x, y, z = p[:, 0], p[:, 1], p[:, 2]
+    q = np.stack([x * np.sqrt(1 - y * y / 2 - z * z / 2 + y * y * z * z / 3),
+                  y * np.sqrt(1 - z * z / 2 - x * x / 2 + z * z * x * x / 3),
+                  z * np.sqrt(1 - x * x / 2 - y * y / 2 + x * x * y * y / 3)], axis=1)
+    return q * radius + np.asarray(center, np.float64), tets
+
+
+@dataclasses.dataclass
+class ClothScene:
+    """Cloth (vertices with cloth triangles) and a tet ball in one vertex numbering (Morton
+    ordered), at one Newton iteration.  base: the ball's elastic + inertia terms and a
+    diagonal mass block per vertex (cloth vertices: their lumped cloth mass), with the
+    inertia gradient of all vertices; the cloth membrane and bending terms and the contacts
+    are added by stgipc.cloth.cloth_system."""
+    name: str
+    base: NewtonSystem
+    tris: np.ndarray          # int32 [T, 3] cloth triangles
+    dminv: np.ndarray         # [T, 4]
+    area: np.ndarray          # [T] rest area x thickness
+    stencil: np.ndarray       # int32 [E, 4]
+    elen: np.ndarray          # [E]
+    Q: np.ndarray             # [E, 16]
+    stretch: float
+    shear: float
+    strain_rate: float
+    bend: float
+    dt: float
+    contacts: np.ndarray      # int32 [C, 4]
+    dhat: float
+    kappa: float
+    cloth_verts: int
+
+
+def make_cloth_sphere(n: int = 256, size: float = 1.0, thickness: float = 1e-3, E_cloth: float = 1e4,
+                      nu: float = 0.45, density_cloth: float = 200.0, strain_rate: float = 1.0,
+                      bend: float = 1e-4, radius: float = 0.3, ball_n: int = 19, E_ball: float = 1e6,
+                      rho_ball: float = 1000.0, dt: float = 1.0 / 60.0, drop_speed: float = 1.0, dhat: float = 1e-6,
+                      kappa: float = 1e4, jitter: float = 1e-4, seed: int = 1002) -> ClothScene:
+    """n x n cloth vertices over size x size m (2 (n-1)^2 triangles), Baraff-Witkin membrane
+    with stretch stiffness E / (2 (1 + nu)) and shear 0.03 x stretch x strain rate, quadratic
+    bending k = bend, thickness and density as given; draped over a tet ball of radius 0.3 m
+    (ball_n^3 hexes, 6 tets each, Neo-Hookean E_ball): its middle follows the ball's cap 0.2 to
+    0.8 mm above the surface out to 0.6 r, then continues along the cap's tangent cone; it
+    moves down at drop_speed (the speed after a 5 cm drop); vertices jittered U(+-jitter) in
+    the plane.  The Newton iteration of the step at which it lands.  kappa is sized to the
+    cloth's weight (0.2 kg/m^2 over some 10^4 pairs: about 1e-5 N per pair, and a pair's barrier
+    force at half the activation distance is about 9e-9 kappa N at dhat = 1e-6); a much stiffer
+    barrier only makes the system worse conditioned."""
+    rng = np.random.default_rng(seed)
+    h = size / (n - 1)
+    g = np.arange(n) * h
+    X, Z = np.meshgrid(g, g, indexing="xy")
+    cloth = np.stack([X.ravel(), np.zeros(n * n), Z.ravel()], axis=1)
+    cloth[:, [0, 2]] += rng.uniform(-jitter, jitter, size=(n * n, 2))
+    ii, jj = np.meshgrid(np.arange(n - 1), np.arange(n - 1), indexing="xy")
+    a = (jj * n + ii).ravel()
+    tris = np.concatenate([np.stack([a, a + 1, a + n + 1], 1), np.stack([a, a + n + 1, a + n], 1)])
+    center = np.array([0.5 * size, radius, 0.5 * size])
+    bpos, btets = ball_mesh(ball_n, radius, center)
+    rest_cloth = cloth.copy()
+    rest_cloth[:, 1] = 2 * radius + 0.05
+    # draped shape
+    r = np.hypot(cloth[:, 0] - center[0], cloth[:, 2] - center[2])
+    r0 = 0.6 * radius
+    cap = lambda rr: center[1] + np.sqrt(radius * radius - rr * rr)
+    slope = r0 / np.sqrt(radius * radius - r0 * r0)
+    gap = rng.uniform(2e-4, 8e-4, size=n * n)
+    cloth[:, 1] = np.where(r < r0, cap(np.minimum(r, r0)) + gap, cap(r0) + gap - (r - r0) * slope)
+    Vc = n * n
+    pos = np.concatenate([cloth, bpos])
+    rest = np.concatenate([rest_cloth, bpos])
+    tets = btets + Vc
+    # one Morton order for all vertices (the MAS banks are runs of consecutive vertices)
+    key = morton_hash(pos)
+    order = np.argsort(key, kind="stable")
+    new_of_old = np.empty_like(order)
+    new_of_old[order] = np.arange(order.size)
+    pos, rest = pos[order], rest[order]
+    tets = new_of_old[tets]
+    tris = new_of_old[tris].astype(np.int64)
+    body = (order >= Vc).astype(np.int64)   # 0 cloth, 1 ball
+    V = pos.shape[0]
+    vel = np.zeros_like(pos)
+    vel[body == 0, 1] = -drop_speed
+    base = _assemble(f"cloth{n}_ball", rest, pos, tets, np.full(tets.shape[0], E_ball), nu, rho_ball, dt, vel,
+                     barriers=[])
+    dminv, area0 = cloth_rest_frame(rest, tris)
+    area = area0 * thickness
+    mass = np.zeros(V)
+    np.add.at(mass, tris.reshape(-1), np.repeat(density_cloth * area / 3.0, 3))
+    # the cloth's lumped mass on its diagonal blocks and its inertia gradient M (x - xtilde)
+    diag = np.arange(base.rows.size - V, base.rows.size)  # _assemble appends one mass block per vertex
+    assert np.array_equal(base.rows[diag], np.arange(V)) and np.array_equal(base.cols[diag], np.arange(V))
+    mb = base.blocks.copy()
+    cm = mass[base.rows[diag]]
+    mb[diag, 0] += cm
+    mb[diag, 4] += cm
+    mb[diag, 8] += cm
+    x_tilde = pos + dt * vel + dt * dt * np.array([0.0, -9.8, 0.0])
+    b = base.b.reshape(V, 3) + mass[:, None] * (pos - x_tilde)
+    pairs_edges = np.concatenate([tris[:, [0, 1]], tris[:, [1, 2]], tris[:, [0, 2]],
+                                  tets[:, [0, 1]], tets[:, [0, 2]], tets[:, [0, 3]], tets[:, [1, 2]], tets[:, [1, 3]],
+                                  tets[:, [2, 3]]])
+    start, num, nlist = edge_neighbors(V, pairs_edges)
+    base = dataclasses.replace(base, blocks=mb, b=b.reshape(-1), neighbor_start=start, neighbor_num=num,
+                               neighbor_list=nlist)
+    st, elen, Q = bending_stencils(rest, tris)
+    # contacts between the cloth and the ball's surface near it
+    faces = np.concatenate([tris, boundary_faces(tets)])
+    near = np.linalg.norm(pos[faces].mean(axis=1) - center, axis=1) < radius + 0.02
+    contacts = contact_pairs(pos, faces[near], body, dhat)
+    stretch = E_cloth / (2 * (1 + nu))
+    return ClothScene(name=f"cloth{n}_ball", base=base, tris=tris.astype(np.int32), dminv=dminv, area=area,
+                      stencil=st, elen=elen, Q=Q, stretch=stretch, shear=0.03 * stretch * strain_rate,
+                      strain_rate=strain_rate, bend=bend, dt=dt, contacts=contacts, dhat=dhat, kappa=kappa,
+                      cloth_verts=Vc)
