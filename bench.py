@@ -18,6 +18,10 @@ FP64 true residual reported).
   e2e    : the FP32 solve with the triplets and b copied host->device from pinned memory and
            x copied back, every step.
 
+Other workloads (parity-test configurations, not the headline): ``--workload abd512`` (512
+affine bodies on a soft slab), ``--workload cloth256`` (a 256 x 256 cloth landing on a tet
+ball), ``--workload batch256`` (256 independent cubes in one launch), ``cube16``.
+
 ``--impl reference`` times the CPU oracle port (the reference's MAS-PCG restated in C,
 oracle/) on all host cores (OpenMP): the reference itself is GPU-only and cannot be built
 here (it needs Eigen 3.4).
@@ -52,7 +56,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch256", "abd512"], default="hetcube48")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch256", "abd512", "cloth256"], default="hetcube48")
     ap.add_argument("--bank", type=int, default=16)
     ap.add_argument("--refine", type=int, default=32)
     ap.add_argument("--batch", type=int, default=8)
@@ -380,88 +384,141 @@ def run_batch(args):
     return 0
 
 
-def abd_cpu_solve_ms(sc, rows, cols, blocks, b, bank, budget_s):
-    """One coupled MAS-PCG solve of the oracle on one host thread: convert + MAS build and
-    assembly + ABD block-Jacobi + PCG to ||r|| / ||b|| <= 1e-4 (time-bounded)."""
+def scene_cpu_solve_ms(W, sc, rows, cols, blocks, b, contacts, bank, budget_s):
+    """One MAS-PCG solve of a scene workload's system by the oracle on one host thread:
+    convert + MAS build and assembly (+ ABD block-Jacobi) + PCG to ||r|| / ||b|| <= 1e-4
+    (time-bounded)."""
     from oracle import abd_oracle as abd, oracle as orc
     orc.build()
-    N, s = sc.bodies, sc.fem
+    mesh, off, N = W["mesh"](sc), W["fem_offset"](sc), W["bodies"](sc)
     t0 = time.perf_counter()
     r, c, bl = orc.convert(rows, cols, blocks)
-    m = orc.Mas(bank, s.num_verts, s.neighbor_start, s.neighbor_num, s.neighbor_list, *s.slot_maps(bank))
-    m.build()
-    m.assemble(r, c, bl, fem_offset=4 * N)
-    ai = abd.block_jacobi(r, c, bl, N)
+    m = orc.Mas(bank, mesh.num_verts, mesh.neighbor_start, mesh.neighbor_num, mesh.neighbor_list,
+                *mesh.slot_maps(bank))
+    m.build(contacts)
+    m.assemble(r, c, bl, fem_offset=off)
+    ai = abd.block_jacobi(r, c, bl, N) if N else None
     t_setup = time.perf_counter() - t0
-    _, st, t_iter, done = orc.pcg_timed(r, c, bl, b, mas=m, fem_offset=4 * N, tol=1e-4, stop_rule="relative",
+    _, st, t_iter, done = orc.pcg_timed(r, c, bl, b, mas=m, fem_offset=off, tol=1e-4, stop_rule="relative",
                                         budget_s=budget_s, abd_bodies=N, abd_inv=ai)
     k = st["iterations"]
     n_it = k if done else orc.extrapolated_iterations(st)
     ms = (t_setup + t_iter * n_it) * 1e3
-    sample = (f"oracle coupled MAS-PCG (bank {bank}): convert + MAS build/assembly + ABD block-Jacobi "
+    sample = (f"oracle MAS-PCG (bank {bank}): convert + MAS build/assembly{' + ABD block-Jacobi' if N else ''} "
               f"({t_setup:.1f} s) + {k} PCG iterations on 1 thread ({'converged' if done else 'time-bounded'}), "
               f"per-iteration time x {n_it} iterations")
     return ms, n_it, sample
 
 
-ABD_DESC = ("stiff-affine hybrid: 512 affine cubes (12 DOF, kappa 1e8) in an 8x8x8 lattice, random rotations, "
-            "bottom layer touching a 64x64x8-hex slab (196,608 tets, E=1e5); 6,144 + 114,075 DOF, dt=1/100")
+def _abd_gpu(sc, dev):
+    from stgipc.abd import coupled_system
+    rows, cols, blocks, b = coupled_system(sc, dev)
+    return rows, cols, blocks, b, None
 
 
-def run_abd(args):
-    """--workload abd512: the coupled affine-body + FEM Newton solve (12x12 ABD tiles as 4x4
-    3x3 blocks, ABD block-Jacobi composed with MAS on the slab) through stg_solve_linear_system."""
-    from stgipc import scenes
+def _abd_cpu(sc):
+    from oracle import abd_oracle as abd
+    return (*abd.coupled_system(sc), None)
+
+
+def _cloth_gpu(sc, dev):
+    from stgipc.cloth import cloth_system
+    return cloth_system(sc, dev)
+
+
+def _cloth_cpu(sc):
+    import numpy as np
+    from oracle import cloth_oracle as co, oracle as orc
+    base = sc.base
+    x = base.pos
+    V = base.num_verts
+    mr, mc, mb, mg = co.membrane(sc.tris, sc.dminv, sc.area, x, sc.stretch, sc.shear, sc.strain_rate, sc.dt)
+    br, bc, bb, bg = co.bending(sc.stencil, sc.Q, sc.elen, x, sc.bend, sc.dt)
+    cr, cc, cb, cg, _ = orc.contact_barrier(sc.contacts, x, sc.dhat, sc.kappa)
+    g = base.b.reshape(V, 3).copy()
+    np.add.at(g, sc.tris.reshape(-1), mg.reshape(-1, 3))
+    np.add.at(g, sc.stencil.reshape(-1), bg.reshape(-1, 3))
+    for p, q in enumerate(sc.contacts):
+        vid = [(-q[0] - 1) if q[0] < 0 else q[0], q[1], q[2], q[3]]
+        for k in range(4):
+            if vid[k] >= 0:
+                g[vid[k]] += cg[p, 3 * k:3 * k + 3]
+    rows = np.concatenate([base.rows, mr, br, cr]).astype(np.int32)
+    cols = np.concatenate([base.cols, mc, bc, cc]).astype(np.int32)
+    return rows, cols, np.concatenate([base.blocks, mb, bb, cb]), g.reshape(-1), sc.contacts
+
+
+SCENE_WORKLOADS = {
+    "abd512": dict(
+        make=lambda seed: __import__("stgipc.scenes", fromlist=["x"]).make_abd_slab(seed=1003 + seed),
+        gpu=_abd_gpu, cpu=_abd_cpu, mesh=lambda sc: sc.fem, fem_offset=lambda sc: 4 * sc.bodies,
+        bodies=lambda sc: sc.bodies,
+        desc=("stiff-affine hybrid: 512 affine cubes (12 DOF, kappa 1e8) in an 8x8x8 lattice, random rotations, "
+              "bottom layer touching a 64x64x8-hex slab (196,608 tets, E=1e5); 6,144 + 114,075 DOF, dt=1/100"),
+        extra=lambda sc: {"bodies": sc.bodies, "contacts": int(sc.contacts.shape[0])}),
+    "cloth256": dict(
+        make=lambda seed: __import__("stgipc.scenes", fromlist=["x"]).make_cloth_sphere(seed=1002 + seed),
+        gpu=_cloth_gpu, cpu=_cloth_cpu, mesh=lambda sc: sc.base, fem_offset=lambda sc: 0, bodies=lambda sc: 0,
+        desc=("cloth-on-solid: 256x256 cloth (65,536 verts, 130,050 tris; Baraff-Witkin membrane from E=1e4, "
+              "thickness 1e-3, quadratic bending 1e-4) landing on a 0.3 m tet ball (41,154 tets, E=1e6), "
+              "point-triangle / edge-edge barriers dhat=1e-3 m; 220,608 DOF, dt=1/60"),
+        extra=lambda sc: {"cloth_tris": int(sc.tris.shape[0]), "bending_stencils": int(sc.stencil.shape[0]),
+                          "contacts": int(sc.contacts.shape[0])}),
+}
+
+
+def run_scene(args):
+    """--workload abd512 | cloth256: a coupled Newton solve built on the device from a scene
+    (stgipc.abd / stgipc.cloth) and solved through stg_solve_linear_system."""
+    W = SCENE_WORKLOADS[args.workload]
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
         if rank != 0:
             return 0
-        from oracle import abd_oracle as abd
-        sc = scenes.make_abd_slab(seed=1003)
-        rows, cols, blocks, b = abd.coupled_system(sc)
+        sc = W["make"](0)
+        rows, cols, blocks, b, cp = W["cpu"](sc)
         times, sample = [], ""
         for step in range(args.warmup + args.steps):
-            ms, _, sample = abd_cpu_solve_ms(sc, rows, cols, blocks, b, args.bank, 20.0)
+            ms, _, sample = scene_cpu_solve_ms(W, sc, rows, cols, blocks, b, cp, args.bank, 20.0)
             if step >= args.warmup:
                 times.append(ms)
         ms = statistics.mean(times)
         print(json.dumps({"metric": METRIC, "value": ms, "unit": "ms", "n_gpus": args.gpus, "steps": args.steps,
                           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
                           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-                          "config": {"workload": "abd512", "desc": ABD_DESC, "dof": sc.n, "bank": args.bank,
-                                     "stop": "||b-Ax||/||b|| <= 1e-4"},
+                          "config": {"workload": args.workload, "desc": W["desc"], "dof": int(b.size),
+                                     "bank": args.bank, "stop": "||b-Ax||/||b|| <= 1e-4"},
                           "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "port",
                                            "sample": "per step: " + sample},
                           "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return 0
     import torch
     from stgipc import PCGSolverConfig, Solver
-    from stgipc.abd import coupled_system
     if world > 1:
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
-    sc = scenes.make_abd_slab(seed=1003 + rank)
-    N, s = sc.bodies, sc.fem
-    rows, cols, blocks, b = coupled_system(sc, dev)
+    sc = W["make"](rank)
+    mesh, off, N = W["mesh"](sc), W["fem_offset"](sc), W["bodies"](sc)
+    rows, cols, blocks, b, P = W["gpu"](sc, dev)
     blocks = blocks.reshape(-1)
     x = torch.zeros_like(b)
-    pm, rm = s.slot_maps(args.bank)
+    pm, rm = mesh.slot_maps(args.bank)
 
     def make(precision):
         cfg = PCGSolverConfig(bank_size=args.bank, precision=precision, stop_rule="relative_residual",
                               global_tol_rate=1e-4, refine_interval=args.refine, loop=args.loop,
                               graph_batch=args.batch, max_iter_ratio=0.3)
         so = Solver(cfg, stream=stream)
-        so.mas_init(s.num_verts, s.neighbor_start, s.neighbor_num, s.neighbor_list, pm, rm)
+        so.mas_init(mesh.num_verts, mesh.neighbor_start, mesh.neighbor_num, mesh.neighbor_list, pm, rm)
         return so
 
     def solve(so, R=rows, Cc=cols, Bk=blocks, bb=b, xx=x, stats=False):
-        return so.solve_linear_system(R, Cc, Bk, bb, xx, fem_block_offset=4 * N, abd_bodies=N, stats=stats)
+        return so.solve_linear_system(R, Cc, Bk, bb, xx, fem_block_offset=off, abd_bodies=N, contacts=P, stats=stats)
 
     def timed(so, k):
         if world > 1:
@@ -523,21 +580,20 @@ def run_abd(args):
     achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        from oracle import abd_oracle as abd
-        R, Cc, Bk, bh = abd.coupled_system(sc)
-        ms_cpu, n_it, sample = abd_cpu_solve_ms(sc, R, Cc, Bk, bh, args.bank, args.cpu_budget_s)
+        R, Cc, Bk, bh, cp = W["cpu"](sc)
+        ms_cpu, n_it, sample = scene_cpu_solve_ms(W, sc, R, Cc, Bk, bh, cp, args.bank, args.cpu_budget_s)
         cpu = {"value": ms_cpu, "unit": "ms", "cores": 1, "kind": "port", "sample": sample}
     if rank == 0:
+        config = {"workload": args.workload, "desc": W["desc"], "dof": int(b.numel()), "nnzb": st_fast["nnzb"],
+                  "triplets": int(rows.numel()), "bank": args.bank, "stop": "||b-Ax||/||b|| <= 1e-4",
+                  "loop": args.loop, "l2": "every solve re-converts and re-assembles from the triplets",
+                  "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+        config.update(W["extra"](sc))
         print(json.dumps({
             "metric": METRIC, "value": ms_fast, "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_fast, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (FP64 dots, FP64 residual replacement)", "data": "synthetic",
-            "value_is": "the FP32-storage coupled solve (no learned correction on this workload)",
-            "config": {"workload": "abd512", "desc": ABD_DESC, "dof": sc.n, "nnzb": st_fast["nnzb"],
-                       "triplets": int(rows.numel()), "bodies": N, "contacts": int(sc.contacts.shape[0]),
-                       "bank": args.bank, "stop": "||b-Ax||/||b|| <= 1e-4", "loop": args.loop,
-                       "l2": "triplets below L2 size; every solve re-converts and re-assembles from them",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "value_is": "the FP32-storage solve (no learned correction on this workload)", "config": config,
             "iterations": st_fast["iterations"], "rel_residual": st_fast["rel_residual"],
             "plain_fp64_ms": ms_plain, "plain_fp64_iterations": st_plain["iterations"],
             "plain_fp64_rel_residual": st_plain["rel_residual"], "fp32_vs_fp64_solution_rel_err": err,
@@ -562,8 +618,8 @@ def run_abd(args):
 
 def main():
     args = parse()
-    if args.workload == "abd512":
-        return run_abd(args)
+    if args.workload in SCENE_WORKLOADS:
+        return run_scene(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch256":
