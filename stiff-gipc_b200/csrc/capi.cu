@@ -333,19 +333,22 @@ int stg_solve_linear_system(stg_handle h, const stg_system* sys, double* x, stg_
         const bool timed = stats != nullptr;
         cudaStream_t s = S.stream;
         const int l0 = S.launches;
+        const bool use_mas = S.cfg.preconditioner == STG_PRECOND_MAS;
         if(timed) STG_CUDA_TRY(cudaEventRecord(S.ev[0], s));
-        STG_TRY(S.convert(sys->triplet_count, sys->rows, sys->cols, sys->blocks, sys->n / 3));
+        // the MAS hierarchy depends on the mesh and the contacts only: built first, so that the
+        // convert can store level 0 and emit the level-1 triplets in the same pass
+        if(use_mas) STG_TRY(S.mas_build(sys->contacts, sys->ncp));
+        if(timed) STG_CUDA_TRY(cudaEventRecord(S.ev[5], s));
+        STG_TRY(S.convert(sys->triplet_count, sys->rows, sys->cols, sys->blocks, sys->n / 3,
+                          use_mas ? sys->fem_block_offset : -1));
         STG_TRY(S.prepare_spmv());
         if(timed) STG_CUDA_TRY(cudaEventRecord(S.ev[1], s));
-        if(S.cfg.preconditioner == STG_PRECOND_MAS)
+        if(use_mas)
         {
-            STG_TRY(S.mas_build(sys->contacts, sys->ncp));
-            if(timed) STG_CUDA_TRY(cudaEventRecord(S.ev[2], s));
             STG_TRY(S.mas_assemble(sys->fem_block_offset));
             S.mas_fem_offset = sys->fem_block_offset;
         }
-        else if(timed)
-            STG_CUDA_TRY(cudaEventRecord(S.ev[2], s));
+        if(timed) STG_CUDA_TRY(cudaEventRecord(S.ev[2], s));
         S.generation++;
         if(timed) STG_CUDA_TRY(cudaEventRecord(S.ev[3], s));
         int st = S.pcg_solve(sys->b, x, sys->n, sys->abd_bodies, sys->abd_inv, stats);
@@ -356,15 +359,15 @@ int stg_solve_linear_system(stg_handle h, const stg_system* sys, double* x, stg_
             double rel = 0;
             STG_TRY(stg::true_residual(S, sys->b, x, sys->n, &rel));
             STG_CUDA_TRY(cudaEventSynchronize(S.ev[4]));
-            float t01 = 0, t12 = 0, t23 = 0, t34 = 0, t04 = 0;
-            cudaEventElapsedTime(&t01, S.ev[0], S.ev[1]);
-            cudaEventElapsedTime(&t12, S.ev[1], S.ev[2]);
-            cudaEventElapsedTime(&t23, S.ev[2], S.ev[3]);
+            float t05 = 0, t51 = 0, t13 = 0, t34 = 0, t04 = 0;
+            cudaEventElapsedTime(&t05, S.ev[0], S.ev[5]);
+            cudaEventElapsedTime(&t51, S.ev[5], S.ev[1]);
+            cudaEventElapsedTime(&t13, S.ev[1], S.ev[3]);
             cudaEventElapsedTime(&t34, S.ev[3], S.ev[4]);
             cudaEventElapsedTime(&t04, S.ev[0], S.ev[4]);
-            stats->ms_convert = t01;
-            stats->ms_mas_build = t12;
-            stats->ms_mas_assemble = t23;
+            stats->ms_convert = t51;
+            stats->ms_mas_build = t05;
+            stats->ms_mas_assemble = t13;
             stats->ms_pcg = t34;
             stats->ms_total = t04;
             stats->rel_residual = rel;

@@ -13,6 +13,7 @@
 // is bitwise deterministic; the summation order (input order) equals that of a stable
 // sort followed by a sequential sum.
 #include "solver.hpp"
+#include "mas_index.cuh"
 
 namespace stg
 {
@@ -233,10 +234,43 @@ __global__ void __launch_bounds__(CONV_LONG_THREADS) k_conv_sort_long(const int*
 constexpr int CONV_EMIT_WARPS = 4;
 constexpr int CONV_EMIT_CAP = 128;
 
+// the fused level-0 pass for unique block o = (r, c) with sum acc (ConvFuse)
+__device__ __forceinline__ void fuse_block(const ConvFuse& F, int r, int c, const double* acc, int o)
+{
+    const int rr = r - F.offset, cc = c - F.offset;
+    const bool in = rr >= 0 && rr < F.V && cc >= 0 && cc < F.V;
+    bool lower_in_bank = false;
+    if(in)
+    {
+        const int sc = F.real_map[cc], sr = F.real_map[rr];
+        if(sc / F.B == sr / F.B)
+        {
+            if(sc >= sr)
+            {
+                double* D = F.mat + ((size_t)(sc / F.B) * F.NS + upper_index(F.B, sr % F.B, sc % F.B)) * 9;
+#pragma unroll
+                for(int e = 0; e < 9; e++) D[e] = acc[e];
+            }
+            else
+                lower_in_bank = true;
+        }
+    }
+    if(F.c1)
+    {
+        if(!in || lower_in_bank)
+        {
+            F.trow[o] = -1;
+            F.tcol[o] = 0;
+        }
+        else
+            coarse_triplet(rr, cc, F.c1[rr], F.c1[cc], acc, F.trow + o, F.tcol + o, F.tblk + 9 * (size_t)o);
+    }
+}
+
 __global__ void __launch_bounds__(32 * CONV_EMIT_WARPS) k_conv_emit(const double* blocks, const int* row_start,
                                                                     const int* perm, const int* scol,
                                                                     const int* ustart, int* out_rows, int* out_cols,
-                                                                    double* out_blocks, int nrows)
+                                                                    double* out_blocks, int nrows, ConvFuse F)
 {
     extern __shared__ double ebuf[];  // [CONV_EMIT_WARPS][CONV_EMIT_CAP * 9]
     const int warps = (gridDim.x * blockDim.x) >> 5;
@@ -289,6 +323,7 @@ __global__ void __launch_bounds__(32 * CONV_EMIT_WARPS) k_conv_emit(const double
                             out_cols[o] = cur;
 #pragma unroll
                             for(int t = 0; t < 9; t++) out_blocks[9 * (size_t)o + t] = acc[t];
+                            if(F.B) fuse_block(F, r, cur, acc, o);
                         }
                         o++;
                         cur = cj;
@@ -308,6 +343,7 @@ __global__ void __launch_bounds__(32 * CONV_EMIT_WARPS) k_conv_emit(const double
                 out_cols[o] = cur;
 #pragma unroll
                 for(int t = 0; t < 9; t++) out_blocks[9 * (size_t)o + t] = acc[t];
+                if(F.B) fuse_block(F, r, cur, acc, o);
             }
             __syncwarp();
             continue;
@@ -333,6 +369,7 @@ __global__ void __launch_bounds__(32 * CONV_EMIT_WARPS) k_conv_emit(const double
                 out_cols[o] = scol[s + a];
 #pragma unroll
                 for(int t = 0; t < 9; t++) out_blocks[9 * (size_t)o + t] = acc[t];
+                if(F.B) fuse_block(F, r, scol[s + a], acc, o);
             }
             base += __popc(hm);
         }
@@ -346,7 +383,7 @@ __global__ void __launch_bounds__(32 * CONV_EMIT_WARPS) k_conv_emit(const double
 // through *unique (one device->host read).
 int convert_into(Solver& S, ConvertScratch& cv, int count, const int* rows, const int* cols, const double* blocks,
                  int nrows, bool skip_negative, DBuf<int>& out_rows, DBuf<int>& out_cols, DBuf<double>& out_blocks,
-                 DBuf<int>& row_ptr, int* unique)
+                 DBuf<int>& row_ptr, int* unique, bool fuse)
 {
     cudaStream_t s = S.stream;
     *unique = 0;
@@ -393,26 +430,62 @@ int convert_into(Solver& S, ConvertScratch& cv, int count, const int* rows, cons
     STG_CUDA_TRY(cudaMemsetAsync(cv.uniq.data() + nrows, 0, sizeof(int), s));
     k_scan_exclusive<<<1, 1024, 0, s>>>(cv.uniq.data(), row_ptr.data(), nullptr, nrows + 1, cv.scratch.data() + 1);
     STG_LAUNCH_CHECK();
+    int h[2] = {0, 0};
+    ConvFuse F;
+    if(fuse)
+    {
+        // the fused level-0 pass needs the unique count first (its level-1 triplet arrays)
+        STG_CUDA_TRY(cudaMemcpyAsync(h, cv.scratch.data() + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        STG_CUDA_TRY(cudaStreamSynchronize(s));
+        if(h[1] != 0)
+        {
+            set_error("convert: " + std::to_string(h[1]) + " triplets have a row or col outside [0, " +
+                      std::to_string(nrows) + ")");
+            return STG_ERR_INVALID;
+        }
+        MasState& m = S.mas;
+        F.B = m.bank;
+        F.NS = nsym(m.bank);
+        F.offset = m.l0_offset;
+        F.V = m.V;
+        F.real_map = m.real_map.data();
+        const size_t nvals = (size_t)m.nbanks * F.NS * 9;
+        STG_TRY(m.mat.resize(nvals));
+        STG_CUDA_TRY(cudaMemsetAsync(m.mat.data(), 0, nvals * sizeof(double), s));
+        F.mat = m.mat.data();
+        if(m.L > 1 && h[0] > 0)
+        {
+            STG_TRY(m.tr_rows.resize(h[0]));
+            STG_TRY(m.tr_cols.resize(h[0]));
+            STG_TRY(m.tr_blocks.resize((size_t)h[0] * 9));
+            F.c1 = m.coarse_tables.data();
+            F.trow = m.tr_rows.data();
+            F.tcol = m.tr_cols.data();
+            F.tblk = m.tr_blocks.data();
+        }
+    }
     const int ge = std::min(div_up((long)nrows * 32, 32 * CONV_EMIT_WARPS), kSMs * 32);
     k_conv_emit<<<ge, 32 * CONV_EMIT_WARPS, sizeof(double) * CONV_EMIT_WARPS * CONV_EMIT_CAP * 9, s>>>(
         blocks, cv.row_start.data(), cv.perm2.data(), cv.scol.data(), row_ptr.data(), out_rows.data(), out_cols.data(),
-        out_blocks.data(), nrows);
+        out_blocks.data(), nrows, F);
     STG_LAUNCH_CHECK();
     S.launches += 7;
-    int h[2] = {0, 0};
-    STG_CUDA_TRY(cudaMemcpyAsync(h, cv.scratch.data() + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
-    STG_CUDA_TRY(cudaStreamSynchronize(s));
-    if(h[1] != 0)
+    if(!fuse)
     {
-        set_error("convert: " + std::to_string(h[1]) + " triplets have a row or col outside [0, " + std::to_string(nrows) +
-                  ")");
-        return STG_ERR_INVALID;
+        STG_CUDA_TRY(cudaMemcpyAsync(h, cv.scratch.data() + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        STG_CUDA_TRY(cudaStreamSynchronize(s));
+        if(h[1] != 0)
+        {
+            set_error("convert: " + std::to_string(h[1]) + " triplets have a row or col outside [0, " +
+                      std::to_string(nrows) + ")");
+            return STG_ERR_INVALID;
+        }
     }
     *unique = h[0];
     return 0;
 }
 
-int Solver::convert(int count, const int* rows, const int* cols, const double* blocks, int nrows_hint)
+int Solver::convert(int count, const int* rows, const int* cols, const double* blocks, int nrows_hint, int fuse_offset)
 {
     cudaStream_t s = stream;
     bcoo.nnzb = 0;
@@ -431,8 +504,12 @@ int Solver::convert(int count, const int* rows, const int* cols, const double* b
         launches += 1;
     }
     int total = 0;
+    const bool fuse = fuse_offset >= 0 && mas.built && mas.V > 0;
+    mas.l0_fused = false;
+    if(fuse) mas.l0_offset = fuse_offset;
     STG_TRY(convert_into(*this, cv, count, rows, cols, blocks, nrows, false, bcoo.rows, bcoo.cols, bcoo.blocks,
-                         bcoo.row_ptr, &total));
+                         bcoo.row_ptr, &total, fuse));
+    mas.l0_fused = fuse;
     bcoo.nnzb = total;
     bcoo.nrows = nrows;
     bcoo.external = false;

@@ -20,12 +20,11 @@
 // deterministic sort/merge of convert.cu instead of FP64 atomics (see the assembly section).
 #include "solver.hpp"
 #include "bank_dev.cuh"
+#include "mas_index.cuh"
 
 namespace stg
 {
 
-__host__ __device__ __forceinline__ int nsym(int B) { return B * (B + 1) / 2; }
-__host__ __device__ __forceinline__ int upper_index(int B, int r, int c) { return B * r - r * (r + 1) / 2 + c; }
 
 // group-local ballot: the B lanes of this lane's bank
 template <int B>
@@ -332,40 +331,6 @@ __global__ void k_mas_store_l0(const int* __restrict__ rows, const int* __restri
 #pragma unroll
         for(int e = 0; e < 9; e++) D[e] = H[e];
     }
-}
-
-// Map an upper block (u <= v) with value H to coarse nodes (a, b) and orient it upper:
-// a < b: H; a > b: H^T at (b, a); a == b: H (u == v) or H + H^T (u < v).
-__device__ __forceinline__ void coarse_triplet(int u, int v, int a, int b, const double* __restrict__ H, int* orow,
-                                               int* ocol, double* oblk)
-{
-    double h[9];
-#pragma unroll
-    for(int e = 0; e < 9; e++) h[e] = H[e];
-    if(a < b || (a == b && u == v))
-    {
-#pragma unroll
-        for(int e = 0; e < 9; e++) oblk[e] = h[e];
-    }
-    else if(a > b)
-    {
-#pragma unroll
-        for(int i = 0; i < 3; i++)
-#pragma unroll
-            for(int j = 0; j < 3; j++) oblk[j * 3 + i] = h[i * 3 + j];
-        const int t = a;
-        a = b;
-        b = t;
-    }
-    else
-    {
-#pragma unroll
-        for(int i = 0; i < 3; i++)
-#pragma unroll
-            for(int j = 0; j < 3; j++) oblk[j * 3 + i] = h[j * 3 + i] + h[i * 3 + j];
-    }
-    *orow = a;
-    *ocol = b;
 }
 
 // A_0 (FEM range of the BCOO) -> level-1 triplets; masked entries get row -1
@@ -929,7 +894,7 @@ int Solver::mas_build(const int* contacts, int ncp)
 
 int convert_into(Solver& S, ConvertScratch& cv, int count, const int* rows, const int* cols, const double* blocks,
                  int nrows, bool skip_negative, DBuf<int>& out_rows, DBuf<int>& out_cols, DBuf<double>& out_blocks,
-                 DBuf<int>& row_ptr, int* unique);
+                 DBuf<int>& row_ptr, int* unique, bool fuse = false);
 
 template <int B>
 static int mas_assemble_t(Solver& S, int offset)
@@ -943,11 +908,15 @@ static int mas_assemble_t(Solver& S, int offset)
     // R, Z: one {x y z 0} float4 slot per node of every level
     STG_TRY(m.R.resize((size_t)m.total_clusters * 4));
     STG_TRY(m.Z.resize((size_t)m.total_clusters * 4));
-    STG_CUDA_TRY(cudaMemsetAsync(m.mat.data(), 0, nvals * sizeof(double), s));
+    // the fine convert of stg_solve_linear_system already stored level 0 and emitted the
+    // level-1 triplets (ConvFuse) when it ran for this offset
+    const bool fused = m.l0_fused && m.l0_offset == offset;
+    m.l0_fused = false;
+    if(!fused) STG_CUDA_TRY(cudaMemsetAsync(m.mat.data(), 0, nvals * sizeof(double), s));
     STG_CUDA_TRY(cudaMemsetAsync(m.R.data(), 0, sizeof(float) * 4 * m.total_clusters, s));
     const int nnzb = S.bcoo.nnzb;
     const int g = std::max(1, std::min(div_up(nnzb, 256), kSMs * 16));
-    if(nnzb > 0)
+    if(nnzb > 0 && !fused)
     {
         k_mas_store_l0<B><<<g, 256, 0, s>>>(S.bcoo.R(), S.bcoo.C(), S.bcoo.B(), nnzb, offset, m.V, m.real_map.data(),
                                             m.mat.data());
@@ -959,13 +928,17 @@ static int mas_assemble_t(Solver& S, int offset)
     if(m.L > 1 && nnzb > 0)
     {
         // level 1 from the fine matrix
-        STG_TRY(m.tr_rows.resize(nnzb));
-        STG_TRY(m.tr_cols.resize(nnzb));
-        STG_TRY(m.tr_blocks.resize((size_t)nnzb * 9));
-        k_mas_agg_l0<B><<<g, 256, 0, s>>>(S.bcoo.R(), S.bcoo.C(), S.bcoo.B(), nnzb, offset, m.V, m.real_map.data(),
-                                          m.coarse_tables.data(), m.tr_rows.data(), m.tr_cols.data(), m.tr_blocks.data());
-        STG_LAUNCH_CHECK();
-        S.launches++;
+        if(!fused)
+        {
+            STG_TRY(m.tr_rows.resize(nnzb));
+            STG_TRY(m.tr_cols.resize(nnzb));
+            STG_TRY(m.tr_blocks.resize((size_t)nnzb * 9));
+            k_mas_agg_l0<B><<<g, 256, 0, s>>>(S.bcoo.R(), S.bcoo.C(), S.bcoo.B(), nnzb, offset, m.V,
+                                              m.real_map.data(), m.coarse_tables.data(), m.tr_rows.data(),
+                                              m.tr_cols.data(), m.tr_blocks.data());
+            STG_LAUNCH_CHECK();
+            S.launches++;
+        }
         int nnz = 0;
         STG_TRY(convert_into(S, m.gcv, nnzb, m.tr_rows.data(), m.tr_cols.data(), m.tr_blocks.data(), m.level_size[2],
                              true, m.ga_rows, m.ga_cols, m.ga_blocks, m.g_rowptr, &nnz));

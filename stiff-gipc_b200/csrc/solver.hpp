@@ -53,6 +53,21 @@ struct Bcoo
     const int* C() const { return external ? ext_cols : cols.data(); }
 };
 
+// The fine convert's fused level-0 pass (stg_solve_linear_system with MAS): every unique block
+// in the FEM range [offset, offset + V) is also written into its level-0 bank matrix (same
+// bank, upper) and, when c1 is given, turned into its level-1 Galerkin triplet at its own
+// index (row -1 where it is masked), as k_mas_store_l0 and k_mas_agg_l0 would from the BCOO.
+struct ConvFuse
+{
+    int B = 0, NS = 0, offset = 0, V = 0;
+    const int* real_map = nullptr;
+    const int* c1 = nullptr;
+    double* mat = nullptr;
+    int* trow = nullptr;
+    int* tcol = nullptr;
+    double* tblk = nullptr;
+};
+
 struct ConvertScratch
 {
     DBuf<int> row_cnt, row_start, cursor, perm, perm2, pcol, scol, uniq, scratch, long_rows;
@@ -61,6 +76,8 @@ struct ConvertScratch
 struct MasState
 {
     bool inited = false, built = false, assembled = false;
+    bool l0_fused = false;        // the last convert wrote level 0 and the level-1 triplets
+    int l0_offset = 0;            // ... for this FEM block offset
     bool identity = false;        // part_map[s] == s for s < V (Morton order): no slot indirection
     int bank = 16, V = 0, M = 0, L = 0, node_offset = 0, nlist_size = 0;
     int total_clusters = 0, nbanks = 0, nb0 = 0;
@@ -179,7 +196,9 @@ struct Solver
     ~Solver();
 
     // stages
-    int convert(int count, const int* rows, const int* cols, const double* blocks, int nrows_hint);
+    // fuse_offset >= 0 (MAS built): also the fused level-0 pass for that FEM block offset
+    int convert(int count, const int* rows, const int* cols, const double* blocks, int nrows_hint,
+                int fuse_offset = -1);
     int bind_bcoo(const double* blocks, const int* rows, const int* cols, int nnzb, int nrows);
     int prepare_spmv();   // row_ptr, transpose refs, FP32 copy, diag inverses
     int spmv(double a, const double* x, double b, double* y);

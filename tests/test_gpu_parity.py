@@ -346,6 +346,31 @@ def test_solve_with_contacts_end_to_end(dev, precision):
         assert np.linalg.norm(xg - xe) <= 1e-3 * np.linalg.norm(xe)
 
 
+@pytest.mark.parametrize("bank", [16, 32])
+def test_fused_level0_pass_bit_exact(dev, bank):
+    """stg_solve_linear_system builds the hierarchy first and lets the fine convert store the
+    level-0 bank blocks and emit the level-1 Galerkin triplets in its emit pass; the bank
+    matrices and inverses it leaves are bit-identical to the oracle's (and so to the
+    standalone stg_mas_assemble path's), here with contacts."""
+    from oracle import oracle as orc
+    from stgipc import PCGSolverConfig, Solver
+    s = cube_system(16)
+    cp = random_contacts(s.num_verts, 400, seed=29)
+    r, c, bl = _converted(s)
+    om = orc.Mas(bank, s.num_verts, s.neighbor_start, s.neighbor_num, s.neighbor_list, *s.slot_maps(bank))
+    om.build(cp)
+    om.assemble(r, c, bl)
+    em, ei = om.matrices()
+    solver = Solver(PCGSolverConfig(bank_size=bank))
+    solver.mas_init(s.num_verts, s.neighbor_start, s.neighbor_num, s.neighbor_list, *s.slot_maps(bank))
+    X = _t(np.zeros(s.n), dev)
+    st = solver.solve_linear_system(_t(s.rows, dev), _t(s.cols, dev), _t(s.blocks.reshape(-1), dev), _t(s.b, dev), X,
+                                    contacts=_t(cp, dev))
+    assert st["status"] == 0
+    gm, gi = solver.export_matrices()
+    assert np.array_equal(gm, em) and np.array_equal(gi, ei)
+
+
 def test_fp32_mode_relative_residual(dev):
     """FP32 SpMV/MAS storage, FP64 dots + residual replacement: FP64 residual <= 1e-4."""
     from oracle import oracle as orc
