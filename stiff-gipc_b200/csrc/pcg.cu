@@ -700,6 +700,34 @@ __device__ __forceinline__ unsigned smem_u32(const void* p)
     return (unsigned)__cvta_generic_to_shared(p);
 }
 
+// L2 eviction priorities for the bulk copies: the SpMV phase streams about 75 MB of block
+// planes per iteration, more than half of L2, which would push out the MAS bank inverses
+// (38.5 MB on the 352,947-DOF cube) and the vectors that the other phases reread every
+// iteration.  Its planes are copied evict-first and the inverses evict-last.
+__device__ __forceinline__ unsigned long long l2_evict_first()
+{
+    unsigned long long p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ unsigned long long l2_evict_last()
+{
+    unsigned long long p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ void tma_load_1d_hint(void* dst, const void* src, unsigned bytes, unsigned bar,
+                                                 unsigned long long policy)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
+        :
+        : "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(bar), "l"(policy)
+        : "memory");
+}
+
 __device__ __forceinline__ void tma_load_1d(void* dst, const void* src, unsigned bytes, unsigned bar)
 {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
@@ -756,8 +784,9 @@ __device__ __noinline__ bool mbar_wait_slow(unsigned bar, unsigned parity)
 __device__ __forceinline__ void d16_issue(const PcgDev& c, char* stage, unsigned bar, int bk)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"((unsigned)D_BUF) : "memory");
-    tma_load_1d(stage, c.inv + (size_t)bk * 136 * 9, D_PBYTES, bar);
-    tma_load_1d(stage + D_PBYTES, c.R + (size_t)bk * 16 * 4, D_RBYTES, bar);
+    const unsigned long long keep = l2_evict_last();
+    tma_load_1d_hint(stage, c.inv + (size_t)bk * 136 * 9, D_PBYTES, bar, keep);
+    tma_load_1d_hint(stage + D_PBYTES, c.R + (size_t)bk * 16 * 4, D_RBYTES, bar, keep);
 }
 
 // Banks [b0, b1).  guarded: only on residual-replacement iterations (host loop).
@@ -1089,13 +1118,14 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T, RTT>::MIN_CTAS) k_phase_a_
                         tma_load_1d(st + CAP * FP::ES, c.frow + rb + (size_t)k * RT, G::FROW, bf);
                         if(nc)
                         {
+                            const unsigned long long stream = l2_evict_first();
 #pragma unroll 1
                             for(int pl = 0; pl < FP::NP; pl++)
-                                tma_load_1d(st + (size_t)16 * pl * CAP, c.fent + 16 * (pl * c.fstride + F0a),
-                                            (unsigned)(16 * nc), bf);
-                            tma_load_1d(st + (size_t)16 * FP::NP * CAP,
-                                        c.fent + 16 * FP::NP * c.fstride + (size_t)FP::TAIL * F0a,
-                                        (unsigned)(FP::TAIL * nc), bf);
+                                tma_load_1d_hint(st + (size_t)16 * pl * CAP, c.fent + 16 * (pl * c.fstride + F0a),
+                                                 (unsigned)(16 * nc), bf, stream);
+                            tma_load_1d_hint(st + (size_t)16 * FP::NP * CAP,
+                                             c.fent + 16 * FP::NP * c.fstride + (size_t)FP::TAIL * F0a,
+                                             (unsigned)(FP::TAIL * nc), bf, stream);
                         }
                         issued = k + 1;
                     }
@@ -1429,10 +1459,13 @@ __device__ __forceinline__ void halo_issue(const PcgDev& c, unsigned char* hsm_,
         const unsigned own = (unsigned)((r1 - r0) * G::SLOT);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_expect_tx(bf, (unsigned)(n2 * FP::ES + G::FROW) + own);
+        const unsigned long long stream = l2_evict_first();
 #pragma unroll 1
         for(int pl = 0; pl < FP::NP; pl++)
-            tma_load_1d(st + (size_t)16 * pl * CAP, c.fent + 16 * (pl * c.fstride + F0a), (unsigned)(16 * n2), bf);
-        tma_load_1d(st + (size_t)16 * FP::NP * CAP, c.htail + (size_t)FP::TAIL * F0a, (unsigned)(FP::TAIL * n2), bf);
+            tma_load_1d_hint(st + (size_t)16 * pl * CAP, c.fent + 16 * (pl * c.fstride + F0a), (unsigned)(16 * n2), bf,
+                             stream);
+        tma_load_1d_hint(st + (size_t)16 * FP::NP * CAP, c.htail + (size_t)FP::TAIL * F0a, (unsigned)(FP::TAIL * n2),
+                         bf, stream);
         tma_load_1d(st + G::PLANES, c.frow + r0, G::FROW, bf);
         tma_load_1d(st + G::PLANES + G::FROW, zp + 8 * (size_t)r0, own, bf);
     }
