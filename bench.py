@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--batch-mode", choices=["concat", "streams"], default="concat",
                     help="batch256: one block-diagonal system per GPU, or one handle per scene on streams")
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
+    ap.add_argument("--spmv-tiles", type=int, default=None,
+                    help="hetcube48: SpMV kernel of the timed FP32 solves (stg_spmv_tiles: -3 upper, -2 halo, "
+                         "64 / 32 full-copy tiles); default: the library's choice")
     return ap.parse_args()
 
 
@@ -130,16 +133,23 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-PROFILE_A = "profiles/k_phase_a_tiled_hetcube48.md"
+# committed ncu summaries of the SpMV-phase kernels on the benchmark system
+PROFILE_A = {-3: ("k_phase_a_upper<float>", "profiles/k_phase_a_upper_hetcube48.md"),
+             64: ("k_phase_a_tiled<float, 64>", "profiles/k_phase_a_tiled_hetcube48.md")}
 
 
-def profiled_traffic(workload):
+def spmv_kernel(rows_per_tile):
+    """(kernel name, ncu summary path) of the FP32 SpMV phase stg_spmv_tiles_info reports."""
+    return PROFILE_A.get(rows_per_tile, (f"k_phase_a_tiled<float, {rows_per_tile}>", None))
+
+
+def profiled_traffic(workload, path):
     """DRAM bytes (read + write) of one SpMV-phase launch from the committed ncu summary of
     the same kernel on the same workload, or None."""
-    if workload != "hetcube48":
+    if workload != "hetcube48" or path is None:
         return None
     try:
-        for line in open(os.path.join(ROOT, PROFILE_A)):
+        for line in open(os.path.join(ROOT, path)):
             if line.startswith("traffic_bytes_per_launch:"):
                 return float(line.split(":")[1])
     except OSError:
@@ -656,6 +666,8 @@ def main():
                               graph_batch=args.batch, max_iter_ratio=0.3)
         s = Solver(cfg, stream=stream)
         s.mas_init(sysm.num_verts, sysm.neighbor_start, sysm.neighbor_num, sysm.neighbor_list, pm, rm)
+        if args.spmv_tiles is not None and precision == "fp32":
+            s.spmv_tiles(args.spmv_tiles)
         return s
 
     fast, plain = make("fp32"), make("fp64")
@@ -751,10 +763,10 @@ def main():
     tuned = make("fp32")
     tuned.spmv_tiles(0)
     solve(tuned)
-    rt_t, us_def, us_alt, us_halo = tuned.spmv_tiles_info()
+    rt_t, us_def, us_alt, us_halo, us_up = tuned.spmv_tiles_info()
     tuned.close()
-    tiles = {"default_rows_per_tile": 64, "tuned": "halo" if rt_t == -2 else f"{rt_t} rows per tile",
-             "us_per_launch": {"tiled 64x4": us_def, "tiled 32x8": us_alt, "halo 64x4": us_halo}}
+    tiles = {"tuned": {-2: "halo", -3: "upper"}.get(rt_t, f"{rt_t} rows per tile"),
+             "us_per_launch": {"tiled 64x4": us_def, "tiled 32x8": us_alt, "halo 64x4": us_halo, "upper 64x4": us_up}}
 
     # roofline of the dominant kernel: the PCG SpMV of the FP32 path, timed live
     solve(fast)
@@ -776,7 +788,8 @@ def main():
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
-    traffic = profiled_traffic(args.workload)
+    spmv_name, spmv_profile = spmv_kernel(fast.spmv_tiles_info()[0])
+    traffic = profiled_traffic(args.workload, spmv_profile)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -822,9 +835,9 @@ def main():
             "fp32_vs_fp64_solution_rel_err": err_fast,
             "phases_ms": {k: round(st_fast[k], 3) for k in ("ms_convert", "ms_mas_build", "ms_mas_assemble", "ms_pcg")},
             "dof_iter_per_s": sysm.n * st_fast["iterations"] / (ms_fast * 1e-3),
-            "roofline": {"bound": "hbm", "kernel": "k_phase_a_tiled<float>", "achieved": achieved, "peak": hbm,
+            "roofline": {"bound": "hbm", "kernel": spmv_name, "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
-                         "traffic_source": PROFILE_A if traffic else None,
+                         "traffic_source": spmv_profile if traffic else None,
                          "timing": "each launch alone after reading a 256 MiB buffer (L2 cold), CUDA events",
                          "bytes_per_launch": spmv_bytes, "ms_per_launch": spmv_ms,
                          "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650"},

@@ -370,19 +370,21 @@ int stg_segment_stats(stg_handle h, int* iterations, double* rel_residual);
 /* ---- BCOO tile autotuner -------------------------------------------------------------- */
 /* No counterpart in the reference.  Kernel of the in-loop SpMV: rows_per_tile rows per
  * tile of the row-sliced full copy, with 256 / rows_per_tile lanes per row (FP32: 64 or 32;
- * FP64: 32 or 16), or -2: the halo kernel (fixed tiles whose column operands are staged in
- * shared memory).  0 = autotune: the next solve of a new shape class (precision, block rows,
- * unique blocks) times every candidate (both tile shapes, and the halo kernel when its
- * windows fit) on that system; the choice is kept for that shape class by every handle of
- * the process.  -1 = the precision's default shape (64 / 32).  Results differ between
- * candidates in the last bits (summation order); a fixed choice keeps solves bitwise
- * reproducible across processes. */
+ * FP64: 32 or 16); -2: the halo kernel (fixed tiles whose column operands are staged in
+ * shared memory); -3: the upper kernel (each upper block streamed once, its transposed
+ * product spilled to the column's row and added there in a fixed order).  0 = autotune: the
+ * next solve of a new shape class (precision, block rows, unique blocks) times every
+ * candidate (both tile shapes, the upper kernel, and the halo kernel when its windows fit)
+ * on that system; the choice is kept for that shape class by every handle of the process.
+ * -1 = the default kernel.  The persistent loop always runs the full-copy SpMV.  Results
+ * differ between candidates in the last bits (summation order); a fixed choice keeps solves
+ * bitwise reproducible across processes. */
 int stg_spmv_tiles(stg_handle h, int rows_per_tile);
-/* Rows per tile of the last solve (-2: the halo kernel), and the autotuner's mean time per
- * launch of each candidate in microseconds (0 when it has not run or the candidate did not
- * fit). */
+/* Kernel of the last solve (rows per tile; -2: the halo kernel; -3: the upper kernel), and
+ * the autotuner's mean time per launch of each candidate in microseconds (0 when it has not
+ * run or the candidate did not fit). */
 int stg_spmv_tiles_info(stg_handle h, int* rows_per_tile, float* us_default, float* us_alternative,
-                        float* us_halo);
+                        float* us_halo, float* us_upper);
 
 /* ---- allocation-free SpMV ---------------------------------------------------------- */
 /* No counterpart in the reference.  The same y = a * A * x + b * y as stg_spmv (same

@@ -708,27 +708,30 @@ int stg_spmv_tiles(stg_handle h, int rows_per_tile)
 {
     CHECK_HANDLE(h);
     const bool fp32 = h->cfg.precision == STG_PREC_FP32;
-    const bool ok = rows_per_tile == 0 || rows_per_tile == -1 || rows_per_tile == -2 ||
+    const bool ok = rows_per_tile == 0 || rows_per_tile == -1 || rows_per_tile == -2 || rows_per_tile == -3 ||
                     (fp32 ? (rows_per_tile == 64 || rows_per_tile == 32) : (rows_per_tile == 32 || rows_per_tile == 16));
     if(!ok)
     {
-        stg::set_error("stg_spmv_tiles: rows per tile must be 0 (autotune), -1 (default), -2 (halo kernel), 64 or 32 "
-                       "(FP32), 32 or 16 (FP64)");
+        stg::set_error("stg_spmv_tiles: rows per tile must be 0 (autotune), -1 (default), -2 (halo kernel), -3 (upper "
+                       "kernel), 64 or 32 (FP32), 32 or 16 (FP64)");
         return STG_ERR_INVALID;
     }
-    h->spmv_rt = rows_per_tile == -2 ? -2 : (rows_per_tile > 0 ? rows_per_tile : 0);
+    h->spmv_rt = (rows_per_tile == -2 || rows_per_tile == -3) ? rows_per_tile : (rows_per_tile > 0 ? rows_per_tile : 0);
     h->spmv_tune = rows_per_tile == 0;
     h->tuned_prec = -1;
     return STG_OK;
 }
 
-int stg_spmv_tiles_info(stg_handle h, int* rows_per_tile, float* us_default, float* us_alternative, float* us_halo)
+int stg_spmv_tiles_info(stg_handle h, int* rows_per_tile, float* us_default, float* us_alternative, float* us_halo,
+                        float* us_upper)
 {
     CHECK_HANDLE(h);
-    if(rows_per_tile) *rows_per_tile = h->pcg_ready ? (h->pcg_dev.halo ? -2 : h->pcg_dev.a_rt) : -1;
+    if(rows_per_tile)
+        *rows_per_tile = h->pcg_ready ? (h->pcg_dev.upper ? -3 : (h->pcg_dev.halo ? -2 : h->pcg_dev.a_rt)) : -1;
     if(us_default) *us_default = h->tune_us[0];
     if(us_alternative) *us_alternative = h->tune_us[1];
     if(us_halo) *us_halo = h->tune_us[2];
+    if(us_upper) *us_upper = h->tune_us[3];
     return STG_OK;
 }
 

@@ -338,6 +338,43 @@ __device__ __forceinline__ double phase_a(const PcgDev& c, int gt, int gn)
     return acc;
 }
 
+// The transposed products H_k^T p_row(k) that the upper SpMV phase spilled for row i (slots
+// t0 .. t1 of its transpose list), added to q_i in list order: a fixed order, so the sum is
+// deterministic.  SPB slots are loaded at a time, all loads of a batch before the first add.
+constexpr int SPB = 8;
+template <typename T>
+__device__ __forceinline__ void spill_add(const PcgDev& c, int t0, int t1, T& q0, T& q1, T& q2)
+{
+    const T* sp = reinterpret_cast<const T*>(c.spill);
+    for(int tb = t0; tb < t1; tb += SPB)
+    {
+        T a[SPB][3];
+#pragma unroll
+        for(int u = 0; u < SPB; u++)
+        {
+            a[u][0] = a[u][1] = a[u][2] = T(0);
+            if(tb + u < t1) ld4(sp + 4 * (size_t)(tb + u), a[u][0], a[u][1], a[u][2]);
+        }
+#pragma unroll
+        for(int u = 0; u < SPB; u++)
+            if(tb + u < t1)
+            {
+                q0 += a[u][0];
+                q1 += a[u][1];
+                q2 += a[u][2];
+            }
+    }
+}
+
+// q_i of the SpMV phase: after the upper kernel (c.spill set) q holds the upper part of the
+// row, and its spilled products are added here
+template <typename T>
+__device__ __forceinline__ void load_q(const PcgDev& c, const T* q, size_t i, T& q0, T& q1, T& q2)
+{
+    ld4(q + 4 * i, q0, q1, q2);
+    if(c.spill) spill_add<T>(c, __ldg(c.t_ptr + i), __ldg(c.t_ptr + i + 1), q0, q1, q2);
+}
+
 // B (MAS): axpy over the FEM range in level-0 slot order + level-0/1 restriction; plain axpy
 // over the ABD range.  Returns this thread's share of r.r.
 // x_i += alpha p_i; r_i -= alpha q_i for block row i (3 dofs); returns the new r_i and adds
@@ -348,7 +385,7 @@ __device__ __forceinline__ void axpy_row(const PcgDev& c, const T* pn, const T* 
 {
     T p0, p1, p2, q0, q1, q2;
     ld4(pn + 8 * (size_t)i + 4, p0, p1, p2);
-    ld4(q + 4 * (size_t)i, q0, q1, q2);
+    load_q<T>(c, q, (size_t)i, q0, q1, q2);
     double* x = c.x + 3 * (size_t)i;
     double* r = c.r + 3 * (size_t)i;
     x[0] += alpha * (double)p0;
@@ -364,7 +401,8 @@ __device__ __forceinline__ void axpy_row(const PcgDev& c, const T* pn, const T* 
 }
 
 // One level-0 slot of phase B (MAS): its row's p, q, x, r, closed mask and level-1 parent,
-// loaded before alpha is known (the loads do not depend on it)
+// loaded before alpha is known (the loads do not depend on it), and after the upper SpMV the
+// bounds of its row's spilled products (loaded and added to q when the slot is updated)
 template <typename T>
 struct BSlot
 {
@@ -373,9 +411,12 @@ struct BSlot
     double x[3], r[3];
     unsigned msk = 0u;
     int gnext = 0;
+    int t0 = 0, t1 = 0;
 };
 
-template <typename T>
+// SPILL: q may need the upper SpMV's spilled products (the persistent kernel never runs that
+// SpMV and compiles without the loop: with it, ptxas 12.9 for sm_100a aborts on that kernel)
+template <typename T, bool SPILL = true>
 __device__ __forceinline__ void b_load(const PcgDev& c, const T* pn, const T* q, int s, BSlot<T>& L)
 {
     L.v = c.identity ? (s < c.V ? s : -1) : (s < c.M ? c.part_map[s] : -1);
@@ -383,6 +424,14 @@ __device__ __forceinline__ void b_load(const PcgDev& c, const T* pn, const T* q,
     const size_t row = (size_t)(c.fem_dof / 3) + L.v;
     ld4(pn + 8 * row + 4, L.p[0], L.p[1], L.p[2]);
     ld4(q + 4 * row, L.q[0], L.q[1], L.q[2]);
+    if constexpr(SPILL)
+    {
+        if(c.spill)
+        {
+            L.t0 = __ldg(c.t_ptr + row);
+            L.t1 = __ldg(c.t_ptr + row + 1);
+        }
+    }
 #pragma unroll
     for(int d = 0; d < 3; d++)
     {
@@ -396,14 +445,31 @@ __device__ __forceinline__ void b_load(const PcgDev& c, const T* pn, const T* q,
 // x_i += alpha p_i, r_i -= alpha q_i of the slot, the level-0 residual slot and the level-0 ->
 // 1 restriction (each component of a level-0 bank sums its members in lane order); every lane
 // of the warp calls it (group shuffles).  Returns the slot's |r_i|^2.
+// st / [slo, shi): the calling warp's staged spill slots (shared memory), or null
 template <typename T, int B>
-__device__ __forceinline__ double b_update(const PcgDev& c, BSlot<T>& L, int s, double alpha)
+__device__ __forceinline__ double b_update(const PcgDev& c, BSlot<T>& L, int s, double alpha, const T* st = nullptr,
+                                           int slo = 0, int shi = 0)
 {
     float r0 = 0.f, r1 = 0.f, r2 = 0.f;
     double rr = 0.0;
     if(L.v >= 0)
     {
         const size_t row = (size_t)(c.fem_dof / 3) + L.v;
+        if(L.t1 > L.t0)
+        {
+            if(st && L.t0 >= slo && L.t1 <= shi)
+            {
+                for(int t = L.t0; t < L.t1; t++)
+                {
+                    const T* a = st + 4 * (t - slo);
+                    L.q[0] += a[0];
+                    L.q[1] += a[1];
+                    L.q[2] += a[2];
+                }
+            }
+            else
+                spill_add<T>(c, L.t0, L.t1, L.q[0], L.q[1], L.q[2]);
+        }
         const double a = c.seg_of_row ? __ldcg(c.seg + SEG_N * c.seg_of_row[row] + SG_ALPHA) : alpha;
 #pragma unroll
         for(int d = 0; d < 3; d++)
@@ -441,9 +507,9 @@ __device__ __forceinline__ double b_update(const PcgDev& c, BSlot<T>& L, int s, 
 // B (MAS): x / r update over the FEM range in level-0 slot order + level-0/1 restriction;
 // plain axpy over the ABD range.  `first` (with have_first): slot gt's loads, issued by the
 // caller before alpha was known.  Returns this thread's share of r.r.
-template <typename T, int B>
+template <typename T, int B, bool SPILL = true>
 __device__ __forceinline__ double phase_b_mas(const PcgDev& c, int gt, int gn, double alpha, BSlot<T>& first,
-                                              bool have_first)
+                                              bool have_first, const T* st = nullptr, int slo = 0, int shi = 0)
 {
     const T* pn = zpbuf<T>(c, iter_parity(c) ^ 1);
     const T* q = reinterpret_cast<const T*>(c.q);
@@ -452,13 +518,13 @@ __device__ __forceinline__ double phase_b_mas(const PcgDev& c, int gt, int gn, d
     int s = gt;
     if(have_first && s < span)
     {
-        acc += b_update<T, B>(c, first, s, alpha);
+        acc += b_update<T, B>(c, first, s, alpha, st, slo, shi);
         s += gn;
     }
     for(; s < span; s += gn)
     {
         BSlot<T> L;
-        b_load<T>(c, pn, q, s, L);
+        b_load<T, SPILL>(c, pn, q, s, L);
         acc += b_update<T, B>(c, L, s, alpha);
     }
     for(int i = gt; i < c.abd_bodies * 4; i += gn)
@@ -899,7 +965,8 @@ constexpr int A_THREADS = (A_CW + 1) * 32;
 // default for each precision is the first of its candidates; the autotuner may pick the
 // other (Solver::spmv_rt).
 template <typename T> constexpr int a_rt_default() { return sizeof(T) == 4 ? 64 : 32; }
-constexpr int SPMV_HALO = -2;  // stg_spmv_tiles value selecting the halo kernel
+constexpr int SPMV_HALO = -2;   // stg_spmv_tiles value selecting the halo kernel
+constexpr int SPMV_UPPER = -3;  // stg_spmv_tiles value selecting the upper kernel
 
 // The autotuner's choices, one per shape class (precision, block rows, unique blocks) for
 // the whole process: the first handle that meets a class times the candidates, every later
@@ -915,7 +982,7 @@ struct TuneKey
 struct TuneVal
 {
     int pick;
-    float us[3];
+    float us[4];
 };
 static std::mutex g_tune_mu;
 static std::map<TuneKey, TuneVal> g_tune;
@@ -926,14 +993,14 @@ static bool tuned_choice(int prec, int nrows, int nnzb, int* pick, float* us)
     const auto it = g_tune.find(TuneKey{prec, nrows, nnzb});
     if(it == g_tune.end()) return false;
     *pick = it->second.pick;
-    for(int i = 0; i < 3; i++) us[i] = it->second.us[i];
+    for(int i = 0; i < 4; i++) us[i] = it->second.us[i];
     return true;
 }
 
 static void record_choice(int prec, int nrows, int nnzb, int pick, const float* us)
 {
     std::lock_guard<std::mutex> lock(g_tune_mu);
-    TuneVal v{pick, {us[0], us[1], us[2]}};
+    TuneVal v{pick, {us[0], us[1], us[2], us[3]}};
     g_tune[TuneKey{prec, nrows, nnzb}] = v;
 }
 template <typename T> constexpr int a_rt_alt() { return sizeof(T) == 4 ? 32 : 16; }
@@ -1009,13 +1076,30 @@ __device__ __forceinline__ void lds_main(unsigned sb, int f, double h[9])
                      : "r"(sb + 16u * p * CAP + 16u * f));
 }
 
+// a row's whole zp slot {z0 z1 z2 -, p0 p1 p2 -} in one 32-byte load (FP32) or two (FP64)
+// (sm_100 256-bit vector loads; the slots are 32- / 64-byte aligned): a neighbour gather is
+// one L1 wavefront per lane instead of two (FP32) or four (FP64)
+__device__ __forceinline__ void ld_zp(const float* a, float& z0, float& z1, float& z2, float& p0, float& p1, float& p2)
+{
+    float w0, w1;
+    asm("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(z0), "=f"(z1), "=f"(z2), "=f"(w0), "=f"(p0), "=f"(p1), "=f"(p2), "=f"(w1)
+        : "l"(a));
+}
+__device__ __forceinline__ void ld_zp(const double* a, double& z0, double& z1, double& z2, double& p0, double& p1,
+                                      double& p2)
+{
+    double w0, w1;
+    asm("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(z0), "=d"(z1), "=d"(z2), "=d"(w0) : "l"(a));
+    asm("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(p0), "=d"(p1), "=d"(p2), "=d"(w1) : "l"(a + 4));
+}
+
 // v_j = z_j + beta p_j gathered from the zp slots
 template <typename T>
 __device__ __forceinline__ void a_gather(int j, const T* zp, T beta, T& x0, T& x1, T& x2)
 {
     T p0, p1, p2;
-    ld4(zp + 8 * (size_t)j, x0, x1, x2);
-    ld4(zp + 8 * (size_t)j + 4, p0, p1, p2);
+    ld_zp(zp + 8 * (size_t)j, x0, x1, x2, p0, p1, p2);
     x0 += beta * p0;
     x1 += beta * p1;
     x2 += beta * p2;
@@ -1261,6 +1345,306 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T, RTT>::MIN_CTAS) k_phase_a_
         }
     }
     // p.q: this CTA's partial only; phase B finishes the sum (consume_sum)
+    __shared__ double red[A_THREADS / 32];
+    const double bs = block_sum<A_THREADS>(acc, red);
+    if(threadIdx.x == 0) c.partials[(size_t)SITE_A * c.slots + blockIdx.x] = bs;
+}
+
+// ---------------------------------------------------------------------------------------
+// A, upper: the SpMV phase streaming each upper block once (UpperPlanes).  The tiling, the
+// bulk-copy ring and the bounded waits are those of k_phase_a_tiled, over the upper copy's
+// entry ranges [row_ptr[r0], row_ptr[r1]) (rounded out to multiples of 4 entries, so that
+// every plane's copy is a 16-byte multiple).  For block k of row i (column j):
+//   - the row's lanes add H_k v_j to q_i in entry order (v = z + beta p gathered; v_i, which
+//     every lane of the row gathers once, is p_new of the row), exactly as the full-copy
+//     kernel adds its upper entries;
+//   - j > i: the lane writes H_k^T v_i into the spill slot of k (its place in row j's
+//     transpose list); phase B adds row j's slots to q_j in list order, so every row's sum
+//     has a fixed order and the phase stays deterministic.
+// q therefore holds the upper part of A p only.  p.q = p^T A p is formed from it without the
+// spilled part: p^T A p = sum_i (2 v_i . (upper row i of A) v - v_i . H_ii v_i).
+// ---------------------------------------------------------------------------------------
+// First row of CTA b of the upper SpMV phase's G CTAs (multiples of 4, so that every tile's
+// row-bound copy is 16-byte aligned); CTA b owns [a_range_start(b), a_range_start(b + 1)).
+__host__ __device__ __forceinline__ int a_range_start(long long b, int G, int nrows)
+{
+    return b == 0 ? 0 : (b >= G ? nrows : (int)((b * nrows / G) & ~3LL));
+}
+
+template <typename T>
+struct AUpper
+{
+    using UP = UpperPlanes<T>;
+    // a row holds about half the entries of its full-copy row: two entries per lane and
+    // batch, and a stage about half the size of the full-copy kernel's, so that three CTAs
+    // fit per SM (72 registers per thread): the phase is latency-bound, and the third CTA
+    // hides more of the gathers' latency than deeper batches or a deeper ring did
+    static constexpr int RT = sizeof(T) == 4 ? 64 : 32;            // rows per tile
+    static constexpr int LPR = 32 * A_CW / RT;                     // consumer lanes per row
+    static constexpr int CAP = 9 * RT;                             // entries per stage (mult. of 4)
+    static constexpr int UB = 2;                                   // entries per lane per batch
+    static constexpr int STAGES = 2;
+    static constexpr int FROW = 4 * (RT + 4);                      // row_ptr[r0 .. r0 + RT + 4)
+    static constexpr int SLOT_OFF = (16 * UP::NP + UP::TAIL) * CAP;  // FP32 slot plane in a stage
+    static constexpr int STAGE = CAP * UP::ES + FROW;
+    static constexpr int META = 16 * STAGES;
+    static constexpr int BARS = 16 * STAGES;
+    static constexpr int SMEM = STAGES * STAGE + META + BARS;
+    static constexpr int MIN_CTAS = 3;
+    static_assert(STAGE % 16 == 0 && SLOT_OFF % 16 == 0, "stage planes must stay 16-byte aligned");
+    static_assert(RT + 4 <= 136, "row-bound copies must stay inside the padded row pointers");
+};
+
+// tail {h8, col} and spill slot of stage entry f
+template <int CAP, int SLOT_OFF>
+__device__ __forceinline__ void lds_utail(unsigned sb, int f, float& h8, int& col, int& slot)
+{
+    unsigned tc;
+    asm volatile("ld.shared.v2.b32 {%0, %1}, [%2];" : "=f"(h8), "=r"(tc) : "r"(sb + 32u * CAP + 8u * f));
+    col = (int)tc;
+    slot = lds_s32(sb + SLOT_OFF + 4u * f);
+}
+template <int CAP, int SLOT_OFF>
+__device__ __forceinline__ void lds_utail(unsigned sb, int f, double& h8, int& col, int& slot)
+{
+    unsigned long long tc;
+    asm volatile("ld.shared.v2.b64 {%0, %1}, [%2];" : "=d"(h8), "=l"(tc) : "r"(sb + 64u * CAP + 16u * f));
+    col = (int)(unsigned)tc;
+    slot = (int)(unsigned)(tc >> 32);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(A_THREADS, AUpper<T>::MIN_CTAS) k_phase_a_upper(PcgDev c)
+{
+    using G = AUpper<T>;
+    using UP = UpperPlanes<T>;
+    constexpr int RT = G::RT, LPR = G::LPR, CAP = G::CAP;
+    extern __shared__ __align__(128) unsigned char asm_[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rb = a_range_start(blockIdx.x, gridDim.x, c.nrows), re = a_range_start(blockIdx.x + 1LL, gridDim.x, c.nrows);
+    const int mine = re > rb ? (re - rb + RT - 1) / RT : 0;
+    const int done = __ldcg(c.flags + F_DONE);
+    const double s_iter = __ldcg(c.scal + SS_ITER), rz_old = __ldcg(c.scal + SS_RZ);
+    int lo = 0, hi = 0;  // producer: entry bounds of the next 32 tiles, one per lane
+    if(warp == A_CW && lane < mine)
+    {
+        const int r0 = rb + lane * RT;
+        lo = __ldg(c.urow + r0);
+        hi = __ldg(c.urow + min(r0 + RT, re));
+    }
+    if(done) return;
+    double rz_new, rz_mix = 0.0;
+    if(c.flex && (long)s_iter > 0)
+        consume_sum2<A_THREADS>(c, SITE_E, c.grid_e, SITE_F, c.grid_e, rz_new, rz_mix);
+    else
+        rz_new = consume_sum<A_THREADS>(c, SITE_E, c.grid_e);
+    const double s_beta = (long)s_iter == 0 ? 0.0 : (rz_new - rz_mix) / rz_old;
+    int* meta = reinterpret_cast<int*>(asm_ + G::STAGES * G::STAGE);
+    const unsigned sbase = smem_u32(asm_);
+    const unsigned bar_full = smem_u32(asm_ + G::STAGES * G::STAGE + G::META);
+    const unsigned bar_empty = bar_full + 8 * G::STAGES;
+    if(threadIdx.x == 0)
+    {
+        for(int s = 0; s < G::STAGES; s++)
+        {
+            mbar_init(bar_full + 8 * s, 1);
+            mbar_init(bar_empty + 8 * s, A_CW);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    const int par = ((long)s_iter) & 1;
+    const T* zp = zpbuf<T>(c, par);
+    T* zpn = zpbuf<T>(c, par ^ 1);
+    T* q = reinterpret_cast<T*>(c.q);
+    T* spill = reinterpret_cast<T*>(c.spill);
+    const T beta = (T)s_beta;
+    double acc = 0;
+    bool failed = false;
+
+    if(warp == A_CW)
+    {
+        // ---- producer warp: lane 0 issues, all lanes fetch the tile bounds ----
+        int issued = 0;
+        for(int k0 = 0; k0 < mine && !failed; k0 += 32)
+        {
+            if(k0 > 0)
+            {
+                lo = hi = 0;
+                if(k0 + lane < mine)
+                {
+                    const int r0 = rb + (k0 + lane) * RT;
+                    lo = __ldg(c.urow + r0);
+                    hi = __ldg(c.urow + min(r0 + RT, re));
+                }
+            }
+            const int cnt = min(32, mine - k0);
+            for(int u = 0; u < cnt; u++)
+            {
+                const int F0 = __shfl_sync(0xffffffffu, lo, u), F1 = __shfl_sync(0xffffffffu, hi, u);
+                const int k = k0 + u, s = k % G::STAGES;
+                if(lane == 0)
+                {
+                    if(k >= G::STAGES && !mbar_wait(bar_empty + 8 * s, ((k / G::STAGES) - 1) & 1)) failed = true;
+                    if(!failed)
+                    {
+                        // 4-entry aligned range: F0a + n4 <= round_up(nnzb, 4) <= the plane stride
+                        const int F0a = F0 & ~3, n4 = ((F1 + 3) & ~3) - F0a;
+                        const bool ovf = n4 > CAP;
+                        const int nc = ovf ? 0 : n4;
+                        meta[4 * s] = F0a;
+                        meta[4 * s + 1] = ovf ? 1 : 0;
+                        unsigned char* st = asm_ + (size_t)s * G::STAGE;
+                        const unsigned bf = bar_full + 8 * s;
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        mbar_expect_tx(bf, (unsigned)(G::FROW + nc * UP::ES));
+                        tma_load_1d(st + CAP * UP::ES, c.urow + rb + (size_t)k * RT, G::FROW, bf);
+                        if(nc)
+                        {
+                            const unsigned long long stream = l2_evict_first();
+                            const size_t S = c.ustride;
+#pragma unroll 1
+                            for(int pl = 0; pl < UP::NP; pl++)
+                                tma_load_1d_hint(st + (size_t)16 * pl * CAP, c.uent + 16 * (pl * S + F0a),
+                                                 (unsigned)(16 * nc), bf, stream);
+                            tma_load_1d_hint(st + (size_t)16 * UP::NP * CAP, c.uent + 16 * UP::NP * S + (size_t)UP::TAIL * F0a,
+                                             (unsigned)(UP::TAIL * nc), bf, stream);
+                            if constexpr(UP::SLOTP > 0)
+                                tma_load_1d_hint(st + G::SLOT_OFF, c.uent + (16 * UP::NP + UP::TAIL) * S + (size_t)UP::SLOTP * F0a,
+                                                 (unsigned)(UP::SLOTP * nc), bf, stream);
+                        }
+                        issued = k + 1;
+                    }
+                }
+                failed = __shfl_sync(0xffffffffu, failed ? 1 : 0, 0) != 0;
+                if(failed) break;
+            }
+        }
+        if(lane == 0)
+        {
+            if(failed)
+            {
+                atomicExch(c.flags + F_STATUS, 6);  // STG_ERR_TIMEOUT
+                atomicExch(c.flags + F_DONE, 1);
+            }
+            for(int k = max(0, issued - G::STAGES); k < issued; k++)
+                mbar_wait(bar_full + 8 * (k % G::STAGES), (k / G::STAGES) & 1);
+        }
+    }
+    else
+    {
+        // ---- consumer warps: LPR lanes per row; lane `sub` of row r sums the entries
+        //      sub, sub + LPR, ... of the row in order, UB at a time ----
+        const int sub = lane & (LPR - 1);
+        const int rloc = warp * (32 / LPR) + lane / LPR;
+        for(int k = 0; k < mine; k++)
+        {
+            const int s = k % G::STAGES;
+            const int r0 = rb + k * RT, r1 = min(r0 + RT, re);
+            const int i = r0 + rloc;
+            // v_i (p_new of the row) does not depend on the stage: gather it before the wait
+            const T bta = (c.seg_of_row && i < r1) ? (T)__ldcg(c.seg + SEG_N * c.seg_of_row[i] + SG_BETA) : beta;
+            T v0 = T(0), v1 = T(0), v2 = T(0);
+            if(i < r1) a_gather<T>(i, zp, bta, v0, v1, v2);
+            if(!__all_sync(0xffffffffu, mbar_wait(bar_full + 8 * s, (k / G::STAGES) & 1)))
+            {
+                failed = true;
+                break;
+            }
+            const unsigned sb = sbase + (unsigned)(s * G::STAGE);
+            const unsigned sfrow = sb + CAP * UP::ES;
+            const int F0a = meta[4 * s];
+            const bool ovf = meta[4 * s + 1] != 0;
+            int f = 0, d = 0;
+            if(i < r1)
+            {
+                const int x0 = lds_s32(sfrow + 4 * rloc), x1 = lds_s32(sfrow + 4 * rloc + 4);
+                f = x0 - F0a;
+                d = x1 - x0;
+            }
+            T y0 = T(0), y1 = T(0), y2 = T(0);
+            double dd = 0.0;  // v_i . H_ii v_i
+            for(int e0 = sub; e0 < d; e0 += G::UB * LPR)
+            {
+                T h8[G::UB], x[G::UB][3];
+                int j[G::UB], sl[G::UB];
+#pragma unroll
+                for(int u = 0; u < G::UB; u++)
+                {
+                    const int e = e0 + u * LPR;
+                    h8[u] = T(0);
+                    j[u] = i;
+                    sl[u] = -1;
+                    if(e < d)
+                    {
+                        if(!ovf)
+                            lds_utail<CAP, G::SLOT_OFF>(sb, f + e, h8[u], j[u], sl[u]);
+                        else
+                        {
+                            T hh[9];
+                            ldg_upper(c.uent, c.ustride, F0a + f + e, hh, j[u], sl[u]);
+                            h8[u] = hh[8];
+                        }
+                    }
+                }
+#pragma unroll
+                for(int u = 0; u < G::UB; u++)
+                {
+                    x[u][0] = v0;
+                    x[u][1] = v1;
+                    x[u][2] = v2;
+                    if(e0 + u * LPR < d && j[u] != i) a_gather<T>(j[u], zp, bta, x[u][0], x[u][1], x[u][2]);
+                }
+#pragma unroll
+                for(int u = 0; u < G::UB; u++)
+                {
+                    const int e = e0 + u * LPR;
+                    if(e < d)
+                    {
+                        T h[9];
+                        int jj, ss;
+                        if(!ovf)
+                            lds_main<CAP>(sb, f + e, h);
+                        else
+                            ldg_upper(c.uent, c.ustride, F0a + f + e, h, jj, ss);
+                        h[8] = h8[u];
+                        mv3<T>(h, false, x[u][0], x[u][1], x[u][2], y0, y1, y2);
+                        T t0 = T(0), t1 = T(0), t2 = T(0);
+                        mv3<T>(h, j[u] != i, v0, v1, v2, t0, t1, t2);
+                        if(j[u] == i)
+                            dd += (double)v0 * (double)t0 + (double)v1 * (double)t1 + (double)v2 * (double)t2;
+                        else if(sl[u] >= 0)
+                            st4(spill + 4 * (size_t)sl[u], t0, t1, t2);
+                    }
+                }
+            }
+            __syncwarp();
+            if(lane == 0) mbar_arrive(bar_empty + 8 * s);
+#pragma unroll
+            for(int o = LPR / 2; o > 0; o >>= 1)
+            {
+                y0 += __shfl_xor_sync(0xffffffffu, y0, o);
+                y1 += __shfl_xor_sync(0xffffffffu, y1, o);
+                y2 += __shfl_xor_sync(0xffffffffu, y2, o);
+                dd += __shfl_xor_sync(0xffffffffu, dd, o);
+            }
+            if(sub == 0 && i < r1)
+            {
+                st4(zpn + 8 * (size_t)i + 4, v0, v1, v2);
+                st4(q + 4 * (size_t)i, y0, y1, y2);
+                const double vy = (double)v0 * (double)y0 + (double)v1 * (double)y1 + (double)v2 * (double)y2;
+                const double pq = 2.0 * vy - dd;
+                acc += pq;
+                if(c.seg_of_row) c.seg_row[i] = pq;
+            }
+        }
+        if(failed && lane == 0)
+        {
+            atomicExch(c.flags + F_STATUS, 6);  // STG_ERR_TIMEOUT
+            atomicExch(c.flags + F_DONE, 1);
+        }
+    }
     __shared__ double red[A_THREADS / 32];
     const double bs = block_sum<A_THREADS>(acc, red);
     if(threadIdx.x == 0) c.partials[(size_t)SITE_A * c.slots + blockIdx.x] = bs;
@@ -1787,13 +2171,47 @@ __global__ void __launch_bounds__(PB, 4) k_phase_b(PcgDev c)
     BSlot<T> first;
     if(B > 0)
         b_load<T>(c, zpbuf<T>(c, iter_parity(c) ^ 1), reinterpret_cast<const T*>(c.q), GT, first);
+    // After the upper SpMV, the spilled products of a warp's 32 consecutive rows (Morton
+    // order: consecutive slots are consecutive rows) are one contiguous run of slots: the warp
+    // copies up to SPW of them into shared memory with coalesced asynchronous copies, issued
+    // before the reductions, instead of each lane reading its own run (32 lines per load).
+    constexpr int SPW = 4096 / (4 * (int)sizeof(T));  // staged slots per warp (4 KB)
+    __shared__ __align__(16) T stage[B > 0 ? PB / 32 : 1][B > 0 ? 4 * SPW : 4];
+    const int lane = threadIdx.x & 31;
+    int slo = 0, shi = 0;
+    if(B > 0 && c.spill && c.identity)
+    {
+        const bool valid = first.v >= 0;
+        const unsigned vm = __ballot_sync(0xffffffffu, valid);
+        if(vm & 1u)
+        {
+            slo = __shfl_sync(0xffffffffu, first.t0, 0);
+            const int hi = __reduce_max_sync(0xffffffffu, valid ? first.t1 : 0);
+            shi = slo + min(hi - slo, SPW);
+            T* sw = stage[threadIdx.x >> 5];
+            const unsigned char* src = reinterpret_cast<const unsigned char*>(c.spill) + (size_t)slo * 4 * sizeof(T);
+            for(int e = lane; e < shi - slo; e += 32)
+#pragma unroll
+                for(int h = 0; h < (int)sizeof(T) / 4; h++)
+                    cp_async16(reinterpret_cast<unsigned char*>(sw) + (size_t)e * 4 * sizeof(T) + 16 * h,
+                               src + (size_t)e * 4 * sizeof(T) + 16 * h);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
     double pq, rz;
     consume_sum2<PB>(c, SITE_A, c.grid_a, SITE_E, c.grid_e, pq, rz);
+    if(B > 0 && c.spill && c.identity)
+    {
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncwarp();
+    }
     double v = 0;
     if(pq > 0.0 && isfinite(pq))  // else breakdown: no update; the last CTA reports it
     {
         const double alpha = rz / pq;
-        v = B > 0 ? phase_b_mas<T, (B > 0 ? B : 16)>(c, GT, GN, alpha, first, true) : phase_b_plain<T>(c, GT, GN, alpha);
+        v = B > 0 ? phase_b_mas<T, (B > 0 ? B : 16)>(c, GT, GN, alpha, first, true, shi > slo ? stage[threadIdx.x >> 5] : nullptr,
+                                                     slo, shi)
+                  : phase_b_plain<T>(c, GT, GN, alpha);
     }
     finish_reduction(c, v, SITE_B, POST_CHECK_PQ, 0, pq, rz);
 }
@@ -2131,7 +2549,8 @@ __global__ void __launch_bounds__(PB) k_pcg_persistent(PcgDev c)
         if(is_done(c)) break;
         const double alpha = __ldcg(c.scal + SS_ALPHA);
         BSlot<T> none;
-        const double vb = B > 0 ? phase_b_mas<T, BB>(c, gt, gn, alpha, none, false) : phase_b_plain<T>(c, gt, gn, alpha);
+        const double vb =
+            B > 0 ? phase_b_mas<T, BB, false>(c, gt, gn, alpha, none, false) : phase_b_plain<T>(c, gt, gn, alpha);
         grid_barrier(c, vb, SITE_B, POST_CHECK, gen);
         if(is_done(c)) break;
         const long k = (long)__ldcg(c.scal + SS_ITER);
@@ -2244,16 +2663,96 @@ __global__ void k_frow(const int* __restrict__ row_ptr, const int* __restrict__ 
         frow[i] = row_ptr[i] + t_ptr[i];
 }
 
+// Builds the upper copy (UpperPlanes) used by the upper SpMV phase: entry k is upper block k
+// in the iteration precision with its column and slot -1; k_upper_slots then gives every
+// block of a transpose list its place t in that list.
+template <typename T>
+__global__ void k_build_upper(const int* __restrict__ cols, const double* __restrict__ blocks, int nnzb, size_t S,
+                              unsigned char* uent)
+{
+    for(int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnzb; k += gridDim.x * blockDim.x)
+    {
+        T h[9];
+        const double* H = blocks + 9 * (size_t)k;
+#pragma unroll
+        for(int t = 0; t < 9; t++) h[t] = (T)H[t];
+        store_upper(uent, S, (size_t)k, h, cols[k], -1);
+    }
+}
+
+template <typename T>
+__global__ void k_upper_slots(const int2* __restrict__ t_ent, const int* __restrict__ t_ptr, int nrows, size_t S,
+                              unsigned char* uent)
+{
+    const int count = t_ptr[nrows];
+    for(int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x)
+        *upper_slot_ptr<T>(uent, S, (size_t)t_ent[t].x) = t;
+}
+
+// Whether the SpMV phase of the next solve runs the upper kernel: when chosen
+// (stg_spmv_tiles), picked by the autotuner, or by default in FP32.  Measured on the
+// 352,947-DOF cube, the FP32 solve takes the same time with either kernel (the upper one
+// moves 1.03x its algorithmic bytes, the full copy 1.68x, and holds half the matrix
+// bytes); in FP64 the upper kernel's spill (32 B per transposed product) costs more than it
+// saves and the full copy is the default.  The persistent loop's SpMV reads the full copy.
+static bool upper_spmv_selected(const Solver& S)
+{
+    if(S.cfg.loop_mode == STG_LOOP_PERSISTENT) return false;
+    if(S.spmv_rt == SPMV_UPPER) return true;
+    if(S.spmv_rt != 0) return false;
+    return S.spmv_tune ? S.tuned_rt == SPMV_UPPER : S.cfg.precision == STG_PREC_FP32;
+}
+
 int pack_blocks(Solver& S)
 {
     Bcoo& A = S.bcoo;
     const int nnzb = A.nnzb;
+    A.upper_built = false;
     if(nnzb < 1) return 0;
     STG_TRY(A.blk64p.resize((size_t)nnzb * 10));
     const bool fp32 = S.cfg.precision == STG_PREC_FP32;
     k_pack_blocks<<<std::max(1, std::min(div_up(nnzb, 256), kSMs * 16)), 256, 0, S.stream>>>(A.B(), nnzb, nullptr,
                                                                                            A.blk64p.data());
     STG_LAUNCH_CHECK();
+    // the autotuner times every kernel: both copies; otherwise the copy the chosen kernel reads
+    const bool tuning = S.spmv_tune && S.spmv_rt == 0 && S.cfg.loop_mode != STG_LOOP_PERSISTENT;
+    const bool need_upper = tuning || upper_spmv_selected(S);
+    const bool need_full = tuning || !upper_spmv_selected(S);
+    if(need_upper)
+    {
+        // plane stride: a multiple of 4 entries covering every 4-aligned tile range
+        A.ustride = ((size_t)nnzb + 7) & ~(size_t)3;
+        STG_TRY(A.urow.resize((size_t)A.nrows + 1 + 136));  // tiles copy row_ptr[r0 .. r0 + RT + 4)
+        STG_CUDA_TRY(cudaMemcpyAsync(A.urow.data(), A.row_ptr.data(), sizeof(int) * ((size_t)A.nrows + 1),
+                                     cudaMemcpyDeviceToDevice, S.stream));
+        const int gu = std::max(1, std::min(div_up(nnzb, 256), kSMs * 16));
+        if(fp32)
+        {
+            STG_TRY(A.uent.resize(A.ustride * UpperPlanes<float>::ES));
+            k_build_upper<float><<<gu, 256, 0, S.stream>>>(A.C(), A.B(), nnzb, A.ustride, A.uent.data());
+            STG_LAUNCH_CHECK();
+            k_upper_slots<float><<<gu, 256, 0, S.stream>>>(A.t_ent.data(), A.t_ptr.data(), A.nrows, A.ustride,
+                                                          A.uent.data());
+        }
+        else
+        {
+            STG_TRY(A.uent.resize(A.ustride * UpperPlanes<double>::ES));
+            k_build_upper<double><<<gu, 256, 0, S.stream>>>(A.C(), A.B(), nnzb, A.ustride, A.uent.data());
+            STG_LAUNCH_CHECK();
+            k_upper_slots<double><<<gu, 256, 0, S.stream>>>(A.t_ent.data(), A.t_ptr.data(), A.nrows, A.ustride,
+                                                           A.uent.data());
+        }
+        STG_LAUNCH_CHECK();
+        S.launches += 2;
+        // spill slots: 4 values of the iteration precision per transpose-list entry (< nnzb)
+        STG_TRY(S.pcg.spill.resize((size_t)nnzb * (fp32 ? 2 : 4)));
+        A.upper_built = true;
+    }
+    if(!need_full)
+    {
+        A.halo_ok = false;
+        return 0;
+    }
     // full symmetric copy: at most 2 * nnzb entries per plane, rounded up to an even count
     // so that every even-aligned entry range of the 8-byte tail plane is a 16-byte multiple
     A.fstride = ((size_t)2 * nnzb + 2) & ~(size_t)1;
@@ -2433,9 +2932,32 @@ static int phase_a_grid_halo(int nrows, int* grid)
     return 0;
 }
 
+// the upper SpMV phase: one resident wave of CTAs
 template <typename T>
-static int phase_a_grid(int nrows, int rt, int* grid, bool halo = false)
+static int phase_a_grid_upper(int nrows, int* grid)
 {
+    static thread_local unsigned long long seen = 0;
+    static thread_local int per_sm_dev[64];
+    int dev = 0;
+    STG_CUDA_TRY(cudaGetDevice(&dev));
+    int& per_sm = per_sm_dev[dev & 63];
+    if(first_on_device(seen))
+    {
+        STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_a_upper<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          AUpper<T>::SMEM));
+        STG_CUDA_TRY(cudaFuncSetAttribute(k_phase_a_upper<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          cudaSharedmemCarveoutMaxShared));
+        STG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase_a_upper<T>, A_THREADS,
+                                                                   AUpper<T>::SMEM));
+    }
+    *grid = std::max(1, std::min(div_up(nrows, AUpper<T>::RT), std::max(per_sm, 1) * kSMs));
+    return 0;
+}
+
+template <typename T>
+static int phase_a_grid(int nrows, int rt, int* grid, bool halo = false, bool upper = false)
+{
+    if(upper) return phase_a_grid_upper<T>(nrows, grid);
     if(halo) return phase_a_grid_halo<T>(nrows, grid);
     if(rt == a_rt_alt<T>()) return phase_a_grid_rt<T, a_rt_alt<T>()>(nrows, grid);
     return phase_a_grid_rt<T, a_rt_default<T>()>(nrows, grid);
@@ -2445,13 +2967,15 @@ template <typename T>
 static int launch_phase_a(const PcgDev& c, cudaStream_t s)
 {
     int grid = 0;
-    STG_TRY(phase_a_grid<T>(c.nrows, c.a_rt, &grid, c.halo != 0));
+    STG_TRY(phase_a_grid<T>(c.nrows, c.a_rt, &grid, c.halo != 0, c.upper != 0));
     if(grid != c.grid_a)
     {
         set_error("SpMV phase grid differs from the one phase B sums over");
         return STG_ERR_INVALID;
     }
-    if(c.halo)
+    if(c.upper)
+        k_phase_a_upper<T><<<grid, A_THREADS, AUpper<T>::SMEM, s>>>(c);
+    else if(c.halo)
         k_phase_a_halo<T><<<grid, A_THREADS, AHalo<T>::SMEM, s>>>(c);
     else if(c.a_rt == a_rt_alt<T>())
         k_phase_a_tiled<T, a_rt_alt<T>()><<<grid, A_THREADS, ATile<T, a_rt_alt<T>()>::SMEM, s>>>(c);
@@ -2468,16 +2992,18 @@ static int launch_phase_a(const PcgDev& c, cudaStream_t s)
 template <typename T>
 static int tune_phase_a(Solver& S, PcgDev c, float* us, int* out)
 {
-    const int cand[3] = {a_rt_default<T>(), a_rt_alt<T>(), SPMV_HALO};
-    const int ncand = S.bcoo.halo_ok ? 3 : 2;
-    us[2] = 0.f;
+    const int cand[4] = {a_rt_default<T>(), a_rt_alt<T>(), SPMV_HALO, SPMV_UPPER};
     float best = 0.f;
     int pick = cand[0];
-    for(int v = 0; v < ncand; v++)
+    for(int v = 0; v < 4; v++)
     {
+        us[v] = 0.f;
+        if((cand[v] == SPMV_HALO && !S.bcoo.halo_ok) || (cand[v] == SPMV_UPPER && !S.bcoo.upper_built)) continue;
         c.halo = cand[v] == SPMV_HALO ? 1 : 0;
-        c.a_rt = c.halo ? a_rt_default<T>() : cand[v];
-        STG_TRY(phase_a_grid<T>(c.nrows, c.a_rt, &c.grid_a, c.halo != 0));
+        c.upper = cand[v] == SPMV_UPPER ? 1 : 0;
+        c.spill = c.upper ? S.pcg.spill.data() : nullptr;
+        c.a_rt = (c.halo || c.upper) ? a_rt_default<T>() : cand[v];
+        STG_TRY(phase_a_grid<T>(c.nrows, c.a_rt, &c.grid_a, c.halo != 0, c.upper != 0));
         for(int i = 0; i < 3; i++) STG_TRY(launch_phase_a<T>(c, S.stream));
         const int reps = 10;
         STG_CUDA_TRY(cudaEventRecord(S.ev[4], S.stream));
@@ -2638,7 +3164,7 @@ template <typename T, int B>
 static int pcg_run(Solver& S, PcgDev& c, int& h_done)
 {
     STG_TRY((set_carveouts<T, B>()));
-    STG_TRY(phase_a_grid<T>(c.nrows, c.a_rt, &c.grid_a, c.halo != 0));
+    STG_TRY(phase_a_grid<T>(c.nrows, c.a_rt, &c.grid_a, c.halo != 0, c.upper != 0));
     c.grid_e = std::max(1, std::min(div_up(c.n, PB), kSMs * 4));  // grid_vec below
     if(c.grid_a > c.slots || c.grid_e > c.slots)
     {
@@ -2957,6 +3483,9 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
     c.hcnt = bcoo.hcnt.data();
     c.hlist = bcoo.hlist.data();
     c.halo = 0;
+    c.uent = bcoo.uent.data();
+    c.urow = bcoo.urow.data();
+    c.ustride = bcoo.ustride;
     c.nrows = bcoo.nrows;
     c.n = n;
     char* vb = reinterpret_cast<char*>(P.vbuf.data());
@@ -3004,11 +3533,12 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
     // the precision's default shape
     c.a_rt = fp32 ? a_rt_default<float>() : a_rt_default<double>();
     c.halo = 0;
+    c.upper = 0;
     if(spmv_rt == SPMV_HALO)
         c.halo = bcoo.halo_ok ? 1 : 0;
     else if(spmv_rt > 0)
         c.a_rt = spmv_rt;
-    else if(spmv_tune)
+    else if(spmv_tune && cfg.loop_mode != STG_LOOP_PERSISTENT)
     {
         if(tuned_prec != (fp32 ? 1 : 0) || tuned_nrows != bcoo.nrows || tuned_nnzb != bcoo.nnzb)
         {
@@ -3027,9 +3557,14 @@ int Solver::pcg_solve(const double* b, double* x, int n, int abd_bodies, const d
         }
         if(tuned_rt == SPMV_HALO)
             c.halo = bcoo.halo_ok ? 1 : 0;
+        else if(tuned_rt == SPMV_UPPER)
+            c.upper = bcoo.upper_built ? 1 : 0;
         else
             c.a_rt = tuned_rt;
     }
+    else if(upper_spmv_selected(*this))
+        c.upper = bcoo.upper_built ? 1 : 0;
+    c.spill = c.upper ? pcg.spill.data() : nullptr;
     if(nseg > 0)
     {
         if(seg_off_host.back() != bcoo.nrows || abd_bodies > 0 || cfg.loop_mode == STG_LOOP_PERSISTENT ||

@@ -26,10 +26,20 @@ struct PcgDev
     const int* hcnt;
     const int* hlist;
     int halo;                 // the SpMV phase runs the halo kernel
+    // upper SpMV phase (UpperPlanes in spmv_core.cuh): the upper copy, its row bounds padded
+    // for the tiles' copies, and the spill slots of the transposed products (4 T per
+    // strictly upper block, in transpose-list order).  spill == null: the full-copy kernels,
+    // and q holds the whole product
+    const unsigned char* uent;
+    const int* urow;
+    size_t ustride;
+    void* spill;
+    int upper;
     const double2* blk64;     // FP64 padded upper blocks (residual replacement)
     int nrows, n;
     // vectors in the iteration precision T, one 4-wide (16 B FP32 / 32 B FP64) slot per block
-    // row so that a neighbour gather is one (FP32) or two (FP64) 16-byte loads:
+    // row; z and p of a row share one 32 / 64-byte slot, so that a neighbour gather is one
+    // (FP32) or two (FP64) 32-byte loads:
     //   zp[2]: per block row {z0 z1 z2 -, p0 p1 p2 -} (8 T); double-buffered across iterations
     //   q    : per block row {q0 q1 q2 -} (4 T)
     // x, r, b stay FP64 in the caller's [3n] layout

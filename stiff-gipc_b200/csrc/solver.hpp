@@ -45,6 +45,11 @@ struct Bcoo
     DBuf<unsigned char> htail;   // {h8, slot} plane replacing {h8, col}
     DBuf<int> hcnt, hlist;       // [tiles], [tiles * HCAP] halo columns, sorted
     bool halo_ok = false;        // every tile fits a stage
+    // upper copy for the upper SpMV phase (UpperPlanes in spmv_core.cuh, k_build_upper)
+    DBuf<unsigned char> uent;
+    DBuf<int> urow;              // [nrows+1] row_ptr, padded for the tiles' row-bound copies
+    size_t ustride = 0;          // entries per plane
+    bool upper_built = false;    // built for the current matrix
     DBuf<double> diag_inv;       // 3x3 block-Jacobi inverses [nrows*9]
     int offdiag = 0;
 
@@ -115,6 +120,7 @@ struct PcgState
     DBuf<unsigned> bar;            // persistent grid barrier
     DBuf<unsigned char> flush;     // 256 MiB written between timed SpMV launches (L2 flush)
     DBuf<double> abd_inv;          // ABD 12x12 block-Jacobi built from the BCOO [bodies * 144]
+    DBuf<double> spill;            // transposed products of the upper SpMV phase (4 T per slot)
     cudaGraphExec_t graph = nullptr;
     PcgDev graph_key{};            // parameter block of the captured graph (handles zeroed)
     PcgDev graph_dev{};            // the same with the graph's conditional handles
@@ -180,8 +186,9 @@ struct Solver
     cudaGraph_t pending_if_body = nullptr;
     PcgDev pcg_dev{};             // parameters of the last solve (measurement hook)
     bool pcg_ready = false;
-    // SpMV tile shape: spmv_rt > 0 fixes the rows per tile; spmv_rt == 0 with spmv_tune set
-    // times the candidates at the next solve of a new shape and keeps the fastest
+    // SpMV kernel: spmv_rt > 0 fixes the rows per tile of the full-copy kernel, -2 the halo
+    // kernel, -3 the upper kernel; spmv_rt == 0 with spmv_tune set times the candidates at the
+    // next solve of a new shape and keeps the fastest
     // independent scenes on contiguous block-row ranges (stg_set_segments)
     int nseg = 0;
     std::vector<int> seg_off_host;    // [nseg + 1]
@@ -191,7 +198,7 @@ struct Solver
     int spmv_rt = 0;
     bool spmv_tune = false;
     int tuned_rt = 0, tuned_prec = -1, tuned_nrows = -1, tuned_nnzb = -1;
-    float tune_us[3] = {0.f, 0.f, 0.f};
+    float tune_us[4] = {0.f, 0.f, 0.f, 0.f};
 
     ~Solver();
 

@@ -151,4 +151,80 @@ __device__ __forceinline__ void store_entry(unsigned char* base, size_t S, size_
     reinterpret_cast<double2*>(base + 64 * S)[f] = make_double2(h[8], __longlong_as_double((long long)(unsigned)col));
 }
 
+// ---------------------------------------------------------------------------------------
+// Upper copy of the matrix for the PCG SpMV: entry k is the k-th block of the sorted unique
+// upper BCOO (rows ascending, columns ascending within a row), so a row range is one
+// contiguous range of every plane.  With S entries per plane:
+//   FP32: plane 0 {h0 h1 h2 h3} at 16 k, plane 1 {h4 h5 h6 h7} at 16 S + 16 k,
+//         tail {h8, col} at 32 S + 8 k, spill slot at 40 S + 4 k              (44 B per entry)
+//   FP64: planes p = 0..3 {h(2p) h(2p+1)} at 16 p S + 16 k,
+//         tail {h8, col, slot} at 64 S + 16 k                                 (80 B per entry)
+// The spill slot of a strictly upper block k (row i, column j > i) is its position t in the
+// transpose list of row j (t_ent[t].x == k): the SpMV writes H_k^T v_i there, and the owner of
+// row j adds its slots t_ptr[j] .. t_ptr[j+1] in that order.  A diagonal block has slot -1.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+struct UpperPlanes
+{
+    static constexpr int NP = sizeof(T) == 4 ? 2 : 4;     // 16-byte value planes
+    static constexpr int TAIL = sizeof(T) == 4 ? 8 : 16;  // bytes of the tail plane
+    static constexpr int SLOTP = sizeof(T) == 4 ? 4 : 0;  // bytes of the separate slot plane
+    static constexpr int ES = 16 * NP + TAIL + SLOTP;     // bytes per entry
+};
+
+__device__ __forceinline__ void store_upper(unsigned char* base, size_t S, size_t k, const float h[9], int col, int slot)
+{
+    reinterpret_cast<float4*>(base)[k] = make_float4(h[0], h[1], h[2], h[3]);
+    reinterpret_cast<float4*>(base + 16 * S)[k] = make_float4(h[4], h[5], h[6], h[7]);
+    reinterpret_cast<float2*>(base + 32 * S)[k] = make_float2(h[8], __int_as_float(col));
+    reinterpret_cast<int*>(base + 40 * S)[k] = slot;
+}
+
+__device__ __forceinline__ void store_upper(unsigned char* base, size_t S, size_t k, const double h[9], int col, int slot)
+{
+#pragma unroll
+    for(int p = 0; p < 4; p++) reinterpret_cast<double2*>(base + 16 * p * S)[k] = make_double2(h[2 * p], h[2 * p + 1]);
+    const long long cs = (long long)(((unsigned long long)(unsigned)slot << 32) | (unsigned)col);
+    reinterpret_cast<double2*>(base + 64 * S)[k] = make_double2(h[8], __longlong_as_double(cs));
+}
+
+// address of the spill slot of entry k (the slot is an int in both layouts)
+template <typename T>
+__device__ __forceinline__ int* upper_slot_ptr(unsigned char* base, size_t S, size_t k)
+{
+    if constexpr(sizeof(T) == 4)
+        return reinterpret_cast<int*>(base + 40 * S) + k;
+    else
+        return reinterpret_cast<int*>(base + 64 * S + 16 * k + 12);
+}
+
+// entry k from global memory through the read-only path
+__device__ __forceinline__ void ldg_upper(const unsigned char* base, size_t S, int k, float h[9], int& col, int& slot)
+{
+    const float4 a = __ldg(reinterpret_cast<const float4*>(base) + k);
+    const float4 b = __ldg(reinterpret_cast<const float4*>(base + 16 * S) + k);
+    const float2 t = __ldg(reinterpret_cast<const float2*>(base + 32 * S) + k);
+    h[0] = a.x; h[1] = a.y; h[2] = a.z; h[3] = a.w;
+    h[4] = b.x; h[5] = b.y; h[6] = b.z; h[7] = b.w;
+    h[8] = t.x;
+    col = __float_as_int(t.y);
+    slot = __ldg(reinterpret_cast<const int*>(base + 40 * S) + k);
+}
+
+__device__ __forceinline__ void ldg_upper(const unsigned char* base, size_t S, int k, double h[9], int& col, int& slot)
+{
+#pragma unroll
+    for(int p = 0; p < 4; p++)
+    {
+        const double2 v = __ldg(reinterpret_cast<const double2*>(base + 16 * p * S) + k);
+        h[2 * p] = v.x;
+        h[2 * p + 1] = v.y;
+    }
+    const double2 t = __ldg(reinterpret_cast<const double2*>(base + 64 * S) + k);
+    h[8] = t.x;
+    const unsigned long long cs = (unsigned long long)__double_as_longlong(t.y);
+    col = (int)(unsigned)cs;
+    slot = (int)(unsigned)(cs >> 32);
+}
+
 }  // namespace stg

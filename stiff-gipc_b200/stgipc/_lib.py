@@ -118,7 +118,7 @@ def lib():
     L.stg_cloth_bending.argtypes = [ci, vp, vp, vp, vp, ci, cd, cd, ci, vp, vp, vp, vp, vp, vp]
     L.stg_contact_barrier.argtypes = [ci, vp, vp, ci, ci, cd, cd, vp, vp, vp, vp, vp, vp]
     L.stg_spmv_tiles_info.argtypes = [vp, C.POINTER(ci), C.POINTER(C.c_float), C.POINTER(C.c_float),
-                                      C.POINTER(C.c_float)]
+                                      C.POINTER(C.c_float), C.POINTER(C.c_float)]
     L.stg_net_configure.argtypes = [vp, ci]
     L.stg_net_graph_info.argtypes = [vp, C.POINTER(ci), C.POINTER(ci)]
     L.stg_net_export_graph.argtypes = [vp, vp, vp, vp, vp, vp, vp]

@@ -245,16 +245,16 @@ class Solver:
     # -- BCOO tile autotuner -------------------------------------------------------------------
     def spmv_tiles(self, rows_per_tile: int):
         """0: autotune at the next solve of a new shape class; -1: default; -2: the halo
-        kernel; else a fixed tile shape."""
+        kernel; -3: the upper kernel; else a fixed tile shape of the full-copy kernel."""
         check(_L.lib().stg_spmv_tiles(self.h, int(rows_per_tile)), "stg_spmv_tiles")
 
     def spmv_tiles_info(self):
-        """(rows per tile of the last solve (-2: halo kernel), tuner us per launch: default
-        shape, alternative shape, halo kernel)."""
-        rt, a, b, h = C.c_int(), C.c_float(), C.c_float(), C.c_float()
-        check(_L.lib().stg_spmv_tiles_info(self.h, C.byref(rt), C.byref(a), C.byref(b), C.byref(h)),
+        """(rows per tile of the last solve (-2: halo kernel, -3: upper kernel), tuner us per
+        launch: default shape, alternative shape, halo kernel, upper kernel)."""
+        rt, a, b, h, u = C.c_int(), C.c_float(), C.c_float(), C.c_float(), C.c_float()
+        check(_L.lib().stg_spmv_tiles_info(self.h, C.byref(rt), C.byref(a), C.byref(b), C.byref(h), C.byref(u)),
               "stg_spmv_tiles_info")
-        return rt.value, a.value, b.value, h.value
+        return rt.value, a.value, b.value, h.value, u.value
 
     # -- learned coarse correction (stg_net_*) ---------------------------------------------
     def net_configure(self, level: int):

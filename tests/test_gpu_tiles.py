@@ -1,6 +1,7 @@
-"""GPU: the BCOO tile autotuner of the in-loop SpMV (stg_spmv_tiles): every tile shape gives
-the same solve up to summation order, the tuner picks the faster of the timed candidates and
-keeps it, and unsupported shapes are rejected."""
+"""GPU: the kernels of the in-loop SpMV and their autotuner (stg_spmv_tiles): every tile shape
+of the full-copy kernel, the halo kernel and the upper kernel give the same solve up to
+summation order, the tuner picks the fastest of the timed candidates and keeps it, and
+unsupported shapes are rejected."""
 import numpy as np
 import pytest
 
@@ -24,12 +25,14 @@ def _solve(s, dev, prec, tiles=None):
 
 @pytest.mark.parametrize("prec,alt,tol", [("fp32", 32, 2e-4), ("fp64", 16, 1e-7)])
 def test_tile_shapes_agree(dev, prec, alt, tol):
-    """Both tile shapes and the halo kernel (operands staged in shared memory) give the same
-    solve up to summation order."""
+    """Both tile shapes, the halo kernel (operands staged in shared memory) and the upper
+    kernel (transposed products spilled to their rows) give the same solve up to summation
+    order."""
     s = cube_system(16)
-    s0, st0, x0 = _solve(s, dev, prec)
-    assert s0.spmv_tiles_info()[0] == (64 if prec == "fp32" else 32)
-    for shape in (alt, -2):
+    s0, st0, x0 = _solve(s, dev, prec, -1)
+    default = s0.spmv_tiles_info()[0]
+    assert default in ((64 if prec == "fp32" else 32), -3)
+    for shape in (64 if prec == "fp32" else 32, alt, -2, -3):
         s1, st1, x1 = _solve(s, dev, prec, shape)
         assert s1.spmv_tiles_info()[0] == shape
         assert abs(st0["iterations"] - st1["iterations"]) <= 1
@@ -40,20 +43,20 @@ def test_tile_shapes_agree(dev, prec, alt, tol):
 def test_autotuner_picks_fastest_and_keeps_it(dev, prec):
     s = cube_system(16)
     solver, st, _ = _solve(s, dev, prec, 0)
-    rt, us_a, us_b, us_h = solver.spmv_tiles_info()
-    cand = ((64, 32) if prec == "fp32" else (32, 16)) + (-2,)
-    assert us_a > 0 and us_b > 0 and us_h > 0
-    us = (us_a, us_b, us_h)
+    rt, us_a, us_b, us_h, us_u = solver.spmv_tiles_info()
+    cand = ((64, 32) if prec == "fp32" else (32, 16)) + (-2, -3)
+    assert us_a > 0 and us_b > 0 and us_h > 0 and us_u > 0
+    us = (us_a, us_b, us_h, us_u)
     assert rt == cand[int(np.argmin(us))]
     import torch
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     x = t(np.zeros(s.n))
     st2 = solver.solve_linear_system(t(s.rows), t(s.cols), t(s.blocks.reshape(-1)), t(s.b), x)
-    assert solver.spmv_tiles_info() == (rt, us_a, us_b, us_h)  # same shape: not re-timed
+    assert solver.spmv_tiles_info() == (rt, us_a, us_b, us_h, us_u)  # same shape: not re-timed
     assert st2["iterations"] == st["iterations"]
     # another handle on the same shape class reuses the process's choice without timing
     other, st3, _ = _solve(s, dev, prec, 0)
-    assert other.spmv_tiles_info() == (rt, us_a, us_b, us_h)
+    assert other.spmv_tiles_info() == (rt, us_a, us_b, us_h, us_u)
 
 
 def test_unsupported_tile_shape_rejected(dev):
