@@ -92,6 +92,14 @@ __device__ __forceinline__ void finish_reduction(const PcgDev& c, double v, int 
     __syncthreads();
     if(!last) return;
     __threadfence();
+    // The post-op reads the scalars and flags (one 128-byte line each) one after another;
+    // fetched into L1 now, while the partials are summed, those reads do not wait on L2.
+    // Only this CTA writes them while the kernel runs, so the L1 copies stay current.
+    if(threadIdx.x == 0)
+    {
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(c.scal));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(c.flags));
+    }
     double acc = 0;
     for(int i = threadIdx.x; i < (int)gridDim.x; i += BLOCK) acc += __ldcg(partials + i);
     const double tot = block_sum<BLOCK>(acc, red);
@@ -156,6 +164,62 @@ __device__ __forceinline__ void consume_sum2(const PcgDev& c, int site_a, int co
         {
             tot[0] = x;
             tot[1] = y;
+        }
+    }
+    __syncthreads();
+    ra = tot[0];
+    rb = tot[1];
+}
+
+// consume_sum2 in two steps, so that the partials' loads can be issued early and other
+// work done while they are in flight: consume2_load fetches this thread's partials (at most
+// K per site; the caller checks K * BLOCK against the counts), consume2_finish sums them in
+// consume_sum2's order (bitwise its result).
+template <int BLOCK, int K>
+__device__ __forceinline__ void consume2_load(const PcgDev& c, int site_a, int count_a, int site_b, int count_b,
+                                              double (&a)[K], double (&b)[K])
+{
+    const double* pa = c.partials + (size_t)site_a * c.slots;
+    const double* pb = c.partials + (size_t)site_b * c.slots;
+#pragma unroll
+    for(int k = 0; k < K; k++)
+    {
+        const int t = threadIdx.x + k * BLOCK;
+        a[k] = t < count_a ? __ldcg(pa + t) : 0.0;
+        b[k] = t < count_b ? __ldcg(pb + t) : 0.0;
+    }
+}
+
+template <int BLOCK, int K>
+__device__ __forceinline__ void consume2_finish(const double (&a)[K], const double (&b)[K], double& ra, double& rb)
+{
+    __shared__ double red[2][BLOCK / 32];
+    __shared__ double tot[2];
+    double x = 0, y = 0;
+#pragma unroll
+    for(int k = 0; k < K; k++)
+    {
+        x += a[k];
+        y += b[k];
+    }
+    x = warp_sum(x);
+    y = warp_sum(y);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if(lane == 0)
+    {
+        red[0][warp] = x;
+        red[1][warp] = y;
+    }
+    __syncthreads();
+    if(warp == 0)
+    {
+        double u = lane < BLOCK / 32 ? red[0][lane] : 0.0, v = lane < BLOCK / 32 ? red[1][lane] : 0.0;
+        u = warp_sum(u);
+        v = warp_sum(v);
+        if(lane == 0)
+        {
+            tot[0] = u;
+            tot[1] = v;
         }
     }
     __syncthreads();
@@ -629,7 +693,8 @@ __device__ __forceinline__ void phase_restrict01(const PcgDev& c, int gt, int gn
 // (C1: level 1 -> 2 over the whole grid; C2: levels >= 2 inside one CTA, which passes
 // block_sync = true).
 template <int B>
-__device__ __forceinline__ void restrict_level(const PcgDev& c, int number, int begin, int gt, int gn)
+__device__ __forceinline__ void restrict_level(const PcgDev& c, int number, int begin, int gt, int gn,
+                                               bool skip_stores = false)
 {
     const int span = (number + 31) / 32 * 32;
     for(int i = gt; i < span; i += gn)
@@ -657,7 +722,7 @@ __device__ __forceinline__ void restrict_level(const PcgDev& c, int number, int 
                 a2 += x2;
             }
         }
-        if(valid && __popc(msk & lanemask_lt(i % B)) == 0)
+        if(valid && !skip_stores && __popc(msk & lanemask_lt(i % B)) == 0)
         {
             const int g = c.going_next[begin + i];
             st4(c.R + 4 * (size_t)g, a0, a1, a2);
@@ -858,12 +923,10 @@ __device__ __forceinline__ void d16_issue(const PcgDev& c, char* stage, unsigned
 // Banks [b0, b1).  guarded: only on residual-replacement iterations (host loop).
 __global__ void __launch_bounds__(D_WARPS * 32) k_phase_d16(PcgDev c, int b0, int b1, int guarded)
 {
-    if(c.flags[F_DONE]) return;
-    if(guarded)
-    {
-        const long k = (long)c.scal[SS_ITER];
-        if(c.prm.refine <= 0 || k % c.prm.refine != 0) return;
-    }
+    // the stop flag (and the replacement test) are loaded with the first bank's copy in
+    // flight, not before it: their latency overlaps the copy's
+    const int done = __ldcg(c.flags + F_DONE);
+    const long k_it = guarded ? (long)__ldcg(c.scal + SS_ITER) : 0;
     extern __shared__ __align__(128) char dsm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     char* base = dsm + (size_t)warp * D_WARP_BYTES;
@@ -894,6 +957,12 @@ __global__ void __launch_bounds__(D_WARPS * 32) k_phase_d16(PcgDev c, int b0, in
         d16_issue(c, stage0, bar0, gw);
     }
     __syncwarp();
+    if(done || (guarded && (c.prm.refine <= 0 || k_it % c.prm.refine != 0)))
+    {
+        // nothing to solve: let the first copy land before the warp's shared memory goes
+        if(lane == 0) mbar_wait(bar0, 0u);
+        return;
+    }
     unsigned ph0 = 0u, ph1 = 0u;
     int buf = 0;
     for(int bk = gw; bk < b1; bk += nw, buf ^= 1)
@@ -1085,6 +1154,8 @@ __device__ __forceinline__ void ld_zp(const float* a, float& z0, float& z1, floa
     asm("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
         : "=f"(z0), "=f"(z1), "=f"(z2), "=f"(w0), "=f"(p0), "=f"(p1), "=f"(p2), "=f"(w1)
         : "l"(a));
+    (void)w0;
+    (void)w1;
 }
 __device__ __forceinline__ void ld_zp(const double* a, double& z0, double& z1, double& z2, double& p0, double& p1,
                                       double& p2)
@@ -1092,6 +1163,8 @@ __device__ __forceinline__ void ld_zp(const double* a, double& z0, double& z1, d
     double w0, w1;
     asm("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(z0), "=d"(z1), "=d"(z2), "=d"(w0) : "l"(a));
     asm("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(p0), "=d"(p1), "=d"(p2), "=d"(w1) : "l"(a + 4));
+    (void)w0;
+    (void)w1;
 }
 
 // v_j = z_j + beta p_j gathered from the zp slots
@@ -1131,16 +1204,6 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T, RTT>::MIN_CTAS) k_phase_a_
         lo = __ldg(c.frow + r0);
         hi = __ldg(c.frow + min(r0 + RT, re));
     }
-    if(done) return;
-    // beta = rz_k / rz_(k-1): rz_k from phase E's partials, rz_(k-1) as phase B recorded it
-    // (the first iteration has p_0 = 0: beta = 0)
-    // flexible PCG (learned correction): beta = r_k.(z_k - z_(k-1)) / r_(k-1).z_(k-1)
-    double rz_new, rz_mix = 0.0;
-    if(c.flex && (long)s_iter > 0)
-        consume_sum2<A_THREADS>(c, SITE_E, c.grid_e, SITE_F, c.grid_e, rz_new, rz_mix);
-    else
-        rz_new = consume_sum<A_THREADS>(c, SITE_E, c.grid_e);
-    const double s_beta = (long)s_iter == 0 ? 0.0 : (rz_new - rz_mix) / rz_old;
     int* meta = reinterpret_cast<int*>(asm_ + G::STAGES * G::STAGE);
     const unsigned sbase = smem_u32(asm_);
     const unsigned bar_full = smem_u32(asm_ + G::STAGES * G::STAGE + G::META);
@@ -1155,6 +1218,54 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T, RTT>::MIN_CTAS) k_phase_a_
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    // tile k into stage k % STAGES (producer lane 0): the row bounds and every plane's range
+    auto issue_tile = [&](int k, int F0, int F1) {
+        const int s = k % G::STAGES;
+        const int F0a = F0 & ~1, n2 = ((F1 + 1) & ~1) - F0a;
+        const bool ovf = n2 > CAP;
+        const int nc = ovf ? 0 : n2;
+        meta[4 * s] = F0a;
+        meta[4 * s + 1] = ovf ? 1 : 0;
+        unsigned char* st = asm_ + (size_t)s * G::STAGE;
+        const unsigned bf = bar_full + 8 * s;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(bf, (unsigned)(G::FROW + nc * FP::ES));
+        tma_load_1d(st + CAP * FP::ES, c.frow + rb + (size_t)k * RT, G::FROW, bf);
+        if(nc)
+        {
+            const unsigned long long stream = l2_evict_first();
+#pragma unroll 1
+            for(int pl = 0; pl < FP::NP; pl++)
+                tma_load_1d_hint(st + (size_t)16 * pl * CAP, c.fent + 16 * (pl * c.fstride + F0a), (unsigned)(16 * nc),
+                                 bf, stream);
+            tma_load_1d_hint(st + (size_t)16 * FP::NP * CAP, c.fent + 16 * FP::NP * c.fstride + (size_t)FP::TAIL * F0a,
+                             (unsigned)(FP::TAIL * nc), bf, stream);
+        }
+    };
+    // The first STAGES tiles depend neither on beta nor on the stop flag: their copies start
+    // now and run while the r.z partials are summed.  A stopped solve drains them and returns.
+    const int pre = min(G::STAGES, mine);
+    if(warp == A_CW)
+        for(int u = 0; u < pre; u++)
+        {
+            const int F0 = __shfl_sync(0xffffffffu, lo, u), F1 = __shfl_sync(0xffffffffu, hi, u);
+            if(lane == 0) issue_tile(u, F0, F1);
+        }
+    // beta = rz_k / rz_(k-1): rz_k from phase E's partials, rz_(k-1) as phase B recorded it
+    // (the first iteration has p_0 = 0: beta = 0)
+    // flexible PCG (learned correction): beta = r_k.(z_k - z_(k-1)) / r_(k-1).z_(k-1)
+    double rz_new, rz_mix = 0.0;
+    if(c.flex && (long)s_iter > 0)
+        consume_sum2<A_THREADS>(c, SITE_E, c.grid_e, SITE_F, c.grid_e, rz_new, rz_mix);
+    else
+        rz_new = consume_sum<A_THREADS>(c, SITE_E, c.grid_e);
+    if(done)
+    {
+        if(warp == A_CW && lane == 0)
+            for(int k = 0; k < pre; k++) mbar_wait(bar_full + 8 * k, 0u);
+        return;
+    }
+    const double s_beta = (long)s_iter == 0 ? 0.0 : (rz_new - rz_mix) / rz_old;
 
     const int par = ((long)s_iter) & 1;
     const T* zp = zpbuf<T>(c, par);
@@ -1167,7 +1278,7 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T, RTT>::MIN_CTAS) k_phase_a_
     if(warp == A_CW)
     {
         // ---- producer warp: lane 0 issues, all lanes fetch the tile bounds ----
-        int issued = 0;
+        int issued = pre;
         for(int k0 = 0; k0 < mine && !failed; k0 += 32)
         {
             if(k0 > 0)
@@ -1185,32 +1296,13 @@ __global__ void __launch_bounds__(A_THREADS, ATile<T, RTT>::MIN_CTAS) k_phase_a_
             {
                 const int F0 = __shfl_sync(0xffffffffu, lo, u), F1 = __shfl_sync(0xffffffffu, hi, u);
                 const int k = k0 + u, s = k % G::STAGES;
+                if(k < pre) continue;
                 if(lane == 0)
                 {
-                    if(k >= G::STAGES && !mbar_wait(bar_empty + 8 * s, ((k / G::STAGES) - 1) & 1)) failed = true;
+                    if(!mbar_wait(bar_empty + 8 * s, ((k / G::STAGES) - 1) & 1)) failed = true;
                     if(!failed)
                     {
-                        const int F0a = F0 & ~1, n2 = ((F1 + 1) & ~1) - F0a;
-                        const bool ovf = n2 > CAP;
-                        const int nc = ovf ? 0 : n2;
-                        meta[4 * s] = F0a;
-                        meta[4 * s + 1] = ovf ? 1 : 0;
-                        unsigned char* st = asm_ + (size_t)s * G::STAGE;
-                        const unsigned bf = bar_full + 8 * s;
-                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                        mbar_expect_tx(bf, (unsigned)(G::FROW + nc * FP::ES));
-                        tma_load_1d(st + CAP * FP::ES, c.frow + rb + (size_t)k * RT, G::FROW, bf);
-                        if(nc)
-                        {
-                            const unsigned long long stream = l2_evict_first();
-#pragma unroll 1
-                            for(int pl = 0; pl < FP::NP; pl++)
-                                tma_load_1d_hint(st + (size_t)16 * pl * CAP, c.fent + 16 * (pl * c.fstride + F0a),
-                                                 (unsigned)(16 * nc), bf, stream);
-                            tma_load_1d_hint(st + (size_t)16 * FP::NP * CAP,
-                                             c.fent + 16 * FP::NP * c.fstride + (size_t)FP::TAIL * F0a,
-                                             (unsigned)(FP::TAIL * nc), bf, stream);
-                        }
+                        issue_tile(k, F0, F1);
                         issued = k + 1;
                     }
                 }
@@ -1432,13 +1524,6 @@ __global__ void __launch_bounds__(A_THREADS, AUpper<T>::MIN_CTAS) k_phase_a_uppe
         lo = __ldg(c.urow + r0);
         hi = __ldg(c.urow + min(r0 + RT, re));
     }
-    if(done) return;
-    double rz_new, rz_mix = 0.0;
-    if(c.flex && (long)s_iter > 0)
-        consume_sum2<A_THREADS>(c, SITE_E, c.grid_e, SITE_F, c.grid_e, rz_new, rz_mix);
-    else
-        rz_new = consume_sum<A_THREADS>(c, SITE_E, c.grid_e);
-    const double s_beta = (long)s_iter == 0 ? 0.0 : (rz_new - rz_mix) / rz_old;
     int* meta = reinterpret_cast<int*>(asm_ + G::STAGES * G::STAGE);
     const unsigned sbase = smem_u32(asm_);
     const unsigned bar_full = smem_u32(asm_ + G::STAGES * G::STAGE + G::META);
@@ -1453,6 +1538,56 @@ __global__ void __launch_bounds__(A_THREADS, AUpper<T>::MIN_CTAS) k_phase_a_uppe
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    // tile k into stage k % STAGES (producer lane 0): the row bounds and every plane's range
+    auto issue_tile = [&](int k, int F0, int F1) {
+        const int s = k % G::STAGES;
+        // 4-entry aligned range: F0a + n4 <= round_up(nnzb, 4) <= the plane stride
+        const int F0a = F0 & ~3, n4 = ((F1 + 3) & ~3) - F0a;
+        const bool ovf = n4 > CAP;
+        const int nc = ovf ? 0 : n4;
+        meta[4 * s] = F0a;
+        meta[4 * s + 1] = ovf ? 1 : 0;
+        unsigned char* st = asm_ + (size_t)s * G::STAGE;
+        const unsigned bf = bar_full + 8 * s;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(bf, (unsigned)(G::FROW + nc * UP::ES));
+        tma_load_1d(st + CAP * UP::ES, c.urow + rb + (size_t)k * RT, G::FROW, bf);
+        if(nc)
+        {
+            const unsigned long long stream = l2_evict_first();
+            const size_t S = c.ustride;
+#pragma unroll 1
+            for(int pl = 0; pl < UP::NP; pl++)
+                tma_load_1d_hint(st + (size_t)16 * pl * CAP, c.uent + 16 * (pl * S + F0a), (unsigned)(16 * nc), bf,
+                                 stream);
+            tma_load_1d_hint(st + (size_t)16 * UP::NP * CAP, c.uent + 16 * UP::NP * S + (size_t)UP::TAIL * F0a,
+                             (unsigned)(UP::TAIL * nc), bf, stream);
+            if constexpr(UP::SLOTP > 0)
+                tma_load_1d_hint(st + G::SLOT_OFF, c.uent + (16 * UP::NP + UP::TAIL) * S + (size_t)UP::SLOTP * F0a,
+                                 (unsigned)(UP::SLOTP * nc), bf, stream);
+        }
+    };
+    // The first STAGES tiles depend neither on beta nor on the stop flag: their copies start
+    // now and run while the r.z partials are summed.  A stopped solve drains them and returns.
+    const int pre = min(G::STAGES, mine);
+    if(warp == A_CW)
+        for(int u = 0; u < pre; u++)
+        {
+            const int F0 = __shfl_sync(0xffffffffu, lo, u), F1 = __shfl_sync(0xffffffffu, hi, u);
+            if(lane == 0) issue_tile(u, F0, F1);
+        }
+    double rz_new, rz_mix = 0.0;
+    if(c.flex && (long)s_iter > 0)
+        consume_sum2<A_THREADS>(c, SITE_E, c.grid_e, SITE_F, c.grid_e, rz_new, rz_mix);
+    else
+        rz_new = consume_sum<A_THREADS>(c, SITE_E, c.grid_e);
+    if(done)
+    {
+        if(warp == A_CW && lane == 0)
+            for(int k = 0; k < pre; k++) mbar_wait(bar_full + 8 * k, 0u);
+        return;
+    }
+    const double s_beta = (long)s_iter == 0 ? 0.0 : (rz_new - rz_mix) / rz_old;
 
     const int par = ((long)s_iter) & 1;
     const T* zp = zpbuf<T>(c, par);
@@ -1466,7 +1601,7 @@ __global__ void __launch_bounds__(A_THREADS, AUpper<T>::MIN_CTAS) k_phase_a_uppe
     if(warp == A_CW)
     {
         // ---- producer warp: lane 0 issues, all lanes fetch the tile bounds ----
-        int issued = 0;
+        int issued = pre;
         for(int k0 = 0; k0 < mine && !failed; k0 += 32)
         {
             if(k0 > 0)
@@ -1484,36 +1619,13 @@ __global__ void __launch_bounds__(A_THREADS, AUpper<T>::MIN_CTAS) k_phase_a_uppe
             {
                 const int F0 = __shfl_sync(0xffffffffu, lo, u), F1 = __shfl_sync(0xffffffffu, hi, u);
                 const int k = k0 + u, s = k % G::STAGES;
+                if(k < pre) continue;
                 if(lane == 0)
                 {
-                    if(k >= G::STAGES && !mbar_wait(bar_empty + 8 * s, ((k / G::STAGES) - 1) & 1)) failed = true;
+                    if(!mbar_wait(bar_empty + 8 * s, ((k / G::STAGES) - 1) & 1)) failed = true;
                     if(!failed)
                     {
-                        // 4-entry aligned range: F0a + n4 <= round_up(nnzb, 4) <= the plane stride
-                        const int F0a = F0 & ~3, n4 = ((F1 + 3) & ~3) - F0a;
-                        const bool ovf = n4 > CAP;
-                        const int nc = ovf ? 0 : n4;
-                        meta[4 * s] = F0a;
-                        meta[4 * s + 1] = ovf ? 1 : 0;
-                        unsigned char* st = asm_ + (size_t)s * G::STAGE;
-                        const unsigned bf = bar_full + 8 * s;
-                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                        mbar_expect_tx(bf, (unsigned)(G::FROW + nc * UP::ES));
-                        tma_load_1d(st + CAP * UP::ES, c.urow + rb + (size_t)k * RT, G::FROW, bf);
-                        if(nc)
-                        {
-                            const unsigned long long stream = l2_evict_first();
-                            const size_t S = c.ustride;
-#pragma unroll 1
-                            for(int pl = 0; pl < UP::NP; pl++)
-                                tma_load_1d_hint(st + (size_t)16 * pl * CAP, c.uent + 16 * (pl * S + F0a),
-                                                 (unsigned)(16 * nc), bf, stream);
-                            tma_load_1d_hint(st + (size_t)16 * UP::NP * CAP, c.uent + 16 * UP::NP * S + (size_t)UP::TAIL * F0a,
-                                             (unsigned)(UP::TAIL * nc), bf, stream);
-                            if constexpr(UP::SLOTP > 0)
-                                tma_load_1d_hint(st + G::SLOT_OFF, c.uent + (16 * UP::NP + UP::TAIL) * S + (size_t)UP::SLOTP * F0a,
-                                                 (unsigned)(UP::SLOTP * nc), bf, stream);
-                        }
+                        issue_tile(k, F0, F1);
                         issued = k + 1;
                     }
                 }
@@ -2056,8 +2168,9 @@ __global__ void __launch_bounds__(A_THREADS, 2) k_phase_a_halo(PcgDev c)
 // E (MAS): z = sum over levels (FP32) on the FEM range + ABD block-Jacobi; share of r.z
 // ABD 12x12 block-Jacobi (abd_preconditioner.cu:20-38): one thread per dof of the first
 // 12 * bodies dofs, z written into the zp slots; returns the share of r.z
+// skip: the solve has stopped (stop flag read with the loads): nothing is stored
 template <typename T>
-__device__ __forceinline__ double abd_apply(const PcgDev& c, T* zp, int gt, int gn)
+__device__ __forceinline__ double abd_apply(const PcgDev& c, T* zp, int gt, int gn, bool skip = false)
 {
     double acc = 0;
     for(int t = gt; t < c.abd_bodies * 12; t += gn)
@@ -2067,6 +2180,7 @@ __device__ __forceinline__ double abd_apply(const PcgDev& c, T* zp, int gt, int 
         double s = 0;
 #pragma unroll
         for(int cc = 0; cc < 12; cc++) s += J[cc] * c.r[body * 12 + cc];
+        if(skip) continue;
         zp[8 * (size_t)(t / 3) + t % 3] = (T)s;
         acc += c.r[t] * (double)(T)s;
     }
@@ -2074,7 +2188,7 @@ __device__ __forceinline__ double abd_apply(const PcgDev& c, T* zp, int gt, int 
 }
 
 template <typename T>
-__device__ __forceinline__ double phase_e_mas(const PcgDev& c, int gt, int gn)
+__device__ __forceinline__ double phase_e_mas(const PcgDev& c, int gt, int gn, bool skip = false)
 {
     T* zp = zpbuf<T>(c, iter_parity(c));
     double acc = 0;
@@ -2094,18 +2208,19 @@ __device__ __forceinline__ double phase_e_mas(const PcgDev& c, int gt, int gn)
             c2 += t2;
         }
         const int row = fem_row + v;
-        st4(zp + 8 * (size_t)row, (T)c0, (T)c1, (T)c2);
         const double* r = c.r + 3 * (size_t)row;
         const double rz = r[0] * (double)(T)c0 + r[1] * (double)(T)c1 + r[2] * (double)(T)c2;
         acc += rz;
+        if(skip) continue;
+        st4(zp + 8 * (size_t)row, (T)c0, (T)c1, (T)c2);
         if(c.seg_of_row) c.seg_row[2 * (size_t)c.nrows + row] = rz;
     }
-    return acc + abd_apply<T>(c, zp, gt, gn);
+    return acc + abd_apply<T>(c, zp, gt, gn, skip);
 }
 
 // E (global block-Jacobi / identity, then the ABD local preconditioner); share of r.z
 template <typename T>
-__device__ __forceinline__ double phase_e_plain(const PcgDev& c, int gt, int gn)
+__device__ __forceinline__ double phase_e_plain(const PcgDev& c, int gt, int gn, bool skip = false)
 {
     T* zp = zpbuf<T>(c, iter_parity(c));
     double acc = 0;
@@ -2120,12 +2235,13 @@ __device__ __forceinline__ double phase_e_plain(const PcgDev& c, int gt, int gn)
             z1 = D[1] * r0 + D[4] * r1 + D[7] * r2;
             z2 = D[2] * r0 + D[5] * r1 + D[8] * r2;
         }
-        st4(zp + 8 * (size_t)bi, (T)z0, (T)z1, (T)z2);
         const double rz = r0 * (double)(T)z0 + r1 * (double)(T)z1 + r2 * (double)(T)z2;
         acc += rz;
+        if(skip) continue;
+        st4(zp + 8 * (size_t)bi, (T)z0, (T)z1, (T)z2);
         if(c.seg_of_row) c.seg_row[2 * (size_t)c.nrows + bi] = rz;
     }
-    return acc + abd_apply<T>(c, zp, gt, gn);
+    return acc + abd_apply<T>(c, zp, gt, gn, skip);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -2166,11 +2282,19 @@ __global__ void __launch_bounds__(PB) k_phase_a(PcgDev c)
 template <typename T, int B>
 __global__ void __launch_bounds__(PB, 4) k_phase_b(PcgDev c)
 {
-    if(c.flags[F_DONE]) return;
-    // the first slot's loads do not depend on alpha: issue them before the reductions
+    // the first slot's loads depend neither on alpha nor on the stop flag: issue them with
+    // the flag's load, before the reductions
+    const int done = __ldcg(c.flags + F_DONE);
     BSlot<T> first;
     if(B > 0)
         b_load<T>(c, zpbuf<T>(c, iter_parity(c) ^ 1), reinterpret_cast<const T*>(c.q), GT, first);
+    // the p.q and r.z partials, in flight with the slot's loads (a grid too large for the
+    // registers sums them in consume_sum2 below)
+    constexpr int PK = 3;
+    const bool early = c.grid_a <= PK * PB && c.grid_e <= PK * PB;
+    double pa[PK], pe[PK];
+    if(early) consume2_load<PB, PK>(c, SITE_A, c.grid_a, SITE_E, c.grid_e, pa, pe);
+    if(done) return;
     // After the upper SpMV, the spilled products of a warp's 32 consecutive rows (Morton
     // order: consecutive slots are consecutive rows) are one contiguous run of slots: the warp
     // copies up to SPW of them into shared memory with coalesced asynchronous copies, issued
@@ -2199,7 +2323,10 @@ __global__ void __launch_bounds__(PB, 4) k_phase_b(PcgDev c)
         asm volatile("cp.async.commit_group;" ::: "memory");
     }
     double pq, rz;
-    consume_sum2<PB>(c, SITE_A, c.grid_a, SITE_E, c.grid_e, pq, rz);
+    if(early)
+        consume2_finish<PB, PK>(pa, pe, pq, rz);
+    else
+        consume_sum2<PB>(c, SITE_A, c.grid_a, SITE_E, c.grid_e, pq, rz);
     if(B > 0 && c.spill && c.identity)
     {
         asm volatile("cp.async.wait_all;" ::: "memory");
@@ -2246,8 +2373,9 @@ __global__ void __launch_bounds__(PB) k_restrict01(PcgDev c, int guarded)
 template <int B>
 __global__ void __launch_bounds__(PB) k_phase_c1(PcgDev c)
 {
-    if(c.flags[F_DONE]) return;
-    if(c.L > 2) restrict_level<B>(c, c.ls[2], c.ls[3], GT, GN);  // level 1's (count, begin)
+    // the stop flag only gates the stores: its load overlaps the level's loads
+    const int done = __ldcg(c.flags + F_DONE);
+    if(c.L > 2) restrict_level<B>(c, c.ls[2], c.ls[3], GT, GN, done != 0);  // level 1's (count, begin)
 }
 
 // C2: levels 2 -> 3 -> ... (small) by one CTA.  All nodes of the levels >= 2 (contiguous
@@ -2262,7 +2390,8 @@ constexpr int C2_SMEM_BYTES = C2_SMEM_NODES * (16 + 4 + 4);
 template <int B>
 __global__ void __launch_bounds__(1024) k_phase_c2(PcgDev c)
 {
-    if(c.flags[F_DONE]) return;
+    // the stop flag only gates the stores: its load overlaps the nodes' loads
+    const int done = __ldcg(c.flags + F_DONE);
     // level sizes from the parameter block (unrolled constant indices: no dependent loads)
     int last_n = 0, last_b = 0;
 #pragma unroll
@@ -2276,7 +2405,7 @@ __global__ void __launch_bounds__(1024) k_phase_c2(PcgDev c)
     const int total = last_b + last_n - b2;
     if(total > C2_SMEM_NODES)
     {
-        phase_c<B>(c, 2, c.L - 1, threadIdx.x, blockDim.x, true);
+        if(!done) phase_c<B>(c, 2, c.L - 1, threadIdx.x, blockDim.x, true);
         return;
     }
     extern __shared__ float4 c2_smem[];
@@ -2333,6 +2462,7 @@ __global__ void __launch_bounds__(1024) k_phase_c2(PcgDev c)
         }
         __syncthreads();
     }
+    if(done) return;
     for(int i = n2 + threadIdx.x; i < total; i += 1024)
         *reinterpret_cast<float4*>(c.R + 4 * (size_t)(b2 + i)) = rv[i];
 }
@@ -2347,8 +2477,10 @@ __global__ void __launch_bounds__(PB) k_phase_d(PcgDev c)
 template <typename T, int B>
 __global__ void __launch_bounds__(PB, 8) k_phase_e(PcgDev c, int op)
 {
-    if(c.flags[F_DONE]) return;
-    const double v = B > 0 ? phase_e_mas<T>(c, GT, GN) : phase_e_plain<T>(c, GT, GN);
+    // the stop flag only gates the stores: its load overlaps the prolongation's loads
+    const int done = __ldcg(c.flags + F_DONE);
+    const double v = B > 0 ? phase_e_mas<T>(c, GT, GN, done != 0) : phase_e_plain<T>(c, GT, GN, done != 0);
+    if(done) return;
     if(op == POST_INIT_RZ)
     {
         finish_reduction(c, v, SITE_E, POST_INIT_RZ);
