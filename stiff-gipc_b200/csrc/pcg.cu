@@ -2824,7 +2824,7 @@ __global__ void k_upper_slots(const int2* __restrict__ t_ent, const int* __restr
 // Whether the SpMV phase of the next solve runs the upper kernel: when chosen
 // (stg_spmv_tiles), picked by the autotuner, or by default in FP32.  Measured on the
 // 352,947-DOF cube, the FP32 solve takes the same time with either kernel (the upper one
-// moves 1.03x its algorithmic bytes, the full copy 1.68x, and holds half the matrix
+// moves 1.05x its algorithmic bytes, the full copy 1.68x, and holds half the matrix
 // bytes); in FP64 the upper kernel's spill (32 B per transposed product) costs more than it
 // saves and the full copy is the default.  The persistent loop's SpMV reads the full copy.
 static bool upper_spmv_selected(const Solver& S)
