@@ -100,8 +100,7 @@ __device__ __forceinline__ void finish_reduction(const PcgDev& c, double v, int 
         asm volatile("prefetch.global.L1 [%0];" ::"l"(c.scal));
         asm volatile("prefetch.global.L1 [%0];" ::"l"(c.flags));
     }
-    double acc = 0;
-    for(int i = threadIdx.x; i < (int)gridDim.x; i += BLOCK) acc += __ldcg(partials + i);
+    const double acc = strided_sum<BLOCK>(partials, (int)gridDim.x);
     const double tot = block_sum<BLOCK>(acc, red);
     if(threadIdx.x == 0)
     {
@@ -122,8 +121,7 @@ __device__ __forceinline__ double consume_sum(const PcgDev& c, int site, int cou
     __shared__ double red[BLOCK / 32];
     __shared__ double tot;
     const double* part = c.partials + (size_t)site * c.slots;
-    double a = 0;
-    for(int t = threadIdx.x; t < count; t += BLOCK) a += __ldcg(part + t);
+    const double a = strided_sum<BLOCK>(part, count);
     const double s = block_sum<BLOCK>(a, red);
     if(threadIdx.x == 0) tot = s;
     __syncthreads();
@@ -140,12 +138,7 @@ __device__ __forceinline__ void consume_sum2(const PcgDev& c, int site_a, int co
     __shared__ double tot[2];
     const double* pa = c.partials + (size_t)site_a * c.slots;
     const double* pb = c.partials + (size_t)site_b * c.slots;
-    double a = 0, b = 0;
-    for(int t = threadIdx.x; t < count_a || t < count_b; t += BLOCK)
-    {
-        if(t < count_a) a += __ldcg(pa + t);
-        if(t < count_b) b += __ldcg(pb + t);
-    }
+    double a = strided_sum<BLOCK>(pa, count_a), b = strided_sum<BLOCK>(pb, count_b);
     a = warp_sum(a);
     b = warp_sum(b);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

@@ -155,6 +155,29 @@ __device__ __forceinline__ void post_op(int op, int slot, double total, double* 
     }
 }
 
+// This thread's sum of p[t] for t = threadIdx.x, threadIdx.x + BLOCK, ... < count, added in
+// that order from zero.  The loads are issued four at a time before their adds: a loop that
+// adds each load as it comes waits one memory round trip per term.  Adding the zeros of the
+// idle slots changes no bit (a sum that starts from +0 is never -0).
+template <int BLOCK>
+__device__ __forceinline__ double strided_sum(const double* p, int count)
+{
+    double a = 0.0;
+    for(int t0 = threadIdx.x; t0 < count; t0 += 4 * BLOCK)
+    {
+        double v[4];
+#pragma unroll
+        for(int u = 0; u < 4; u++)
+        {
+            const int t = t0 + u * BLOCK;
+            v[u] = t < count ? __ldcg(p + t) : 0.0;
+        }
+#pragma unroll
+        for(int u = 0; u < 4; u++) a += v[u];
+    }
+    return a;
+}
+
 // Every CTA contributes `v` (valid in all threads; summed over the block).  The last CTA to
 // arrive sums the per-CTA partials in index order and applies the post-op.  Deterministic
 // for a fixed grid size.  Must be called by all threads of every CTA of the grid.
@@ -175,8 +198,7 @@ __device__ __forceinline__ void grid_reduce_finish(double v, double* partials, u
     __syncthreads();
     if(!last) return;
     __threadfence();
-    double acc = 0;
-    for(int i = threadIdx.x; i < (int)gridDim.x; i += BLOCK) acc += __ldcg(partials + i);
+    const double acc = strided_sum<BLOCK>(partials, (int)gridDim.x);
     const double tot = block_sum<BLOCK>(acc, red);
     if(threadIdx.x == 0)
     {
